@@ -1,0 +1,366 @@
+"""Benchmark of the dense statevector engine (one JSON line on rank 0).
+
+Headline workload (metric "gate-layer HBM GB/s at 30q c64"): a 30-qubit
+complex64 random circuit of 40 layers -- U3(theta, phi, lambda) on every qubit
+with angles U[0, 2pi) from the seed, then a brick wall of CZ -- fused into tile
+passes.  One step = the whole 40-layer circuit applied to the 8 GiB state that
+stays resident in HBM (inputs far larger than the 126 MB L2).
+value = fused passes x 2 x 2^30 x 8 B / step time (algorithmic bytes: one read
+and one write of the state per pass).
+
+Secondary block "vqe" (metric "VQE grads/s adjoint vs parameter-shift"): the
+24-qubit complex64 hardware-efficient ansatz of 10 layers (480 parameters)
+with the open-chain transverse-field Ising Hamiltonian; adjoint gradients per
+second against parameter-shift gradients (2 x 480 forward runs) on the same
+kernels.
+
+Multi-GPU: replicas only -- every rank runs the same workload on its own GPU,
+value is the sum over ranks, time the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'dense-evolution_b200'))
+sys.path.insert(0, ROOT)
+
+N_QUBITS, LAYERS, SEED = 30, 40, 2024
+VQE_N, VQE_LAYERS = 24, 10
+METRIC = 'gate-layer HBM GB/s at 30q c64; VQE grads/s adjoint vs parameter-shift'
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), 'measured (MEASURED_PEAKS.json hbm_gbs)'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback 6.65 TB/s'
+
+
+def _profile_traffic():
+    """DRAM bytes per fused-pass launch from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, 'profiles', 'fused_pass_30q_c64.txt')
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith('dram_bytes_per_launch_full_size:'):
+                    return float(line.split(':', 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--query-gpu={self.Q}', '--format=csv,noheader,nounits',
+                                          '-lms', '200', '-i', str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(',')]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower() == 'active':
+                    reasons.add(name)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled'], 'samples': 0}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': max(mx), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    return ws, rank, local
+
+
+def _max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (a NumPy restatement of the reference's eager path)
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(n=N_QUBITS, gates=3):
+    """Time `gates` single-gate passes of the workload at full size on the host
+    (complex64, like the workload); returns GB/s by the same algorithmic-byte rule."""
+    from oracle import sv_oracle as O
+    from dense_evolution.workloads import brick_u3_circuit
+    circ = O.transpile(brick_u3_circuit(n, 1, SEED))[:gates]
+    sv = np.zeros(1 << n, dtype=np.complex64)
+    sv[0] = 1
+    t0 = time.perf_counter()
+    for cmd in circ:
+        sv = O.run_circuit(sv, n, [cmd], do_transpile=False)
+    dt = time.perf_counter() - t0
+    gbs = len(circ) * 2 * (1 << n) * 8 / dt / 1e9
+    return {'value': gbs, 'unit': 'GB/s', 'cores': 1, 'kind': 'port',
+            'sample': f'{len(circ)} single-gate passes (first gates of layer 0) of the {n}-qubit complex64 '
+                      f'circuit through the NumPy oracle, {dt:.1f} s'}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    res = None
+    t0 = time.perf_counter()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(N_QUBITS, gates=1)
+        if i >= args.warmup:
+            vals.append(r['value'])
+        res = r
+    v = float(np.mean(vals))
+    line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'GB/s', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'complex64', 'data': 'synthetic',
+            'config': {'workload': f'{N_QUBITS}-qubit complex64 random circuit, {LAYERS} layers of U3 + brick CZ '
+                                   f'(one reference pass per gate)', 'seed': SEED},
+            'cpu_baseline': {'value': v, 'unit': 'GB/s', 'cores': 1, 'kind': 'port',
+                             'sample': 'one single-gate pass per step at 30 qubits, NumPy oracle'},
+            'e2e': {'value': v, 'unit': 'GB/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+            'wall_s': time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    import dense_evolution as de
+    from dense_evolution import _native as N
+    from dense_evolution.circuits.compiler import CompiledCircuit
+    from dense_evolution.workloads import brick_u3_circuit
+
+    dev = torch.device('cuda', torch.cuda.current_device())
+    st = torch.cuda.current_stream()
+    n = N_QUBITS
+    circ = brick_u3_circuit(n, LAYERS, SEED)
+    t_c = time.perf_counter()
+    plan = CompiledCircuit(de.QuantumTranspiler.transpile(circ), n, torch.complex64)
+    compile_s = time.perf_counter() - t_c
+    npasses = len(plan.packed.passes)
+    sv = torch.empty(1 << n, dtype=torch.complex64, device=dev)
+    lib = N.lib()
+    N.check(lib.desv_init_basis(ctypes.c_void_p(sv.data_ptr()), n, N.DESV_C64, 0, ctypes.c_void_p(st.cuda_stream)),
+            'init')
+    ops_t, mats_t = plan.device_arrays(dev)
+    passes = plan.packed.passes
+    pass_bytes = 2 * (1 << n) * 8
+
+    def one_pass(i):
+        N.check(lib.desv_apply_passes(ctypes.c_void_p(sv.data_ptr()), n, N.DESV_C64,
+                                      ctypes.c_void_p(passes[i:i + 1].ctypes.data), 1,
+                                      ctypes.c_void_p(ops_t.data_ptr()), ctypes.c_void_p(mats_t.data_ptr()),
+                                      ctypes.c_void_p(st.cuda_stream)), 'pass')
+
+    for _ in range(args.warmup):
+        for i in range(npasses):
+            one_pass(i)
+    torch.cuda.synchronize()
+    _barrier(ws)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps * npasses + 1)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        _barrier(ws)
+        ev[0].record()
+        k = 1
+        for _ in range(args.steps):
+            for i in range(npasses):
+                one_pass(i)
+                ev[k].record()
+                k += 1
+        torch.cuda.synchronize()
+    N.device_status()
+    total_ms = ev[0].elapsed_time(ev[-1])
+    per_pass = np.array([ev[j].elapsed_time(ev[j + 1]) for j in range(len(ev) - 1)])
+    ms_step = _max_over_ranks(total_ms / args.steps, ws)
+    value = ws * npasses * pass_bytes / (ms_step / 1e3) / 1e9
+    avg_pass_ms = float(per_pass.mean())
+    achieved = pass_bytes / (avg_pass_ms / 1e3) / 1e9
+    peak, peak_src = _peaks()
+    traffic = _profile_traffic()
+
+    # ---- end to end through the public API: fresh seeded angles every step,
+    # circuit transpile + fusion + H2D of the op/matrix tables, run, <Z_i> read back
+    sim = de.DenseSVSimulator(n, use_float32=True)
+    e2e_times, h2d = [], 0
+    for i in range(args.warmup + args.steps):
+        c = brick_u3_circuit(n, LAYERS, SEED + 1 + i)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.set_initial_state(None)
+        plan_i = sim.compile(c)
+        sim.run_circuit(c)
+        z = sim.expectation_z()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_times.append(dt)
+            h2d = int(plan_i.packed.ops.nbytes + plan_i.device_arrays(dev)[1].numel() * 4)
+        sim._plans.clear()
+    e2e_step = _max_over_ranks(float(np.mean(e2e_times)), ws)
+    e2e_passes = npasses
+    e2e_value = ws * e2e_passes * pass_bytes / e2e_step / 1e9
+    del sim
+    torch.cuda.empty_cache()
+
+    vqe = run_vqe(args) if not args.skip_vqe else None
+    cpu = cpu_baseline() if (rank == 0 and ws == 1 and not args.skip_cpu) else None
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'complex64 (fp32 gate math)', 'data': 'synthetic',
+            'config': {'workload': f'{n}-qubit complex64 random circuit, {LAYERS} layers of U3 on every qubit + '
+                                   f'brick-wall CZ, fused into tile passes', 'seed': SEED, 'qubits': n,
+                       'layers': LAYERS, 'fused_passes': npasses, 'tile_bits': plan.tile_bits,
+                       'l2': 'state (8 GiB) far larger than L2; no flush needed', 'parallelism': f'replicas x{ws}'},
+            'passes_per_step': npasses, 'layers_per_s': ws * LAYERS / (ms_step / 1e3),
+            'ms_per_layer': ms_step / LAYERS, 'compile_s': compile_s,
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_src,
+                         'kernel': 'k_fused_pass<float2,12,4>', 'algorithmic_bytes_per_launch': pass_bytes,
+                         'avg_launch_ms': avg_pass_ms, 'min_launch_ms': float(per_pass.min()),
+                         'max_launch_ms': float(per_pass.max())},
+            'e2e': {'value': e2e_value, 'unit': 'GB/s', 'h2d_bytes_per_step': h2d,
+                    'd2h_bytes_per_step': (n + 1) * 8, 'ms_per_step': e2e_step * 1e3,
+                    'path': 'DenseSVSimulator.run_circuit (new angles each step: transpile + fusion + upload) + '
+                            'expectation_z()'},
+            'gpu_launches': args.steps * npasses,
+            'clocks': clk.summary(),
+            'cpu_baseline': cpu,
+            'vqe': vqe,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_vqe(args):
+    """Config 3: adjoint grads/s vs parameter-shift grads/s at 24q complex64."""
+    import torch
+    import dense_evolution as de
+    from dense_evolution.workloads import hea_circuit, tfim_terms
+    n, layers = VQE_N, VQE_LAYERS
+    fn, npar = de.circuit_to_energy_fn(hea_circuit(n, layers), n, use_float32=True)
+    prog = fn.program
+    op = de.PauliSumOperator(tfim_terms(n), n)
+    theta = np.random.default_rng(SEED).uniform(-np.pi, np.pi, npar)
+    for _ in range(max(1, args.warmup)):
+        prog.value_and_grad(theta, op)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = max(3, args.steps)
+    for _ in range(reps):
+        e, g, _ = prog.value_and_grad(theta, op)
+    torch.cuda.synchronize()
+    adj_s = (time.perf_counter() - t0) / reps
+    # parameter shift on the same kernels: 2 * npar forward runs + <H>
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ps = prog.parameter_shift_grad(theta, op)
+    torch.cuda.synchronize()
+    ps_s = time.perf_counter() - t0
+    return {'workload': f'{n}-qubit complex64 HEA, {layers} layers (RY,RZ + CX ladder), {npar} parameters, '
+                        f'TFIM open chain', 'energy': e, 'adjoint_grads_per_s': 1.0 / adj_s,
+            'parameter_shift_grads_per_s': 1.0 / ps_s, 'adjoint_over_parameter_shift': ps_s / adj_s,
+            'max_abs_grad_diff_adjoint_vs_shift': float(np.max(np.abs(g - ps))),
+            'forward_passes': int(len(prog.forward.packed.passes)),
+            'backward_passes': int(len(prog.back.passes)), 'adjoint_ms': adj_s * 1e3, 'shift_ms': ps_s * 1e3}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--skip-vqe', action='store_true')
+    ap.add_argument('--skip-cpu', action='store_true')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == '__main__':
+    main()

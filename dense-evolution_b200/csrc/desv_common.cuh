@@ -1,0 +1,136 @@
+// Shared device helpers of libdesv: complex arithmetic, the sm_90+/sm_100
+// bulk-copy (TMA, non-tensor) + mbarrier primitives written as inline PTX,
+// bounded waits, and the host-side error plumbing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "desv.h"
+
+namespace desv {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int check_launch(const char *what);
+int sm_count();
+
+// Device-side status word: bounded waits set it instead of hanging.  Each
+// translation unit has its own copy (no relocatable device code); every unit
+// registers a reader with the API layer at load time.
+#define DESV_DEV_TIMEOUT 1
+static __device__ int g_dev_status = 0;
+void register_status_reader(int (*reader)());
+static int tu_status_read_clear() {
+    int h = 0;
+    if (cudaMemcpyFromSymbol(&h, g_dev_status, sizeof(int)) != cudaSuccess) return 0;
+    if (h) {
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_dev_status, &zero, sizeof(int));
+    }
+    return h;
+}
+static const int tu_status_registered = (register_status_reader(&tu_status_read_clear), 0);
+
+// ---------------------------------------------------------------- complex
+template <typename R> struct CT;
+template <> struct CT<float> { using T = float2; };
+template <> struct CT<double> { using T = double2; };
+template <typename R> using cx = typename CT<R>::T;
+
+__device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+
+// acc + a*b
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 acc) {
+    return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y)));
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 acc) {
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// real coefficient r times a, plus acc
+__device__ __forceinline__ float2 rfma(float r, float2 a, float2 acc) {
+    return make_float2(fmaf(r, a.x, acc.x), fmaf(r, a.y, acc.y));
+}
+__device__ __forceinline__ double2 rfma(double r, double2 a, double2 acc) {
+    return make_double2(fma(r, a.x, acc.x), fma(r, a.y, acc.y));
+}
+template <typename T> __device__ __forceinline__ T cneg(T a) { a.x = -a.x; a.y = -a.y; return a; }
+
+__device__ __forceinline__ float2 shfl_xor(float2 v, int m) {
+    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+__device__ __forceinline__ double2 shfl_xor(double2 v, int m) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// insert a zero bit at position p of x
+__device__ __forceinline__ uint64_t insert0(uint64_t x, int p) {
+    uint64_t lo = x & ((1ull << p) - 1ull);
+    return ((x >> p) << (p + 1)) | lo;
+}
+
+// ---------------------------------------------------------------- mbarrier / bulk copy (PTX ISA 8.0+, sm_90+)
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~`limit` polls (each try_wait itself blocks for a
+// hardware-defined slice), records DESV_DEV_TIMEOUT and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t limit = (1u << 22)) {
+    for (uint32_t it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(&g_dev_status, DESV_DEV_TIMEOUT);
+    return false;
+}
+// global -> shared bulk copy, completion counted on `bar` (bytes multiple of 16, both 16B aligned)
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst_smem)),
+        "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// shared -> global bulk copy in the issuing thread's bulk group
+__device__ __forceinline__ void bulk_s2g(void *dst_gmem, const void *src_smem, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem),
+                 "r"(smem_addr(src_smem)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+}  // namespace desv

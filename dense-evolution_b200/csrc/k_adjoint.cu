@@ -1,0 +1,237 @@
+// Fused adjoint backward pass (adjoint-method gradient of E = <psi|H|psi>).
+//
+// The reference differentiates with jax.grad through lax.scan
+// (solvers/autodiff.py:136-166), which stores a residual state per gate.  The
+// adjoint method needs two working states instead: phi (the circuit state,
+// un-applied gate by gate) and lambda (= H psi, un-applied alongside).  For a
+// gate U(theta) with dU/dtheta = G U, the derivative is 2 Re<lambda|G|phi>
+// taken just before U is un-applied.  Here one tile pass loads the phi and
+// lambda tiles, walks its stretch of the reversed circuit in registers -- GRAD
+// ops accumulate the FP64 inner products, inverse-gate ops un-apply -- and
+// writes both tiles back: 4 * 2^n amplitudes of HBM traffic per pass for any
+// number of gates and gradient terms in it.
+#include "desv_common.cuh"
+#include "stage_ops.cuh"
+#include "tile_pipeline.cuh"
+
+namespace desv {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Re sum conj(b) (G a) for a 2x2 generator on register slot S (compile-time
+// register indices keep a[] and b[] in registers).
+template <int S, typename T>
+__device__ __forceinline__ decltype(T().x) grad_reg(const T (&a)[16], const T (&b)[16], T g00, T g01, T g10, T g11,
+                                                    int cs) {
+    decltype(T().x) acc = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if ((j >> S) & 1) continue;
+        if (cs >= 0 && !((j >> cs) & 1)) continue;
+        const int j1 = j | (1 << S);
+        const T v0 = cfma(g01, a[j1], cmul(g00, a[j]));
+        const T v1 = cfma(g11, a[j1], cmul(g10, a[j]));
+        acc += b[j].x * v0.x + b[j].y * v0.y + b[j1].x * v1.x + b[j1].y * v1.y;
+    }
+    return acc;
+}
+
+// Re sum conj(b) (G a) over the thread's amplitudes for a GRAD op.
+//   s1 == 0: G = 2x2 generator on register slot / lane bit s0 (controls as M1)
+//   s1 == 1: G = diagonal over global bits ga, gb (factor d[bit(ga) + 2 bit(gb)])
+template <typename T>
+__device__ __forceinline__ double grad_term(const T (&a)[16], const T (&b)[16], const desv_op &op, const T *mp,
+                                            uint64_t tg, int lane) {
+    // predicate is applied at the end: lane-bit generators shuffle with every lane
+    const bool pred = (tg & op.cmask) == op.cval;
+    typedef decltype(a[0].x) R;
+    R acc = 0;
+    if (op.s1 == 1) {
+        const T d0 = mp[0], d1 = mp[1], d2 = mp[2], d3 = mp[3];
+        const int fa = op.ga == 0xFF ? 0 : (int)((tg >> op.ga) & 1ull);
+        const int fb = op.gb == 0xFF ? 0 : (int)((tg >> op.gb) & 1ull);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int ba = op.sa >= 0 ? ((j >> op.sa) & 1) : fa;
+            const int bb = op.sb >= 0 ? ((j >> op.sb) & 1) : fb;
+            const int k = ba | (bb << 1);
+            const T f = k == 0 ? d0 : k == 1 ? d1 : k == 2 ? d2 : d3;
+            const T ga = cmul(f, a[j]);
+            acc += b[j].x * ga.x + b[j].y * ga.y;
+        }
+        return pred ? (double)acc : 0.0;
+    }
+    const T g00 = mp[0], g01 = mp[1], g10 = mp[2], g11 = mp[3];
+    const int cs = op.cslot;
+    if (op.s0 >= 16) {
+        const int lb = op.s0 - 16;
+        const int mine = (lane >> lb) & 1;
+        const T cself = mine ? g11 : g00, coth = mine ? g10 : g01;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (cs >= 0 && !((j >> cs) & 1)) continue;
+            const T p = shfl_xor(a[j], 1 << lb);
+            const T v = cfma(coth, p, cmul(cself, a[j]));
+            acc += b[j].x * v.x + b[j].y * v.y;
+        }
+        return pred ? (double)acc : 0.0;
+    }
+    switch (op.s0) {
+        case 0: acc = grad_reg<0>(a, b, g00, g01, g10, g11, cs); break;
+        case 1: acc = grad_reg<1>(a, b, g00, g01, g10, g11, cs); break;
+        case 2: acc = grad_reg<2>(a, b, g00, g01, g10, g11, cs); break;
+        default: acc = grad_reg<3>(a, b, g00, g01, g10, g11, cs); break;
+    }
+    return pred ? (double)acc : 0.0;
+}
+
+template <typename T, int K, int NBUF>
+__global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, TileGeom g, const desv_op *ops,
+                                                                int nops, const T *mats, int nparams, double *part) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
+    double *acc = reinterpret_cast<double *>(smem + 128 + (size_t)NBUF * 2 * (1u << K) * sizeof(T));
+    for (int i = threadIdx.x; i < NW * nparams; i += blockDim.x) acc[i] = 0.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    PipeArrays<T, 2> A;
+    A.ptr[0] = phi;
+    A.ptr[1] = lam;
+    A.load[0] = A.load[1] = true;
+    A.store[0] = A.store[1] = true;
+    auto body = [&](T *const *sp, uint64_t base, uint64_t) {
+        T *sphi = sp[0], *slam = sp[1];
+        int k = 0;
+#pragma unroll 1
+        while (k < nops) {
+            const desv_op st = ops[k];
+            const int cnt = (int)st.mat;
+            const uint32_t idx = stage_base(threadIdx.x, st.g);
+            const uint32_t o0 = 1u << st.g[0], o1 = 1u << st.g[1], o2 = 1u << st.g[2], o3 = 1u << st.g[3];
+            T a[16], b[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const uint32_t off = idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) +
+                                     ((j & 8) ? o3 : 0u);
+                a[j] = sphi[off];
+                b[j] = slam[off];
+            }
+            const uint64_t tg = base | tile_local_to_global(g, idx);
+#pragma unroll 1
+            for (int q = 1; q <= cnt; ++q) {
+                const desv_op op = ops[k + q];
+                if (op.kind == DESV_OP_GRAD) {
+                    double v = grad_term(a, b, op, mats + op.mat, tg, lane);
+                    v = warp_sum_d(v);
+                    if (lane == 0) acc[warp * nparams + op.param] += v;
+                } else {
+                    apply_one_op(a, op, mats, tg, lane);
+                    apply_one_op(b, op, mats, tg, lane);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const uint32_t off = idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) +
+                                     ((j & 8) ? o3 : 0u);
+                sphi[off] = a[j];
+                slam[off] = b[j];
+            }
+            __syncthreads();
+            k += 1 + cnt;
+        }
+    };
+    __syncthreads();
+    run_tiles<T, K, NBUF, 2>(g, A, body, smem);
+    __syncthreads();
+    for (int p = threadIdx.x; p < nparams; p += blockDim.x) {
+        double s = 0;
+        for (int w = 0; w < NW; ++w) s += acc[w * nparams + p];
+        part[(size_t)blockIdx.x * nparams + p] = s;
+    }
+}
+
+// grad[map[p]] += 2 * sum_r part[r * np + p]   (fixed summation order)
+__global__ void k_grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad) {
+    __shared__ double sh[32];
+    for (int p = 0; p < np; ++p) {
+        double v = 0;
+        for (int r = threadIdx.x; r < rows; r += blockDim.x) v += part[(size_t)r * np + p];
+        v = warp_sum_d(v);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        __syncthreads();
+        if (l == 0) sh[w] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+            grad[map[p]] += 2.0 * t;
+        }
+    }
+}
+
+constexpr int ADJ_MAX_PARAMS = 1024;
+constexpr int ADJ_MAX_ROWS = 1184;  // partial-sum rows per pass (= grid bound)
+
+template <typename T, int K, int NBUF> static size_t adj_smem(int nparams) {
+    constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
+    return 128 + (size_t)NBUF * 2 * (1u << K) * sizeof(T) + (size_t)NW * nparams * sizeof(double);
+}
+
+template <typename T, int K, int NBUF>
+static int launch_adj(T *phi, T *lam, const TileGeom &g, const desv_op *ops, int nops, const T *mats, int nparams,
+                      double *part, int *grid_out, cudaStream_t st) {
+    static int bps[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smax = adj_smem<T, K, NBUF>(ADJ_MAX_PARAMS);
+    if (bps[dev & 63] == 0) {
+        cudaFuncSetAttribute(k_adjoint_pass<T, K, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_adjoint_pass<T, K, NBUF>, 1 << (K - 4), smax);
+        bps[dev & 63] = b > 0 ? b : 1;
+    }
+    const uint64_t ntiles = 1ull << (g.n - K);
+    uint64_t cap = (uint64_t)sm_count() * bps[dev & 63];
+    if (cap > ADJ_MAX_ROWS) cap = ADJ_MAX_ROWS;
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    *grid_out = grid;
+    k_adjoint_pass<T, K, NBUF><<<grid, 1 << (K - 4), adj_smem<T, K, NBUF>(nparams), st>>>(phi, lam, g, ops, nops, mats,
+                                                                                          nparams, part);
+    return check_launch("adjoint pass");
+}
+
+int adjoint_pass(void *phi, void *lam, int dtype, const TileGeom &g, const desv_op *ops, int nops, const void *mats,
+                 int nparams, double *part, int *grid_out, cudaStream_t st) {
+    if (nparams < 0 || nparams > ADJ_MAX_PARAMS) return fail(DESV_EINVAL, "adjoint pass: at most 1024 parameters");
+    if (dtype == DESV_C64) {
+        float2 *p = static_cast<float2 *>(phi), *l = static_cast<float2 *>(lam);
+        const float2 *m = static_cast<const float2 *>(mats);
+        switch (g.K) {
+            case 9: return launch_adj<float2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+            case 10: return launch_adj<float2, 10, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+            case 11: return launch_adj<float2, 11, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+            default: return fail(DESV_EINVAL, "adjoint pass: complex64 tile_bits must be 9..11");
+        }
+    }
+    double2 *p = static_cast<double2 *>(phi), *l = static_cast<double2 *>(lam);
+    const double2 *m = static_cast<const double2 *>(mats);
+    switch (g.K) {
+        case 9: return launch_adj<double2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+        case 10: return launch_adj<double2, 10, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+        default: return fail(DESV_EINVAL, "adjoint pass: complex128 tile_bits must be 9..10");
+    }
+}
+
+int grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad, cudaStream_t st) {
+    k_grad_reduce<<<1, 256, 0, st>>>(part, rows, np, map, grad);
+    return check_launch("gradient reduce");
+}
+
+size_t adjoint_scratch_bytes(int max_params) {
+    return (size_t)ADJ_MAX_ROWS * (size_t)(max_params > 0 ? max_params : 1) * sizeof(double) + 4096;
+}
+
+}  // namespace desv

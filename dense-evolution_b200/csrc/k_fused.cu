@@ -1,0 +1,93 @@
+// Fused gate pass: one HBM read + one HBM write of the state per pass, all of
+// the pass's gates applied to shared-memory tiles in register stages.
+// Replaces the per-gate lax.scan step of the reference
+// (dense_evolution/circuits/compiler.py:136-355), which reads, gathers and
+// writes the full state once per gate.
+#include "desv_common.cuh"
+#include "stage_ops.cuh"
+#include "tile_pipeline.cuh"
+
+namespace desv {
+
+template <typename T, int K>
+__device__ __forceinline__ void fused_tile_body(T *s, uint64_t base, const TileGeom &g, const desv_op *ops, int nops,
+                                                const T *mats) {
+    const int lane = threadIdx.x & 31;
+    int k = 0;
+#pragma unroll 1
+    while (k < nops) {
+        const desv_op st = ops[k];
+        const int cnt = (int)st.mat;
+        const uint32_t idx = stage_base(threadIdx.x, st.g);
+        const uint32_t o0 = 1u << st.g[0], o1 = 1u << st.g[1], o2 = 1u << st.g[2], o3 = 1u << st.g[3];
+        T a[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            a[j] = s[idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) + ((j & 8) ? o3 : 0u)];
+        const uint64_t tg = base | tile_local_to_global(g, idx);
+        run_stage_ops(a, ops + k + 1, cnt, mats, tg, lane);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            s[idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) + ((j & 8) ? o3 : 0u)] = a[j];
+        __syncthreads();
+        k += 1 + cnt;
+    }
+}
+
+template <typename T, int K, int NBUF>
+__global__ void __launch_bounds__(1 << (K - 4)) k_fused_pass(T *sv, TileGeom g, const desv_op *ops, int nops,
+                                                              const T *mats) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    PipeArrays<T, 1> A;
+    A.ptr[0] = sv;
+    A.load[0] = true;
+    A.store[0] = true;
+    auto body = [&](T *const *sp, uint64_t base, uint64_t) { fused_tile_body<T, K>(sp[0], base, g, ops, nops, mats); };
+    run_tiles<T, K, NBUF, 1>(g, A, body, smem);
+}
+
+template <typename T, int K, int NBUF>
+static int launch_fused(T *sv, const TileGeom &g, const desv_op *ops, int nops, const T *mats, cudaStream_t st) {
+    static int bps[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smem = 128 + (size_t)NBUF * (1u << K) * sizeof(T);
+    if (bps[dev & 63] == 0) {
+        cudaFuncSetAttribute(k_fused_pass<T, K, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fused_pass<T, K, NBUF>, 1 << (K - 4), smem);
+        bps[dev & 63] = b > 0 ? b : 1;
+    }
+    const uint64_t ntiles = 1ull << (g.n - K);
+    const uint64_t cap = (uint64_t)sm_count() * bps[dev & 63];
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    k_fused_pass<T, K, NBUF><<<grid, 1 << (K - 4), smem, st>>>(sv, g, ops, nops, mats);
+    return check_launch("fused pass");
+}
+
+int fused_pass(void *sv, int dtype, const TileGeom &g, const desv_op *ops, int nops, const void *mats,
+               cudaStream_t st) {
+    if (dtype == DESV_C64) {
+        float2 *p = static_cast<float2 *>(sv);
+        const float2 *m = static_cast<const float2 *>(mats);
+        switch (g.K) {
+            case 9: return launch_fused<float2, 9, 4>(p, g, ops, nops, m, st);
+            case 10: return launch_fused<float2, 10, 4>(p, g, ops, nops, m, st);
+            case 11: return launch_fused<float2, 11, 4>(p, g, ops, nops, m, st);
+            case 12: return launch_fused<float2, 12, 4>(p, g, ops, nops, m, st);
+            case 13: return launch_fused<float2, 13, 3>(p, g, ops, nops, m, st);
+            default: return fail(DESV_EINVAL, "fused pass: complex64 tile_bits must be 9..13");
+        }
+    }
+    double2 *p = static_cast<double2 *>(sv);
+    const double2 *m = static_cast<const double2 *>(mats);
+    switch (g.K) {
+        case 9: return launch_fused<double2, 9, 4>(p, g, ops, nops, m, st);
+        case 10: return launch_fused<double2, 10, 4>(p, g, ops, nops, m, st);
+        case 11: return launch_fused<double2, 11, 4>(p, g, ops, nops, m, st);
+        case 12: return launch_fused<double2, 12, 3>(p, g, ops, nops, m, st);
+        default: return fail(DESV_EINVAL, "fused pass: complex128 tile_bits must be 9..12");
+    }
+}
+
+}  // namespace desv

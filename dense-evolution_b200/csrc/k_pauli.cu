@@ -1,0 +1,272 @@
+// Fused Pauli-sum kernels: <psi|H|psi> and H|psi> for H = sum_k c_k P_k.
+//
+// The reference applies one term at a time, each as >= 4 full passes
+// (arange, XOR, a per-qubit coefficient array, a gather -- physics/
+// observables.py:63-94,152-186,250-308).  Here the host groups terms into
+// tile passes: every term whose flip mask lies inside a pass's tile bits is
+// evaluated from the shared-memory tile, so all terms of a pass cost one read
+// of psi.  (P_k psi)[i] = psi[i ^ x_k] * c_k * (-1)^popcount((i ^ x_k) & z_k),
+// where c_k already carries the i^(#Y) factor.  Per amplitude the term sum is
+// formed in the state's precision; the expectation is accumulated in FP64.
+#include "desv_common.cuh"
+#include "tile_pipeline.cuh"
+
+namespace desv {
+
+constexpr int PAULI_THREADS = 256;
+constexpr int PAULI_MAX_TERMS = 512;
+
+template <typename T> struct TermTab {
+    uint32_t xl[PAULI_MAX_TERMS];
+    uint32_t zl[PAULI_MAX_TERMS];
+    T c[PAULI_MAX_TERMS];
+    uint8_t pb[PAULI_MAX_TERMS];
+};
+
+__device__ __forceinline__ uint32_t global_to_tile_local(const TileGeom &g, uint64_t m) {
+    uint32_t x = (uint32_t)(m & ((1ull << g.L) - 1ull));
+    for (int i = 0; i < g.K - g.L; ++i)
+        if ((m >> g.high[i]) & 1ull) x |= 1u << (g.L + i);
+    return x;
+}
+
+// MODE 0: expectation only; 1: matvec overwrite (+ optional expectation); 2: matvec accumulate
+template <typename T, int K, int NBUF, int MODE>
+__global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, TileGeom g, const desv_pauli_term *terms,
+                                                         int nterms, int want_e, double *part) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int NARR = MODE == 0 ? 1 : 2;
+    TermTab<T> *tab = reinterpret_cast<TermTab<T> *>(smem + 128 + (size_t)NBUF * NARR * (1u << K) * sizeof(T));
+    for (int k = threadIdx.x; k < nterms; k += blockDim.x) {
+        const desv_pauli_term tm = terms[k];
+        tab->xl[k] = global_to_tile_local(g, tm.xmask);
+        tab->zl[k] = global_to_tile_local(g, tm.zmask);
+        T c;
+        c.x = (decltype(c.x))tm.cre;
+        c.y = (decltype(c.y))tm.cim;
+        tab->c[k] = c;
+    }
+    PipeArrays<T, NARR> A;
+    A.ptr[0] = const_cast<T *>(psi);
+    A.load[0] = true;
+    A.store[0] = false;
+    if (NARR == 2) {
+        A.ptr[NARR - 1] = out;
+        A.load[NARR - 1] = MODE == 2;
+        A.store[NARR - 1] = true;
+    }
+    double ere = 0, eim = 0;
+    auto body = [&](T *const *sp, uint64_t base, uint64_t) {
+        // parity of the tile's fixed bits under each term's sign mask
+        for (int k = threadIdx.x; k < nterms; k += blockDim.x)
+            tab->pb[k] = (uint8_t)(__popcll(base & terms[k].zmask) & 1);
+        __syncthreads();
+        const T *s = sp[0];
+#pragma unroll 1
+        for (uint32_t j = threadIdx.x; j < (1u << K); j += PAULI_THREADS) {
+            T v = mk(decltype(s[0].x)(0), decltype(s[0].x)(0));
+            uint32_t last_x = 0xFFFFFFFFu;
+            T p = s[j];
+#pragma unroll 4
+            for (int k = 0; k < nterms; ++k) {
+                const uint32_t xl = tab->xl[k];
+                if (xl != last_x) {
+                    p = s[j ^ xl];
+                    last_x = xl;
+                }
+                const int sg = (__popc((j ^ xl) & tab->zl[k]) ^ tab->pb[k]) & 1;
+                const T c = tab->c[k];
+                v = sg ? cfma(cneg(c), p, v) : cfma(c, p, v);
+            }
+            if (MODE != 0 || want_e) {
+                const T a = s[j];
+                ere += (double)a.x * (double)v.x + (double)a.y * (double)v.y;
+                eim += (double)a.x * (double)v.y - (double)a.y * (double)v.x;
+            }
+            if (MODE == 1) sp[NARR - 1][j] = v;
+            if (MODE == 2) {
+                T o = sp[NARR - 1][j];
+                o.x += v.x;
+                o.y += v.y;
+                sp[NARR - 1][j] = o;
+            }
+        }
+    };
+    __syncthreads();
+    run_tiles<T, K, NBUF, NARR>(g, A, body, smem);
+    if (want_e) {
+        __shared__ double sh[32];
+        double r = ere;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        double i2 = eim;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) i2 += __shfl_xor_sync(0xffffffffu, i2, o);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        __syncthreads();
+        if (l == 0) sh[w] = r;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int k = 0; k < PAULI_THREADS / 32; ++k) t += sh[k];
+            part[2 * blockIdx.x] = t;
+        }
+        __syncthreads();
+        if (l == 0) sh[w] = i2;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int k = 0; k < PAULI_THREADS / 32; ++k) t += sh[k];
+            part[2 * blockIdx.x + 1] = t;
+        }
+    }
+}
+
+template <typename T, int K, int NBUF, int MODE>
+static int launch_pauli(const T *psi, T *out, const TileGeom &g, const desv_pauli_term *terms, int nterms, int want_e,
+                        double *part, int *grid_out, cudaStream_t st) {
+    static int bps[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    constexpr int NARR = MODE == 0 ? 1 : 2;
+    const size_t smem = 128 + (size_t)NBUF * NARR * (1u << K) * sizeof(T) + sizeof(TermTab<T>);
+    if (bps[dev & 63] == 0) {
+        cudaFuncSetAttribute(k_pauli<T, K, NBUF, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_pauli<T, K, NBUF, MODE>, PAULI_THREADS, smem);
+        bps[dev & 63] = b > 0 ? b : 1;
+    }
+    const uint64_t ntiles = 1ull << (g.n - K);
+    const uint64_t cap = (uint64_t)sm_count() * bps[dev & 63];
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    *grid_out = grid;
+    k_pauli<T, K, NBUF, MODE><<<grid, PAULI_THREADS, smem, st>>>(psi, out, g, terms, nterms, want_e, part);
+    return check_launch("pauli pass");
+}
+
+// Terms whose flip mask spans more high bits than a tile holds: every thread
+// reads psi[i] and psi[i ^ x] straight from global memory (i ^ x keeps
+// consecutive i contiguous, so the loads stay coalesced).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_pauli_direct(const T *psi, T *out, uint64_t dim,
+                                                      const desv_pauli_term *terms, int nterms, int want_e,
+                                                      double *part) {
+    double ere = 0, eim = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+        T v = mk(decltype(psi[0].x)(0), decltype(psi[0].x)(0));
+        for (int k = 0; k < nterms; ++k) {
+            const desv_pauli_term tm = terms[k];
+            const uint64_t src = i ^ tm.xmask;
+            const T p = psi[src];
+            T c;
+            c.x = (decltype(c.x))tm.cre;
+            c.y = (decltype(c.y))tm.cim;
+            v = (__popcll(src & tm.zmask) & 1) ? cfma(cneg(c), p, v) : cfma(c, p, v);
+        }
+        if (want_e) {
+            const T a = psi[i];
+            ere += (double)a.x * (double)v.x + (double)a.y * (double)v.y;
+            eim += (double)a.x * (double)v.y - (double)a.y * (double)v.x;
+        }
+        if (MODE == 1) out[i] = v;
+        if (MODE == 2) {
+            T o = out[i];
+            o.x += v.x;
+            o.y += v.y;
+            out[i] = o;
+        }
+    }
+    if (want_e) {
+        __shared__ double sh[32];
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ere += __shfl_xor_sync(0xffffffffu, ere, o);
+            eim += __shfl_xor_sync(0xffffffffu, eim, o);
+        }
+        if (l == 0) sh[w] = ere;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+            part[2 * blockIdx.x] = t;
+        }
+        __syncthreads();
+        if (l == 0) sh[w] = eim;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+            part[2 * blockIdx.x + 1] = t;
+        }
+    }
+}
+
+int pauli_direct(const void *psi, void *out, int dtype, int mode, int n, const desv_pauli_term *terms, int nterms,
+                 int want_e, double *part, int *grid_out, cudaStream_t st) {
+    const uint64_t dim = 1ull << n;
+    uint64_t b = (dim + 255) / 256;
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    const int grid = (int)(b < cap ? b : cap);
+    *grid_out = grid;
+#define DESV_PD(T, M)                                                                                          \
+    k_pauli_direct<T, M><<<grid, 256, 0, st>>>(static_cast<const T *>(psi), static_cast<T *>(out), dim, terms, \
+                                               nterms, want_e, part)
+    if (dtype == DESV_C64) {
+        if (mode == 0) DESV_PD(float2, 0);
+        else if (mode == 1) DESV_PD(float2, 1);
+        else DESV_PD(float2, 2);
+    } else {
+        if (mode == 0) DESV_PD(double2, 0);
+        else if (mode == 1) DESV_PD(double2, 1);
+        else DESV_PD(double2, 2);
+    }
+#undef DESV_PD
+    return check_launch("pauli direct pass");
+}
+
+template <typename T, int K, int MODE>
+static int pauli_k(const T *p, T *o, const TileGeom &g, const desv_pauli_term *terms, int nterms, int want_e,
+                   double *part, int *grid_out, cudaStream_t st) {
+    return launch_pauli<T, K, 4, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+}
+
+template <typename T, int MODE>
+static int pauli_dispatch(const T *p, T *o, const TileGeom &g, const desv_pauli_term *terms, int nterms, int want_e,
+                          double *part, int *grid_out, cudaStream_t st, int kmax) {
+    if (g.K > kmax) return fail(DESV_EINVAL, "pauli pass: tile_bits too large for this precision");
+    switch (g.K) {
+        case 1: return pauli_k<T, 1, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 2: return pauli_k<T, 2, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 3: return pauli_k<T, 3, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 4: return pauli_k<T, 4, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 5: return pauli_k<T, 5, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 6: return pauli_k<T, 6, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 7: return pauli_k<T, 7, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 8: return pauli_k<T, 8, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 9: return pauli_k<T, 9, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 10: return pauli_k<T, 10, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        default: return pauli_k<T, 11, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+    }
+}
+
+// Tile of up to 2^11 amplitudes for complex64 and 2^10 for complex128 (16 KB).
+int pauli_pass(const void *psi, void *out, int dtype, int mode, const TileGeom &g, const desv_pauli_term *terms,
+               int nterms, int want_e, double *part, int *grid_out, cudaStream_t st) {
+    if (nterms > PAULI_MAX_TERMS) return fail(DESV_EINVAL, "pauli pass: more than 512 terms in one pass");
+    if (g.K < 5 && g.K != g.n) return fail(DESV_EINVAL, "pauli pass: tile smaller than 2^5 must cover the state");
+    if (dtype == DESV_C64) {
+        const float2 *p = static_cast<const float2 *>(psi);
+        float2 *o = static_cast<float2 *>(out);
+        if (mode == 0) return pauli_dispatch<float2, 0>(p, o, g, terms, nterms, want_e, part, grid_out, st, 11);
+        if (mode == 1) return pauli_dispatch<float2, 1>(p, o, g, terms, nterms, want_e, part, grid_out, st, 11);
+        return pauli_dispatch<float2, 2>(p, o, g, terms, nterms, want_e, part, grid_out, st, 11);
+    }
+    const double2 *p = static_cast<const double2 *>(psi);
+    double2 *o = static_cast<double2 *>(out);
+    if (mode == 0) return pauli_dispatch<double2, 0>(p, o, g, terms, nterms, want_e, part, grid_out, st, 10);
+    if (mode == 1) return pauli_dispatch<double2, 1>(p, o, g, terms, nterms, want_e, part, grid_out, st, 10);
+    return pauli_dispatch<double2, 2>(p, o, g, terms, nterms, want_e, part, grid_out, st, 10);
+}
+
+}  // namespace desv

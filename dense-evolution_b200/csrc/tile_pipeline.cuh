@@ -1,0 +1,166 @@
+// Tile geometry and the persistent bulk-copy pipeline shared by the fused
+// gate kernel, the Pauli kernels and the adjoint kernel.
+//
+// A tile is 2^K amplitudes: the L lowest index bits (contiguous runs of 2^L
+// amplitudes in HBM) plus K-L arbitrary higher bits `high[]`.  In shared
+// memory a tile is stored densely by its tile-local index j: bits 0..L-1 of j
+// are index bits 0..L-1, bit L+i of j is index bit high[i].  Tiles are
+// enumerated by the remaining n-K index bits `rest[]` (ascending), so
+// consecutive tile ids are neighbours in memory.
+//
+// Each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... through a ring
+// of NBUF shared-memory slots.  Warp 0 issues one cp.async.bulk per 2^L-run
+// (loads complete on the slot's mbarrier, stores go into per-lane bulk
+// groups), every thread runs the body on the slot in shared memory.  Loads
+// run D = NBUF-2 tiles ahead when the body's results are stored (one slot is
+// still draining its store), NBUF-1 tiles ahead otherwise.
+#pragma once
+
+#include "desv_common.cuh"
+
+namespace desv {
+
+struct TileGeom {
+    int n, K, L, nrest;
+    uint8_t high[16];
+    uint8_t rest[40];
+};
+
+__device__ __forceinline__ uint64_t tile_local_to_global(const TileGeom &g, uint32_t j) {
+    uint64_t x = j & ((1u << g.L) - 1u);
+    const int nh = g.K - g.L;
+#pragma unroll 1
+    for (int i = 0; i < nh; ++i)
+        if ((j >> (g.L + i)) & 1u) x |= 1ull << g.high[i];
+    return x;
+}
+
+__device__ __forceinline__ uint64_t tile_base(const TileGeom &g, uint64_t t) {
+    uint64_t b = 0;
+#pragma unroll 1
+    for (int i = 0; i < g.nrest; ++i)
+        if ((t >> i) & 1ull) b |= 1ull << g.rest[i];
+    return b;
+}
+
+__device__ __forceinline__ uint64_t chunk_offset(const TileGeom &g, uint32_t c) {
+    uint64_t o = 0;
+    const int nh = g.K - g.L;
+#pragma unroll 1
+    for (int i = 0; i < nh; ++i)
+        if ((c >> i) & 1u) o |= 1ull << g.high[i];
+    return o;
+}
+
+// Arrays taking part in a pipelined sweep.  Array 0 is always loaded.
+template <typename T, int NARR> struct PipeArrays {
+    T *ptr[NARR];
+    bool load[NARR];
+    bool store[NARR];
+};
+
+// Run `body(smem_slot_arrays, tile_base, tile_id)` over every tile.  Returns
+// false (after draining in-flight copies) if a bounded wait gave up.
+template <typename T, int K, int NBUF, int NARR, class Body>
+__device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body &body, unsigned char *smem) {
+    constexpr uint32_t TILE = 1u << K;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    T *bufs = reinterpret_cast<T *>(smem + 128);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t ntiles = 1u << (g.n - K);
+    const uint32_t cnt = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const uint32_t chunk = 1u << g.L, nchunks = 1u << (K - g.L);
+    const uint32_t chunk_bytes = chunk * sizeof(T);
+
+    bool any_store = false;
+    uint32_t load_bytes = 0;
+#pragma unroll
+    for (int a = 0; a < NARR; ++a) {
+        any_store |= A.store[a];
+        if (A.load[a]) load_bytes += TILE * sizeof(T);
+    }
+    const uint32_t D = any_store ? (NBUF - 2) : (NBUF - 1);
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NBUF; ++b) mbar_init(&full[b], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    auto slot_ptr = [&](uint32_t slot, int a) { return bufs + (size_t)(slot * NARR + a) * TILE; };
+    auto issue_load = [&](uint32_t i) {
+        const uint32_t slot = i % NBUF;
+        const uint64_t base = tile_base(g, blockIdx.x + (uint64_t)i * gridDim.x);
+        if (lane == 0) mbar_arrive_expect_tx(&full[slot], load_bytes);
+        __syncwarp();
+        for (uint32_t c = lane; c < nchunks; c += 32) {
+            const uint64_t off = base + chunk_offset(g, c);
+#pragma unroll
+            for (int a = 0; a < NARR; ++a)
+                if (A.load[a]) bulk_g2s(slot_ptr(slot, a) + (size_t)c * chunk, A.ptr[a] + off, chunk_bytes, &full[slot]);
+        }
+    };
+
+    if (warp == 0)
+        for (uint32_t i = 0; i < D && i < cnt; ++i) issue_load(i);
+
+    bool ok = true;
+    uint32_t i = 0;
+    for (; i < cnt; ++i) {
+        const uint32_t slot = i % NBUF;
+        if (warp == 0 && i + D < cnt) {
+            if (any_store) bulk_wait_read<1>();
+            __syncwarp();
+            issue_load(i + D);
+        }
+        const bool waited = mbar_wait_bounded(&full[slot], (i / NBUF) & 1u);
+        if (!__syncthreads_and(waited)) { ok = false; break; }
+        T *sp[NARR];
+#pragma unroll
+        for (int a = 0; a < NARR; ++a) sp[a] = slot_ptr(slot, a);
+        const uint64_t tid = blockIdx.x + (uint64_t)i * gridDim.x;
+        const uint64_t base = tile_base(g, tid);
+        body(sp, base, tid);
+        if (any_store) {
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (warp == 0) {
+                for (uint32_t c = lane; c < nchunks; c += 32) {
+                    const uint64_t off = base + chunk_offset(g, c);
+#pragma unroll
+                    for (int a = 0; a < NARR; ++a)
+                        if (A.store[a]) bulk_s2g(A.ptr[a] + off, sp[a] + (size_t)c * chunk, chunk_bytes);
+                }
+                bulk_commit();
+            }
+        } else {
+            __syncthreads();
+        }
+    }
+    if (!ok && warp == 0) {
+        // drain loads still in flight (bounded) so no copy targets freed shared memory
+        for (uint32_t j = i; j < cnt && j < i + D + 1; ++j) mbar_wait_bounded(&full[j % NBUF], (j / NBUF) & 1u, 1u << 16);
+    }
+    if (warp == 0 && any_store) bulk_wait_all();
+    return ok;
+}
+
+// host-side geometry builder
+inline bool make_geom(TileGeom &g, int n, int K, int L, const uint8_t *high) {
+    if (K > n || L < 1 || L > K || n > 34) return false;
+    g.n = n; g.K = K; g.L = L;
+    uint64_t tmask = (1ull << L) - 1ull;
+    for (int i = 0; i < K - L; ++i) {
+        if (high[i] < L || high[i] >= n) return false;
+        if (i && high[i] <= high[i - 1]) return false;
+        g.high[i] = high[i];
+        tmask |= 1ull << high[i];
+    }
+    int r = 0;
+    for (int b = 0; b < n; ++b)
+        if (!((tmask >> b) & 1ull)) g.rest[r++] = (uint8_t)b;
+    g.nrest = r;
+    return r == n - K;
+}
+
+}  // namespace desv

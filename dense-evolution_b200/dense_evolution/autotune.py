@@ -1,0 +1,91 @@
+"""Tile-size autotuner for the fused passes.
+
+A fused pass's tile is 2^K amplitudes (K register+lane bits).  Larger tiles
+fit more gates per HBM round trip but hold fewer pipeline slots per SM.  The
+tuner times each supported K on a synthetic brick-wall layer at the requested
+qubit count and stores the winner per (GPU name, qubits, precision) in a JSON
+cache (``$DESV_TUNE_CACHE`` or ``~/.cache/desv_tune.json``).  Without a cached
+entry the defaults below apply; ``DESV_TILE_BITS`` overrides both.
+"""
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+import torch
+
+_lock = threading.Lock()
+_cache = None
+SUPPORTED = {torch.complex64: (9, 10, 11, 12, 13), torch.complex128: (9, 10, 11, 12)}
+DEFAULT = {torch.complex64: 12, torch.complex128: 11}
+
+
+def _path() -> str:
+    return os.environ.get('DESV_TUNE_CACHE', os.path.join(os.path.expanduser('~'), '.cache', 'desv_tune.json'))
+
+
+def _load():
+    global _cache
+    if _cache is None:
+        try:
+            with open(_path()) as f:
+                _cache = json.load(f)
+        except (OSError, ValueError):
+            _cache = {}
+    return _cache
+
+
+def _key(n, dtype):
+    name = torch.cuda.get_device_name() if torch.cuda.is_available() else 'cpu'
+    return f'{name}|{n}|{"c64" if dtype == torch.complex64 else "c128"}'
+
+
+def tile_bits(n: int, dtype: torch.dtype) -> int:
+    env = os.environ.get('DESV_TILE_BITS')
+    if env:
+        return min(int(env), n)
+    with _lock:
+        c = _load()
+        k = c.get(_key(n, dtype)) if torch.cuda.is_available() else None
+    return min(int(k) if k else DEFAULT[dtype], n)
+
+
+def record(n: int, dtype: torch.dtype, k: int):
+    with _lock:
+        c = _load()
+        c[_key(n, dtype)] = int(k)
+        try:
+            os.makedirs(os.path.dirname(_path()), exist_ok=True)
+            with open(_path(), 'w') as f:
+                json.dump(c, f, indent=1)
+        except OSError:
+            pass
+
+
+def tune(n: int, dtype: torch.dtype, layers: int = 4, reps: int = 3, seed: int = 0) -> dict:
+    """Time every supported tile size on a random U3 + brick-CZ circuit of `layers`
+    layers at n qubits; record and return {K: ms per pass}."""
+    import numpy as np
+    from .circuits.compiler import CompiledCircuit, QuantumTranspiler
+    from .workloads import brick_u3_circuit
+    circ = QuantumTranspiler.transpile(brick_u3_circuit(n, layers, seed))
+    sv = torch.zeros(1 << n, dtype=dtype, device='cuda')
+    sv[0] = 1
+    res = {}
+    for k in SUPPORTED[dtype]:
+        if k > n:
+            continue
+        plan = CompiledCircuit(circ, n, dtype, tile_bits=k)
+        plan.run(sv)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            plan.run(sv)
+        e1.record()
+        torch.cuda.synchronize()
+        res[k] = e0.elapsed_time(e1) / reps
+    best = min(res, key=res.get)
+    record(n, dtype, best)
+    return res

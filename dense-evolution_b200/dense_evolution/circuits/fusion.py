@@ -1,0 +1,549 @@
+"""Fusion pass: transpiled gate tuples -> fused tile passes for libdesv.
+
+The reference compiler has no fusion: every gate row of
+``circuits/compiler.py:318-355`` is one full read + gather + write of the
+state.  This pass rewrites a transpiled circuit into a handful of HBM passes:
+
+1. **Lowering.**  Every gate becomes an IR gate on index bits (qubit q is bit
+   n-1-q, MSB-first): a 2x2 matrix on a target bit with optional control
+   bits (h, rx, cx, cy, ...), a diagonal on two bits (cz, cp, crz), a dense
+   4x4 on two bits (untranspiled swap/iswap/ecr) or a global scalar (gphase).
+2. **1-qubit fusion.**  Runs of uncontrolled 1-qubit gates on one bit are
+   multiplied into one 2x2 in FP64 (U3 -> Rz.Ry.Rz.GPhase collapses back into
+   one matrix).  Diagonal / anti-diagonal / real / phase-only matrices are
+   flagged so the kernel uses the cheaper update.
+3. **Pass scheduling.**  A pass owns a tile of 2^K amplitudes: the L low index
+   bits plus K-L chosen high bits.  Gates are taken greedily in circuit order
+   while their NON-DIAGONAL bits fit the tile; diagonal actions (cz, cp, crz,
+   controls) never need their bits in the tile.  A gate that cannot run is
+   deferred and blocks later gates that do not commute with it (gates commute
+   when every shared bit is acted on diagonally by both).
+4. **Stage scheduling.**  Inside a pass each register stage owns 4 tile bits
+   (>= 5); tile bits 0..4 are warp lanes and are available in every stage.
+   The same greedy rule assigns the pass's ops to stages.
+
+The output is packed into the ``desv_pass`` / ``desv_op`` structs of
+``include/desv.h`` plus a pool of complex matrices.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .. import _native as N
+from .gates import GATES, PARAMETRIC_GATES
+
+LANE_BITS = 5
+REG_SLOTS = 4
+MIN_FUSED_QUBITS = 9  # 5 lane bits + 4 register bits
+
+_STATIC_1Q = ('h', 'x', 'y', 'z', 's', 'sdg', 't', 'tdg', 'sx')
+_PARAM_1Q = ('rx', 'ry', 'rz', 'p', 'u1', 'phase', 'gphase')
+# generator G with dU/dtheta = G U for the differentiable gates (adjoint method)
+GENERATOR = {'rx': 'x', 'ry': 'y', 'rz': 'z', 'p': 'p1', 'u1': 'p1', 'phase': 'p1', 'cp': 'cp', 'cphase': 'cp',
+             'crz': 'crz'}
+
+
+def _unknown(name):
+    return ValueError(
+        f"unknown gate '{name}' -- not in GATES or PARAMETRIC_GATES. A typo in a gate name used to be "
+        f"silently dropped from the circuit instead of raising (issue #4).")
+
+
+@dataclass
+class IRGate:
+    """One gate on index bits.  kind: 'm1' | 'd2' | 'm2' | 'scalar'."""
+    kind: str
+    name: str
+    t: int = -1              # m1 target bit; d2 / m2: bit a (LOW bit of the matrix index)
+    t2: int = -1             # d2 / m2: bit b (HIGH bit of the matrix index)
+    cbits: Tuple[int, ...] = ()
+    cvals: Tuple[int, ...] = ()
+    value: float = 0.0       # parameter value
+    slot: int = -1           # theta slot (energy functions), -1 = constant
+    const: Optional[np.ndarray] = None  # matrix of non-parametric gates
+
+    def matrix(self, theta=None) -> np.ndarray:
+        v = self.value if (self.slot < 0 or theta is None) else float(theta[self.slot])
+        if self.const is not None:
+            return self.const
+        return gate_matrix_of(self.kind, self.name, v)
+
+
+def _is_diag(m: np.ndarray) -> bool:
+    return m.shape == (2, 2) and m[0, 1] == 0 and m[1, 0] == 0
+
+
+def gate_matrix_of(kind: str, name: str, v: float) -> np.ndarray:
+    """FP64 matrix of a parametric IR gate (m1: 2x2; d2: 4 diagonal factors)."""
+    if kind == 'm1':
+        if name in ('p', 'u1', 'phase'):
+            return PARAMETRIC_GATES['p'](v)
+        if name == 'gphase':
+            return PARAMETRIC_GATES['gphase'](v)
+        return PARAMETRIC_GATES[name](v)
+    if kind == 'd2':
+        if name in ('cp', 'cphase'):
+            return np.array([1, 1, 1, np.exp(1j * v)], dtype=np.complex128)
+        if name == 'crz':  # factor index: bit(control) + 2 * bit(target)
+            return np.array([1, np.exp(-0.5j * v), 1, np.exp(0.5j * v)], dtype=np.complex128)
+    if kind == 'scalar':
+        return np.full(4, np.exp(1j * v), dtype=np.complex128)
+    raise ValueError(f'no parametric matrix for {kind} {name}')
+
+
+def lower(target: Sequence[tuple], n: int, slots: Optional[Sequence[int]] = None) -> List[IRGate]:
+    """Transpiled gate tuples -> IR gates.  `slots[i]` (optional) is the theta
+    slot of gate i (energy functions) or -1."""
+    out: List[IRGate] = []
+    for gi, cmd in enumerate(target):
+        name = (cmd[0] if isinstance(cmd[0], str) else str(cmd[0])).lower()
+        a = cmd[1:]
+        slot = -1 if slots is None else int(slots[gi])
+
+        def qbit(q, what='gate'):
+            qi = int(q)
+            if not 0 <= qi < n:
+                raise ValueError(f"Qubit index {qi} out of range [0, {n}) in {what} '{name}'")
+            return n - 1 - qi
+
+        def two(with_param: bool):
+            if len(a) < 2:
+                raise ValueError(f"gate '{name}' needs two qubits")
+            c, t = qbit(a[0]), qbit(a[1])
+            if c == t:
+                raise ValueError('Control and target qubits must differ')
+            p = float(a[2]) if with_param and len(a) > 2 else 0.0
+            return c, t, p
+
+        if name == 'id':
+            if a:
+                qbit(a[0])
+            continue
+        if name in _STATIC_1Q:
+            if not a:
+                raise ValueError(f"gate '{name}' needs a qubit")
+            out.append(IRGate('m1', name, t=qbit(a[0]), const=GATES[name]))
+        elif name in _PARAM_1Q:
+            if not a:
+                raise ValueError(f"gate '{name}' needs a qubit")
+            t = qbit(a[0])
+            p = float(a[1]) if len(a) > 1 else 0.0
+            if name == 'gphase':
+                out.append(IRGate('scalar', name, value=p, slot=slot))
+            else:
+                out.append(IRGate('m1', name, t=t, value=p, slot=slot))
+        elif name in ('u3', 'u2'):
+            need = 4 if name == 'u3' else 3
+            if len(a) < need:
+                raise ValueError(f"gate '{name}' needs {need - 1} parameters")
+            t = qbit(a[0])
+            out.append(IRGate('m1', name, t=t, const=PARAMETRIC_GATES[name](*[float(x) for x in a[1:need]])))
+        elif name in ('cx', 'cy'):
+            c, t, _ = two(False)
+            out.append(IRGate('m1', name, t=t, cbits=(c,), cvals=(1,), const=GATES[name[1]]))
+        elif name == 'cz':
+            c, t, _ = two(False)
+            out.append(IRGate('d2', name, t=c, t2=t, const=np.array([1, 1, 1, -1], dtype=np.complex128)))
+        elif name in ('cp', 'cphase', 'crz'):
+            c, t, p = two(True)
+            out.append(IRGate('d2', name, t=c, t2=t, value=p, slot=slot))
+        elif name in ('swap', 'iswap', 'ecr'):
+            # exact CX decompositions (same as the transpiler's): keeps every gate of
+            # a fused pass a 2x2 / diagonal, whichever bits it touches
+            q1, q2 = int(a[0]), int(a[1])
+            two(False)
+            if name == 'swap':
+                sub = [('cx', q1, q2), ('cx', q2, q1), ('cx', q1, q2)]
+            elif name == 'iswap':
+                sub = [('s', q1), ('h', q1), ('s', q2), ('cx', q1, q2), ('cx', q2, q1), ('h', q2)]
+            else:
+                sub = [('s', q1), ('sx', q2), ('cx', q1, q2), ('x', q1), ('gphase', q1, -np.pi / 4.0)]
+            out.extend(lower(sub, n))
+        else:
+            raise _unknown(cmd[0])
+    return out
+
+
+# ---------------------------------------------------------------------------
+# fused ops
+# ---------------------------------------------------------------------------
+
+@dataclass
+class FOp:
+    kind: str                       # 'm1' | 'd2' | 'm2' | 'scalar'
+    t: int = -1
+    t2: int = -1
+    cbits: Tuple[int, ...] = ()
+    cvals: Tuple[int, ...] = ()
+    src: List[IRGate] = field(default_factory=list)
+    nd: int = 0
+    d: int = 0
+
+    def matrix(self, theta=None) -> np.ndarray:
+        if self.kind == 'm1':
+            m = np.eye(2, dtype=np.complex128)
+            for g in self.src:
+                if g.kind == 'scalar':
+                    m = np.exp(1j * (g.value if g.slot < 0 or theta is None else float(theta[g.slot]))) * m
+                else:
+                    m = g.matrix(theta) @ m
+            return m
+        if self.kind in ('d2', 'scalar'):
+            v = np.ones(4, dtype=np.complex128)
+            for g in self.src:
+                v = v * g.matrix(theta)
+            return v
+        return self.src[0].matrix(theta)
+
+
+def fuse_1q(gates: Sequence[IRGate], merge: bool = True) -> List[FOp]:
+    """Merge runs of uncontrolled 1-qubit gates per bit (and global scalars into
+    the next 1-qubit run) into single 2x2 ops; keep everything else in order."""
+    out: List[FOp] = []
+    pending = {}        # bit -> FOp under construction (not yet in `out`)
+    scal: List[IRGate] = []
+
+    def flush(bits_mask: int):
+        for b in [b for b in pending if (bits_mask >> b) & 1]:
+            out.append(pending.pop(b))
+
+    for g in gates:
+        if g.kind == 'scalar':
+            if merge and pending:
+                next(iter(pending.values())).src.append(g)
+            else:
+                scal.append(g)
+            continue
+        if g.kind == 'm1' and not g.cbits and merge:
+            op = pending.get(g.t)
+            if op is None:
+                op = FOp('m1', t=g.t)
+                pending[g.t] = op
+            op.src.append(g)
+            continue
+        touched = 0
+        for b in (g.t, g.t2, *g.cbits):
+            if b >= 0:
+                touched |= 1 << b
+        flush(touched)
+        out.append(FOp(g.kind, t=g.t, t2=g.t2, cbits=g.cbits, cvals=g.cvals, src=[g]))
+    flush(~0)
+    for s in scal:
+        out.append(FOp('scalar', src=[s]))
+    for op in out:
+        _classify(op)
+    return out
+
+
+def _classify(op: FOp):
+    """Bits acted on non-diagonally (`nd`) and diagonally (`d`)."""
+    nd = d = 0
+    for b in op.cbits:
+        d |= 1 << b
+    if op.kind == 'm1':
+        diag = all(g.kind == 'scalar' or (g.const is not None and _is_diag(g.const)) or
+                   (g.const is None and g.name in ('rz', 'p', 'u1', 'phase')) for g in op.src)
+        if diag:
+            d |= 1 << op.t
+        else:
+            nd |= 1 << op.t
+    elif op.kind == 'd2':
+        d |= (1 << op.t) | (1 << op.t2)
+    elif op.kind == 'm2':
+        nd |= (1 << op.t) | (1 << op.t2)
+    op.nd, op.d = nd, d
+
+
+# ---------------------------------------------------------------------------
+# scheduling
+# ---------------------------------------------------------------------------
+
+def _bits(mask: int):
+    b = 0
+    while mask:
+        if mask & 1:
+            yield b
+        mask >>= 1
+        b += 1
+
+
+def _greedy(ids: Sequence[int], ops: Sequence[FOp], fits) -> Tuple[List[int], List[int]]:
+    """Take ops in order while `fits(op)` (which may grow the resource set);
+    a deferred op blocks every later op that does not commute with it."""
+    taken, deferred = [], []
+    b_any = b_nd = 0
+    for i in ids:
+        op = ops[i]
+        if ((op.nd | op.d) & b_any) or (op.nd & b_nd) or not fits(op):
+            deferred.append(i)
+            b_any |= op.nd
+            b_nd |= op.d
+        else:
+            taken.append(i)
+    return taken, deferred
+
+
+@dataclass
+class PassSpec:
+    K: int
+    L: int
+    high: List[int]
+    stages: List[Tuple[List[int], List[int]]]   # (register tile-local bits[4], op ids)
+
+
+def schedule(ops: Sequence[FOp], n: int, kmax: int) -> List[PassSpec]:
+    K = min(kmax, n)
+    remaining = list(range(len(ops)))
+    passes: List[PassSpec] = []
+    while remaining:
+        H = set()
+
+        def fits_pass(op):
+            need = {b for b in _bits(op.nd) if b >= LANE_BITS} - H
+            if len(H) + len(need) > K - LANE_BITS:
+                return False
+            H.update(need)
+            return True
+
+        taken, remaining = _greedy(remaining, ops, fits_pass)
+        if not taken:
+            raise RuntimeError('fusion: no schedulable gate (internal error)')
+        # widen the low contiguous run while the tile has spare bits
+        L = LANE_BITS
+        while True:
+            high = sorted(h for h in H if h >= L)
+            L2 = K - len(high)
+            if L2 == L:
+                break
+            L = L2
+        high = sorted(h for h in H if h >= L)
+        assert len(high) == K - L
+        tl = {b: b for b in range(L)}
+        for i, h in enumerate(high):
+            tl[h] = L + i
+        passes.append(PassSpec(K, L, high, _stages(taken, ops, tl, K)))
+    return passes
+
+
+def _stages(ids: List[int], ops: Sequence[FOp], tl: dict, K: int):
+    stages = []
+    remaining = list(ids)
+    while remaining:
+        G: List[int] = []
+
+        def fits_stage(op):
+            need = []
+            for b in _bits(op.nd):
+                p = tl[b]
+                if op.kind == 'm2' and p < LANE_BITS:
+                    return False          # a dense 4x4 needs both bits in registers
+                if p >= LANE_BITS and p not in G and p not in need:
+                    need.append(p)
+            if op.kind in ('m1', 'g1'):
+                creg = [tl[c] for c in op.cbits if c in tl and tl[c] >= LANE_BITS and (tl[c] in G or tl[c] in need)]
+                if len(creg) > 1:
+                    return False
+            if len(G) + len(need) > REG_SLOTS:
+                return False
+            G.extend(need)
+            return True
+
+        taken, remaining = _greedy(remaining, ops, fits_stage)
+        if not taken:
+            raise RuntimeError('fusion: no schedulable op in a stage (internal error)')
+        g = sorted(G)
+        for p in range(LANE_BITS, K):
+            if len(g) == REG_SLOTS:
+                break
+            if p not in g:
+                g.append(p)
+        stages.append((sorted(g), taken))
+    return stages
+
+
+# ---------------------------------------------------------------------------
+# packing
+# ---------------------------------------------------------------------------
+
+def _m1_flags(m: np.ndarray) -> int:
+    f = 0
+    if m[0, 1] == 0 and m[1, 0] == 0:
+        f |= N.F_DIAG
+        if m[0, 0] == 1:
+            f |= N.F_PHASE1
+    elif m[0, 0] == 0 and m[1, 1] == 0:
+        f |= N.F_ANTI
+    if not np.any(m.imag):
+        f |= N.F_REAL
+    return f
+
+
+def _clean(m: np.ndarray) -> np.ndarray:
+    m = np.array(m, dtype=np.complex128)
+    scale = max(1.0, float(np.abs(m).max()))
+    re, im = m.real.copy(), m.imag.copy()
+    re[np.abs(re) < 1e-15 * scale] = 0.0
+    im[np.abs(im) < 1e-15 * scale] = 0.0
+    return re + 1j * im
+
+
+class Packed:
+    """Packed pass/op/matrix arrays (host) for one fused circuit."""
+
+    def __init__(self, n: int, ops: List[FOp], passes: List[PassSpec], adjoint: bool = False):
+        self.n = n
+        self.fops = ops
+        self.specs = passes
+        self.adjoint = adjoint
+        recs, pass_rows, self.op_slots = [], [], []   # op_slots: (record index, fop index)
+        self.m2_swap = {}
+        self.diag1 = {}        # record index -> control value on gb (None: no gb control) for 1-bit diagonals
+        self.param_map: List[int] = []                # adjoint: local gradient slot -> theta index
+        for ps in passes:
+            begin = len(recs)
+            map_begin = len(self.param_map)
+            local = {}
+            tl = {b: b for b in range(ps.L)}
+            for i, h in enumerate(ps.high):
+                tl[h] = ps.L + i
+            for g, ids in ps.stages:
+                rec = np.zeros((), dtype=N.OP_DTYPE)
+                rec['kind'] = N.OP_STAGE
+                rec['g'] = g
+                rec['mat'] = len(ids)
+                rec['param'] = -1
+                recs.append(rec)
+                slot_of = {p: s for s, p in enumerate(g)}
+                for i in ids:
+                    self._pending_diag1 = 'none'
+                    rec = self._op_record(ops[i], tl, slot_of)
+                    if self._pending_diag1 != 'none':
+                        self.diag1[len(recs)] = self._pending_diag1
+                    if ops[i].kind in ('g1', 'gd'):
+                        th = ops[i].src[0].slot
+                        if th not in local:
+                            local[th] = len(local)
+                            self.param_map.append(th)
+                        rec['param'] = local[th]
+                    recs.append(rec)
+                    self.op_slots.append((len(recs) - 1, i))
+                    if ops[i].kind == 'm2':
+                        self.m2_swap[len(recs) - 1] = slot_of[tl[ops[i].t]] > slot_of[tl[ops[i].t2]]
+            end = len(recs)
+            row = np.zeros((), dtype=N.ADJ_PASS_DTYPE if adjoint else N.PASS_DTYPE)
+            row['tile_bits'], row['low_bits'], row['op_begin'], row['op_end'] = ps.K, ps.L, begin, end
+            h = np.zeros(16, np.uint8)
+            h[:len(ps.high)] = ps.high
+            row['high'] = h
+            if adjoint:
+                row['nparams'], row['map_begin'] = len(local), map_begin
+            pass_rows.append(row)
+        pdt = N.ADJ_PASS_DTYPE if adjoint else N.PASS_DTYPE
+        self.ops = np.array(recs, dtype=N.OP_DTYPE) if recs else np.zeros(0, N.OP_DTYPE)
+        self.passes = np.array(pass_rows, dtype=pdt) if pass_rows else np.zeros(0, pdt)
+        self.nstages = sum(len(p.stages) for p in passes)
+        self.max_params = max([int(r['nparams']) for r in pass_rows], default=0) if adjoint else 0
+
+    def _op_record(self, op: FOp, tl: dict, slot_of: dict):
+        rec = np.zeros((), dtype=N.OP_DTYPE)
+        rec['param'] = -1
+        rec['cslot'] = -1
+        rec['ga'] = rec['gb'] = 0xFF
+        rec['sa'] = rec['sb'] = -1
+        cmask = cval = 0
+        if op.kind in ('m1', 'g1') and not (op.nd >> op.t) & 1:
+            # diagonal on its target: a DIAG record over (target, first control), so the
+            # target needs no register slot or lane
+            rec['kind'] = N.OP_DIAG if op.kind == 'm1' else N.OP_GRAD
+            rec['s1'] = 1 if op.kind == 'g1' else 0
+            ctl = None
+            rec['ga'] = op.t
+            if op.t in tl and tl[op.t] in slot_of:
+                rec['sa'] = slot_of[tl[op.t]]
+            for i, (c, v) in enumerate(zip(op.cbits, op.cvals)):
+                if i == 0:
+                    rec['gb'] = c
+                    if c in tl and tl[c] in slot_of:
+                        rec['sb'] = slot_of[tl[c]]
+                    ctl = v
+                else:
+                    cmask |= 1 << c
+                    cval |= v << c
+            self._pending_diag1 = ctl
+        elif op.kind in ('m1', 'g1'):
+            rec['kind'] = N.OP_M1 if op.kind == 'm1' else N.OP_GRAD
+            rec['s1'] = 0
+            p = tl[op.t]
+            rec['s0'] = slot_of[p] if p >= LANE_BITS else 16 + p
+            for c, v in zip(op.cbits, op.cvals):
+                if c in tl and tl[c] in slot_of:
+                    rec['cslot'] = slot_of[tl[c]]
+                else:
+                    cmask |= 1 << c
+                    cval |= v << c
+        elif op.kind in ('d2', 'scalar', 'gd'):
+            rec['kind'] = N.OP_DIAG if op.kind != 'gd' else N.OP_GRAD
+            rec['s1'] = 1 if op.kind == 'gd' else 0
+            for key, skey, b in (('ga', 'sa', op.t), ('gb', 'sb', op.t2)):
+                if b >= 0:
+                    rec[key] = b
+                    if b in tl and tl[b] in slot_of:
+                        rec[skey] = slot_of[tl[b]]
+        elif op.kind == 'm2':
+            rec['kind'] = N.OP_M2
+            sa, sb = slot_of[tl[op.t]], slot_of[tl[op.t2]]
+            rec['s0'], rec['s1'] = min(sa, sb), max(sa, sb)
+        rec['cmask'], rec['cval'] = cmask, cval
+        return rec
+
+    def materialize(self, theta=None, dtype=np.complex64):
+        """Matrix pool and per-op flags for the given parameters."""
+        pool = []
+        ops = self.ops
+        for rec_i, fi in self.op_slots:
+            op = self.fops[fi]
+            m = _clean(op.matrix(theta))
+            ops[rec_i]['mat'] = sum(len(x) for x in pool)
+            if rec_i in self.diag1:
+                # 1-bit diagonal as a table over (target, control): off-control rows are the
+                # identity for gates and zero for generators
+                ctl = self.diag1[rec_i]
+                d = np.array([m[0, 0], m[1, 1]], dtype=np.complex128)
+                off = np.zeros(2) if op.kind == 'g1' else np.ones(2)
+                if ctl is None:
+                    tab = np.concatenate([d, d])
+                elif ctl == 1:
+                    tab = np.concatenate([off, d])
+                else:
+                    tab = np.concatenate([d, off])
+                if op.kind == 'm1':
+                    ops[rec_i]['flags'] = N.F_SIGN if (not np.any(tab.imag) and np.all(np.abs(tab.real) == 1)) else 0
+                pool.append(tab.astype(np.complex128))
+            elif op.kind == 'm1':
+                ops[rec_i]['flags'] = _m1_flags(m)
+                pool.append(m.reshape(-1))
+            elif op.kind in ('g1', 'gd'):
+                pool.append(m.reshape(-1))
+            elif op.kind in ('d2', 'scalar'):
+                ops[rec_i]['flags'] = N.F_SIGN if (not np.any(m.imag) and np.all(np.abs(m.real) == 1)) else 0
+                pool.append(m.reshape(-1))
+            else:
+                # kernel row index = 2*bit(s1) + bit(s0); m is indexed 2*bit(t2) + bit(t)
+                if self.m2_swap[rec_i]:
+                    perm = [0, 2, 1, 3]
+                    m = m[np.ix_(perm, perm)]
+                pool.append(m.reshape(-1))
+        mats = np.concatenate(pool).astype(dtype) if pool else np.zeros(4, dtype=dtype)
+        return mats
+
+
+def build(target: Sequence[tuple], n: int, kmax: int, slots=None, merge_1q: bool = True):
+    """Lower + fuse + schedule + pack a transpiled circuit."""
+    ir = lower(target, n, slots)
+    fops = fuse_1q(ir, merge=merge_1q)
+    if n < MIN_FUSED_QUBITS:
+        return ir, fops, None
+    return ir, fops, Packed(n, fops, schedule(fops, n, kmax))

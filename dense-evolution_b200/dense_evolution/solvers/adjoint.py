@@ -1,0 +1,325 @@
+"""Adjoint-method gradients of E(theta) = Re<psi(theta)|H|psi(theta)>.
+
+Three device statevectors (the reference's JAX path keeps one residual per
+gate instead, ``solvers/autodiff.py:136-166``):
+
+* psi -- the forward state, returned to the caller untouched;
+* lambda -- H psi, un-applied gate by gate in reverse;
+* mu -- a working copy of psi, un-applied alongside lambda.
+
+For each parametric gate U(theta_k) = exp(theta_k G_k)-style with
+dU/dtheta = G U, dE/dtheta_k = 2 Re<lambda|G|mu> evaluated right before U is
+un-applied from mu and lambda.  On states of >= 9 qubits the reversed circuit
+(GRAD probes + inverse gates) is fused into tile passes that read and write
+mu and lambda once per pass (``desv_adjoint_passes``); smaller states walk
+gate by gate and materialise G mu in a scratch state.
+
+Generators: rx -> -i/2 X, ry -> -i/2 Y, rz -> -i/2 Z, p/u1/phase -> i|1><1|,
+cp -> i|11><11|, crz -> -i/2 |1><1| (x) Z.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from .. import _native as N
+from ..circuits import fusion
+from ..circuits.compiler import CompiledCircuit, apply_fop
+from ..physics.observables import PauliPlan, PauliSumOperator, plan_for
+
+_HALF_I = -0.5j
+_GEN_1Q = {
+    'rx': np.array([[0, _HALF_I], [_HALF_I, 0]], dtype=np.complex128),
+    'ry': np.array([[0, -0.5], [0.5, 0]], dtype=np.complex128),
+    'rz': np.array([[_HALF_I, 0], [0, 0.5j]], dtype=np.complex128),
+    'p': np.array([[0, 0], [0, 1j]], dtype=np.complex128),
+}
+_GEN_1Q['u1'] = _GEN_1Q['phase'] = _GEN_1Q['p']
+# diagonal generators over (control bit, target bit): index bit(c) + 2 bit(t)
+_GEN_D2 = {
+    'cp': np.array([0, 0, 0, 1j], dtype=np.complex128),
+    'crz': np.array([0, _HALF_I, 0, 0.5j], dtype=np.complex128),
+}
+_GEN_D2['cphase'] = _GEN_D2['cp']
+
+
+class BOp(fusion.FOp):
+    """A backward op: an inverse gate ('m1' / 'd2' / 'm2' / 'scalar') or a
+    gradient probe ('g1' 2x2 generator, 'gd' diagonal generator)."""
+
+    def matrix(self, theta=None) -> np.ndarray:
+        g = self.src[0]
+        if self.kind == 'g1':
+            return _GEN_1Q[g.name]
+        if self.kind == 'gd':
+            return _GEN_D2[g.name]
+        m = g.matrix(theta)
+        if self.kind == 'scalar':
+            v = np.exp(1j * (g.value if g.slot < 0 or theta is None else float(theta[g.slot])))
+            return np.full(4, np.conj(v), dtype=np.complex128)
+        if self.kind == 'd2':
+            return np.conj(m)
+        return np.conj(m).T
+
+
+def backward_ops(ir: List[fusion.IRGate]) -> List[BOp]:
+    ops: List[BOp] = []
+    for g in reversed(ir):
+        if g.slot >= 0 and g.kind == 'm1' and g.name in _GEN_1Q:
+            ops.append(BOp('g1', t=g.t, cbits=g.cbits, cvals=g.cvals, src=[g]))
+        elif g.slot >= 0 and g.kind == 'd2' and g.name in _GEN_D2:
+            ops.append(BOp('gd', t=g.t, t2=g.t2, src=[g]))
+        ops.append(BOp(g.kind, t=g.t, t2=g.t2, cbits=g.cbits, cvals=g.cvals, src=[g]))
+    for op in ops:
+        _classify_backward(op)
+    return ops
+
+
+def _classify_backward(op: BOp):
+    g = op.src[0]
+    nd = d = 0
+    for b in op.cbits:
+        d |= 1 << b
+    if op.kind == 'g1':
+        if g.name in ('rx', 'ry'):
+            nd |= 1 << op.t
+        else:
+            d |= 1 << op.t
+    elif op.kind in ('gd', 'd2'):
+        d |= (1 << op.t) | (1 << op.t2)
+    elif op.kind == 'm1':
+        diag = (g.const is not None and fusion._is_diag(g.const)) or (g.const is None and g.name in
+                                                                       ('rz', 'p', 'u1', 'phase'))
+        if diag:
+            d |= 1 << op.t
+        else:
+            nd |= 1 << op.t
+    elif op.kind == 'm2':
+        nd |= (1 << op.t) | (1 << op.t2)
+    op.nd, op.d = nd, d
+
+
+def _adjoint_tile_bits(n: int, dtype) -> int:
+    return min(11 if dtype == torch.complex64 else 10, n)
+
+
+class AdjointProgram:
+    """Forward + adjoint plans of one parametrised circuit at one precision."""
+
+    def __init__(self, rows, slots, n: int, dtype=torch.complex128):
+        self.n = int(n)
+        self.dtype = dtype
+        self.rows, self.slots = rows, slots
+        self.forward = CompiledCircuit(rows, self.n, dtype, slots=slots)
+        self.ir = self.forward.ir
+        self.bops = backward_ops(self.ir)
+        self.nparams = 1 + max([s for s in slots if s >= 0], default=-1)
+        if self.n >= fusion.MIN_FUSED_QUBITS:
+            kb = _adjoint_tile_bits(self.n, dtype)
+            specs = fusion.schedule(self.bops, self.n, kb)
+            specs = _split_params(specs, self.bops, 1024)
+            self.back = fusion.Packed(self.n, self.bops, specs, adjoint=True)
+        else:
+            self.back = None
+        self._back_dev = None
+        self._scratch = None
+
+    # ------------------------------------------------------------ helpers
+    def _device(self):
+        return N.require_cuda()
+
+    def initial_state(self, stato_zero=None) -> torch.Tensor:
+        dev = self._device()
+        if stato_zero is None:
+            sv = torch.empty(1 << self.n, dtype=self.dtype, device=dev)
+            N.check(N.lib().desv_init_basis(ctypes.c_void_p(sv.data_ptr()), self.n, N.dtype_code(sv), 0,
+                                            ctypes.c_void_p(N.stream_ptr())), 'init')
+            return sv
+        if isinstance(stato_zero, torch.Tensor):
+            return stato_zero.detach().to(device=dev, dtype=self.dtype).reshape(-1).clone()
+        return torch.from_numpy(np.asarray(stato_zero).astype(np.complex128).reshape(-1)).to(dev).to(self.dtype)
+
+    def forward_state(self, theta: np.ndarray, stato_zero=None) -> torch.Tensor:
+        psi = self.initial_state(stato_zero)
+        self.forward.run(psi, theta=theta)
+        return psi
+
+    def hamiltonian(self, h):
+        """('pauli', PauliPlan) or ('dense', tensor)."""
+        if isinstance(h, PauliSumOperator):
+            return 'pauli', plan_for(h.terms, self.n, h.n_qubits, self.dtype)
+        if isinstance(h, PauliPlan):
+            return 'pauli', h
+        if isinstance(h, (list, tuple)):
+            return 'pauli', plan_for(list(h), self.n, None, self.dtype)
+        t = h if isinstance(h, torch.Tensor) else torch.from_numpy(np.asarray(h))
+        return 'dense', t.to(device=self._device(), dtype=self.dtype)
+
+    def apply_h(self, h, psi: torch.Tensor, need_lambda: bool):
+        """(lambda or None, energy float)."""
+        kind, H = self.hamiltonian(h)
+        if kind == 'pauli':
+            if need_lambda:
+                lam, e = H.matvec(psi, want_expect=True)
+                return lam, float(e[0].item())
+            return None, float(H.expect(psi)[0].item())
+        lam = H @ psi
+        e = float(torch.vdot(psi.to(torch.complex128), lam.to(torch.complex128)).real.item())
+        return (lam if need_lambda else None), e
+
+    # ------------------------------------------------------------ gradient
+    def gradient(self, theta: np.ndarray, psi: torch.Tensor, lam: torch.Tensor) -> np.ndarray:
+        """dE/dtheta by the adjoint method; psi is not modified, lam is consumed."""
+        mu = psi.clone()
+        grad = torch.zeros(max(self.nparams, 1), dtype=torch.float64, device=psi.device)
+        if self.back is None:
+            self._gradient_per_gate(theta, mu, lam, grad)
+        else:
+            self._gradient_fused(theta, mu, lam, grad)
+        return grad[:self.nparams].cpu().numpy()
+
+    def _gradient_fused(self, theta, mu, lam, grad):
+        dev = mu.device
+        key = np.asarray(theta, dtype=np.float64).tobytes()
+        rdt = np.float32 if self.dtype == torch.complex64 else np.float64
+        cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
+        if self._back_dev is None or self._back_dev[0] != key:
+            mats = self.back.materialize(theta, cdt)
+            ops_t = torch.from_numpy(self.back.ops.view(np.uint8).copy()).to(dev)
+            mats_t = torch.from_numpy(mats.view(rdt).copy()).to(dev)
+            map_t = torch.tensor(self.back.param_map or [0], dtype=torch.int32, device=dev)
+            self._back_dev = (key, ops_t, mats_t, map_t)
+        _, ops_t, mats_t, map_t = self._back_dev
+        need = int(N.lib().desv_adjoint_scratch_bytes(max(self.back.max_params, 1)))
+        if self._scratch is None or self._scratch.numel() * 8 < need:
+            self._scratch = torch.empty((need + 7) // 8, dtype=torch.float64, device=dev)
+        p = self.back.passes
+        N.check(N.lib().desv_adjoint_passes(
+            ctypes.c_void_p(mu.data_ptr()), ctypes.c_void_p(lam.data_ptr()), self.n, N.dtype_code(mu),
+            ctypes.c_void_p(p.ctypes.data), len(p), ctypes.c_void_p(ops_t.data_ptr()),
+            ctypes.c_void_p(mats_t.data_ptr()), ctypes.c_void_p(map_t.data_ptr()), ctypes.c_void_p(grad.data_ptr()),
+            ctypes.c_void_p(self._scratch.data_ptr()), self._scratch.numel() * 8,
+            ctypes.c_void_p(N.stream_ptr())), 'adjoint passes')
+
+    def _gradient_per_gate(self, theta, mu, lam, grad):
+        st = ctypes.c_void_p(N.stream_ptr())
+        tmp = torch.empty_like(mu)
+        inner = torch.empty((len(self.bops), 2), dtype=torch.float64, device=mu.device)
+        sc = N.scratch(self.n, mu.device)
+        probes = []
+        for i, op in enumerate(self.bops):
+            if op.kind in ('g1', 'gd'):
+                tmp.copy_(mu)
+                m = op.matrix(theta)
+                if op.kind == 'g1':
+                    bits, full = [op.t], m
+                else:
+                    bits, full = [op.t, op.t2], np.diag(m)     # row = bit(t) + 2 bit(t2)
+                mat = np.ascontiguousarray(np.asarray(full, dtype=np.complex128).reshape(-1)).view(np.float64)
+                tb = (ctypes.c_int * len(bits))(*bits)
+                N.check(N.lib().desv_apply_gate(ctypes.c_void_p(tmp.data_ptr()), self.n, N.dtype_code(tmp),
+                                                len(bits), tb, 0, 0, ctypes.c_void_p(mat.ctypes.data), st),
+                        'apply generator')
+                row = inner[i]
+                N.check(N.lib().desv_inner(ctypes.c_void_p(lam.data_ptr()), ctypes.c_void_p(tmp.data_ptr()), self.n,
+                                           N.dtype_code(mu), ctypes.c_void_p(row.data_ptr()),
+                                           ctypes.c_void_p(sc.data_ptr()), sc.numel() * 8, st), 'inner')
+                probes.append((op.src[0].slot, i))
+            else:
+                apply_fop(mu, self.n, op, theta, st)
+                apply_fop(lam, self.n, op, theta, st)
+        if probes:
+            vals = inner[:, 0].cpu().numpy()
+            acc = np.zeros(grad.numel())
+            for s_, i in probes:
+                acc[s_] += 2.0 * vals[i]
+            grad += torch.from_numpy(acc).to(grad.device)
+
+    # ------------------------------------------------------------ public
+    def energy(self, theta, h, stato_zero=None):
+        """(E as a float64 tensor -- differentiable when theta requires grad, psi)."""
+        if isinstance(theta, torch.Tensor) and theta.requires_grad:
+            box = {}
+            e = _EnergyFunction.apply(theta, self, h, stato_zero, box)
+            return e, box['sv']
+        th = _as_theta(theta)
+        psi = self.forward_state(th, stato_zero)
+        _, e = self.apply_h(h, psi, need_lambda=False)
+        return torch.tensor(e, dtype=torch.float64), psi
+
+    def value_and_grad(self, theta, h, stato_zero=None):
+        """(E, dE/dtheta as NumPy float64, psi) without autograd bookkeeping."""
+        th = _as_theta(theta)
+        psi = self.forward_state(th, stato_zero)
+        lam, e = self.apply_h(h, psi, need_lambda=True)
+        return e, self.gradient(th, psi, lam), psi
+
+    def parameter_shift_grad(self, theta, h, stato_zero=None) -> np.ndarray:
+        """Parameter-shift gradient on the same kernels: two forward runs + <H> per
+        parameter (+-pi/2 for rx/ry/rz/p/u1/cp; four-term rule for crz)."""
+        th = _as_theta(theta)
+        kinds = {}
+        for g in self.ir:
+            if g.slot >= 0:
+                kinds[g.slot] = g.name
+
+        def f(t):
+            psi = self.forward_state(t, stato_zero)
+            return self.apply_h(h, psi, need_lambda=False)[1]
+
+        grad = np.zeros(self.nparams)
+        for k in range(self.nparams):
+            e = np.zeros(self.nparams)
+            e[k] = 1.0
+            if kinds.get(k) == 'crz':
+                c1 = (np.sqrt(2) + 1) / (4 * np.sqrt(2))
+                c2 = (np.sqrt(2) - 1) / (4 * np.sqrt(2))
+                grad[k] = c1 * (f(th + np.pi / 2 * e) - f(th - np.pi / 2 * e)) - \
+                    c2 * (f(th + 3 * np.pi / 2 * e) - f(th - 3 * np.pi / 2 * e))
+            else:
+                grad[k] = 0.5 * (f(th + np.pi / 2 * e) - f(th - np.pi / 2 * e))
+        return grad
+
+
+def _as_theta(theta) -> np.ndarray:
+    if isinstance(theta, torch.Tensor):
+        return theta.detach().cpu().numpy().astype(np.float64).reshape(-1)
+    return np.asarray(theta, dtype=np.float64).reshape(-1)
+
+
+def _split_params(specs, ops, cap):
+    """Keep every pass at <= cap distinct gradient slots (split stage lists)."""
+    out = []
+    for ps in specs:
+        cur, seen = [], set()
+        for g, ids in ps.stages:
+            slots = {ops[i].src[0].slot for i in ids if ops[i].kind in ('g1', 'gd')}
+            if cur and len(seen | slots) > cap:
+                out.append(fusion.PassSpec(ps.K, ps.L, ps.high, cur))
+                cur, seen = [], set()
+            cur.append((g, ids))
+            seen |= slots
+        out.append(fusion.PassSpec(ps.K, ps.L, ps.high, cur))
+    return out
+
+
+class _EnergyFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, theta_t, prog: AdjointProgram, h, stato_zero, box):
+        th = _as_theta(theta_t)
+        psi = prog.forward_state(th, stato_zero)
+        lam, e = prog.apply_h(h, psi, need_lambda=True)
+        box['sv'] = psi
+        ctx.prog, ctx.th, ctx.psi, ctx.lam = prog, th, psi, lam
+        ctx.tdev, ctx.tdtype = theta_t.device, theta_t.dtype
+        return torch.tensor(e, dtype=torch.float64, device=theta_t.device)
+
+    @staticmethod
+    def backward(ctx, g):
+        grad = ctx.prog.gradient(ctx.th, ctx.psi, ctx.lam)
+        gt = torch.from_numpy(grad).to(device=ctx.tdev, dtype=ctx.tdtype)
+        return g * gt, None, None, None, None

@@ -1,0 +1,185 @@
+/*
+ * desv.h -- C ABI of libdesv.so, the B200 (sm_100a) dense statevector engine.
+ *
+ * Every entry point is stream-ordered on a caller-supplied cudaStream_t
+ * (passed as void*; NULL = legacy default stream), takes device pointers the
+ * caller owns, returns an int status (DESV_OK == 0, negative on error) and
+ * never aborts.  desv_last_error() returns the message of the last failure on
+ * the calling thread.  No entry point allocates device memory: reductions
+ * take a caller-provided scratch buffer whose size desv_scratch_bytes()
+ * reports.
+ *
+ * Statevector layout: 2^n amplitudes, complex64 (float2) or complex128
+ * (double2), interleaved re/im, MSB-first qubit order -- qubit q is bit
+ * (n-1-q) of the amplitude index, as in the reference
+ * (dense_evolution/backends/statevector.py:22-33, compiler.py:186-195).
+ * All bit arguments below are INDEX BIT positions (0 = least significant);
+ * the host library translates qubit -> bit.
+ */
+#ifndef DESV_H
+#define DESV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DESV_ABI_VERSION 1
+
+/* amplitude types */
+#define DESV_C64 0
+#define DESV_C128 1
+
+/* status codes */
+#define DESV_OK 0
+#define DESV_EINVAL (-1)
+#define DESV_ENOMEM (-2)
+#define DESV_ETIMEOUT (-3)
+#define DESV_ECUDA (-4)
+#define DESV_EUNSUPPORTED (-5)
+
+/* fused-pass op kinds (desv_op.kind) */
+#define DESV_OP_STAGE 0 /* start of a register stage: g[0..3] = tile-local bit positions */
+#define DESV_OP_M1 1    /* 2x2 on register slot s0 (0..3) or lane bit (s0 = 16 + bit, bit < 5) */
+#define DESV_OP_M2 2    /* 4x4 on register slots s0 < s1; row index = 2*bit(s1) + bit(s0) */
+#define DESV_OP_DIAG 3  /* diagonal on global bits ga, gb: factor d[bit(ga) + 2*bit(gb)] */
+#define DESV_OP_GRAD 4  /* adjoint passes only: add Re<lambda|G|phi> to gradient slot `param`;
+                           s1 == 0: G = 2x2 generator on s0 (controls as M1),
+                           s1 == 1: G = diagonal over ga/gb (as DIAG) */
+
+/* desv_op.flags */
+#define DESV_F_REAL 1   /* M1: all entries real */
+#define DESV_F_DIAG 2   /* M1: off-diagonal entries zero */
+#define DESV_F_PHASE1 4 /* M1: diagonal with m00 == 1 (only |1> rows change) */
+#define DESV_F_ANTI 8   /* M1: diagonal entries zero (X, Y, controlled-X/Y) */
+#define DESV_F_SIGN 16  /* DIAG: every factor is +1 or -1 */
+#define DESV_F_PARAM 32 /* M1/DIAG (adjoint plans): this op carries gradient parameter `param` */
+
+/* One register-stage op of a fused pass (40 bytes, little-endian, packed by
+ * the host fusion pass -- dense_evolution/circuits/fusion.py). */
+typedef struct desv_op {
+    uint8_t kind;
+    uint8_t flags;
+    int8_t s0, s1;   /* M1 / M2 register slots (see kinds) */
+    int8_t cslot;    /* M1: control on register slot (-1: none) */
+    uint8_t ga, gb;  /* DIAG: global bit positions (0xFF: absent) */
+    int8_t sa, sb;   /* DIAG: register slot holding ga / gb in this stage, -1 if thread-fixed */
+    uint8_t g[4];    /* STAGE: tile-local bit positions of register slots 0..3 (ascending, >= 5) */
+    uint8_t pad0[3];
+    uint32_t mat;    /* first complex element of this op's matrix in the matrix pool */
+    int32_t param;   /* adjoint plans: gradient slot of this op (-1: none) */
+    uint64_t cmask;  /* thread-level control: apply iff (index & cmask) == cval */
+    uint64_t cval;   /* (cmask never covers this stage's register bits) */
+} desv_op;
+
+/* One fused pass: a tile of 2^tile_bits amplitudes = the low_bits contiguous
+ * index bits plus the high[] bits; all ops [op_begin, op_end) run on the tile
+ * in shared memory between one HBM read and one HBM write. */
+typedef struct desv_pass {
+    int32_t tile_bits; /* K, 9..12 (complex64) / 9..11 (complex128) */
+    int32_t low_bits;  /* L >= 5 */
+    int32_t op_begin, op_end;
+    uint8_t high[16];  /* K - L global bit positions >= L, ascending */
+} desv_pass;
+
+/* One fused pass of the adjoint backward sweep over (phi, lambda): like
+ * desv_pass, plus the gradient slots its GRAD ops use -- slot s adds into
+ * grad[map[map_begin + s]]. */
+typedef struct desv_adj_pass {
+    int32_t tile_bits, low_bits, op_begin, op_end;
+    uint8_t high[16];
+    int32_t nparams, map_begin;
+    int32_t pad[2];
+} desv_adj_pass;
+
+/* A Pauli term group of the fused Pauli kernels: all terms sharing one flip mask. */
+typedef struct desv_pauli_term {
+    uint64_t xmask; /* X|Y index bits: (P psi)[i] = psi[i ^ xmask] * ... */
+    uint64_t zmask; /* Y|Z index bits: sign (-1)^popcount((i ^ xmask) & zmask) */
+    double cre, cim; /* coefficient times i^(number of Y) */
+} desv_pauli_term;
+
+/* One tile pass of the Pauli kernels: terms [term_begin, term_end) whose flip
+ * masks lie inside the tile (low_bits contiguous bits + high[]).  tile_bits
+ * == 0 marks a direct pass for flip masks wider than any tile: partners are
+ * then read straight from global memory. */
+typedef struct desv_pauli_pass {
+    int32_t tile_bits, low_bits, term_begin, term_end;
+    uint8_t high[16];
+} desv_pauli_pass;
+
+/* ---- library ---------------------------------------------------------- */
+int desv_abi_version(void);
+int desv_last_error(char *buf, size_t len);
+/* Reads (and clears) the device-side status word that bounded waits inside
+ * kernels set instead of hanging; synchronizes `stream`. */
+int desv_device_status(void *stream);
+/* Bytes of scratch the reductions of an n-qubit state need. */
+size_t desv_scratch_bytes(int n, int dtype);
+
+/* ---- state (replaces DenseSVSimulator._reset_sv / set_initial_state,
+ *      backends/statevector.py:101-137) ------------------------------------ */
+int desv_init_basis(void *sv, int n, int dtype, uint64_t index, void *stream);
+/* sv *= (re + i im)  (normalize, statevector.py:141-147) */
+int desv_scale(void *sv, int n, int dtype, double re, double im, void *stream);
+
+/* ---- gates (replaces apply_gate_1q/_2q, apply_cx/cz/rx/ry/rz,
+ *      statevector.py:167-268, and one row of the compiled step
+ *      _apply_gate_fast_step, circuits/compiler.py:136-315) -------------- */
+/* ntargets 1 or 2; target_bits[0] is the LOW bit of the matrix index for 2
+ * targets (row = 2*bit(target_bits[1]) + bit(target_bits[0])); mat is
+ * row-major interleaved re,im doubles (8 or 32 values). */
+int desv_apply_gate(void *sv, int n, int dtype, int ntargets, const int *target_bits,
+                    uint64_t ctrl_mask, uint64_t ctrl_val, const double *mat, void *stream);
+
+/* ---- fused passes (replaces the lax.scan over gate rows,
+ *      circuits/compiler.py:318-355) ---------------------------------------- */
+/* ops_dev / mats_dev: device arrays of desv_op and complex (float2 for C64,
+ * double2 for C128); passes: HOST array. */
+int desv_apply_passes(void *sv, int n, int dtype, const desv_pass *passes, int npasses,
+                      const desv_op *ops_dev, const void *mats_dev, void *stream);
+
+/* ---- adjoint gradient (replaces jax.grad through the lax.scan of
+ *      solvers/autodiff.py:136-166) ----------------------------------------- */
+size_t desv_adjoint_scratch_bytes(int max_params_per_pass);
+/* Runs the backward passes in place on phi (circuit output, un-applied back
+ * to the input) and lambda (H psi); grad_dev[map[...]] += 2 Re<lambda|G|phi>
+ * per GRAD op (grad_dev is NOT zeroed here). */
+int desv_adjoint_passes(void *phi, void *lam, int n, int dtype, const desv_adj_pass *passes, int npasses,
+                        const desv_op *ops_dev, const void *mats_dev, const int32_t *map_dev, double *grad_dev,
+                        void *scratch, size_t scratch_bytes, void *stream);
+
+/* ---- reductions (FP64 accumulation; statevector.py:141-147,272-358,599-607,
+ *      utils/measurement.py:71-94) ------------------------------------------ */
+/* out_dev[0] = sum |a_i|^2 (double, device) */
+int desv_norm2(const void *sv, int n, int dtype, double *out_dev, void *scratch, size_t scratch_bytes,
+               void *stream);
+/* out_dev[0..1] = <a|b> (re, im) */
+int desv_inner(const void *a, const void *b, int n, int dtype, double *out_dev, void *scratch,
+               size_t scratch_bytes, void *stream);
+/* out_dev[b] = sum_i |a_i|^2 * bit_b(i) for every bit b < n, out_dev[n] = sum_i |a_i|^2 */
+int desv_bit_marginals(const void *sv, int n, int dtype, double *out_dev, void *scratch,
+                       size_t scratch_bytes, void *stream);
+/* probs_dev[i] = |a_i|^2 (double) */
+int desv_probabilities(const void *sv, int n, int dtype, double *probs_dev, void *stream);
+/* measurement collapse: zero amplitudes whose bit `bit` != outcome, scale the rest by `scale` */
+int desv_collapse(void *sv, int n, int dtype, int bit, int outcome, double scale, void *stream);
+
+/* ---- Pauli sums (replaces pauli_sum_expectation / pauli_sum_matvec,
+ *      physics/observables.py:63-186,250-308) ------------------------------- */
+/* out_dev[0..1] = sum_k <psi|c_k P_k|psi> (re, im), FP64 accumulation. */
+int desv_pauli_expect(const void *psi, int n, int dtype, const desv_pauli_pass *passes, int npasses,
+                      const desv_pauli_term *terms_dev, double *out_dev, void *scratch,
+                      size_t scratch_bytes, void *stream);
+/* out = H psi (overwrites out); if expect_dev != NULL also accumulates
+ * <psi|H psi> into expect_dev[0..1] like desv_pauli_expect. */
+int desv_pauli_matvec(const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes,
+                      int npasses, const desv_pauli_term *terms_dev, double *expect_dev, void *scratch,
+                      size_t scratch_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DESV_H */

@@ -1,0 +1,152 @@
+"""NumPy interpreter of the packed fused-pass format (include/desv.h) -- test
+infrastructure.  It executes desv_pass / desv_op records exactly as the CUDA
+kernels define them (tile = low bits + high bits, stages of 4 register bits,
+lanes = bits 0..4, controls / diagonal bits read from the global index), so
+the host fusion pass and packer can be checked against the oracle on a CPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+OP_STAGE, OP_M1, OP_M2, OP_DIAG, OP_GRAD = 0, 1, 2, 3, 4
+
+
+def _tile_index_map(n, K, L, high):
+    """global indices of every tile: array [ntiles, 2^K]"""
+    rest = [b for b in range(n) if b >= L and b not in high]
+    j = np.arange(1 << K, dtype=np.int64)
+    loc = j & ((1 << L) - 1)
+    for i, h in enumerate(high):
+        loc |= ((j >> (L + i)) & 1) << h
+    t = np.arange(1 << (n - K), dtype=np.int64)
+    base = np.zeros_like(t)
+    for i, b in enumerate(rest):
+        base |= ((t >> i) & 1) << b
+    return base[:, None] | loc[None, :]
+
+
+def _bit(idx, b):
+    return (idx >> b) & 1
+
+
+def run_passes(sv, n, passes, ops, mats, lam=None, grad=None, param_map=None):
+    """Apply passes in place to sv (and lam for adjoint passes); returns sv (, lam, grad)."""
+    sv = sv.copy()
+    lam = None if lam is None else lam.copy()
+    for ps in passes:
+        K, L = int(ps['tile_bits']), int(ps['low_bits'])
+        high = [int(h) for h in ps['high'][:K - L]]
+        gi = _tile_index_map(n, K, L, high)                 # [T, 2^K]
+        a = sv[gi]
+        b = None if lam is None else lam[gi]
+        k = int(ps['op_begin'])
+        end = int(ps['op_end'])
+        nparams = int(ps['nparams']) if 'nparams' in (ps.dtype.names or ()) else 0
+        while k < end:
+            st = ops[k]
+            assert st['kind'] == OP_STAGE
+            cnt = int(st['mat'])
+            g = [int(x) for x in st['g']]
+            assert len(set(g)) == 4 and min(g) >= 5 and max(g) < K
+            gmask = 0
+            for x in g:
+                gmask |= 1 << (x if x < L else high[x - L])
+            tg = gi & ~gmask      # the kernel's per-thread index: register bits cleared
+            for q in range(1, cnt + 1):
+                op = ops[k + q]
+                if op['kind'] in (OP_M1, OP_M2, OP_GRAD):
+                    assert int(op['cmask']) & gmask == 0, 'control on a register bit must use cslot'
+                if op['kind'] == OP_GRAD:
+                    v = _grad(a, b, tg, op, g, mats, L, high)
+                    grad[param_map[int(ps['map_begin']) + int(op['param'])]] += 2.0 * v
+                    continue
+                a = _apply(a, tg, op, g, mats)
+                if b is not None:
+                    b = _apply(b, tg, op, g, mats)
+            k += 1 + cnt
+        sv[gi] = a
+        if lam is not None:
+            lam[gi] = b
+    if lam is None:
+        return sv
+    return sv, lam, grad
+
+
+def _target_local(op):
+    s0 = int(op['s0'])
+    return s0
+
+
+def _pred(gi, op, g):
+    # thread-level control on the amplitude's global index with register bits cleared
+    cm, cv = int(op['cmask']), int(op['cval'])
+    return (gi & cm) == cv
+
+
+def _apply(a, gi, op, g, mats):
+    kind = int(op['kind'])
+    m0 = int(op['mat'])
+    pred = _pred(gi, op, g)
+    if kind == OP_M1:
+        m = mats[m0:m0 + 4].reshape(2, 2)
+        s0 = int(op['s0'])
+        tl = (s0 - 16) if s0 >= 16 else g[s0]
+        cs = int(op['cslot'])
+        bit = (np.arange(a.shape[1]) >> tl) & 1
+        partner = np.arange(a.shape[1]) ^ (1 << tl)
+        p = a[:, partner]
+        new = np.where(bit[None, :] == 0, m[0, 0] * a + m[0, 1] * p, m[1, 0] * p + m[1, 1] * a)
+        ok = pred
+        if cs >= 0:
+            ok = ok & (((np.arange(a.shape[1]) >> g[cs]) & 1)[None, :] == 1)
+        return np.where(ok, new, a)
+    if kind == OP_M2:
+        m = mats[m0:m0 + 16].reshape(4, 4)
+        t0, t1 = g[int(op['s0'])], g[int(op['s1'])]
+        j = np.arange(a.shape[1])
+        r = ((j >> t1) & 1) * 2 + ((j >> t0) & 1)
+        base = j & ~((1 << t0) | (1 << t1))
+        cols = [base, base | (1 << t0), base | (1 << t1), base | (1 << t0) | (1 << t1)]
+        new = sum(m[r, c][None, :] * a[:, cols[c]] for c in range(4))
+        return np.where(pred, new, a)
+    if kind == OP_DIAG:
+        d = mats[m0:m0 + 4]
+        ba, bb = _diag_bits(gi, op, g, a.shape[1])
+        f = d[ba + 2 * bb]
+        return np.where(pred, a * f, a)
+    raise AssertionError(kind)
+
+
+def _diag_bits(tg, op, g, width):
+    j = np.arange(width)
+    out = []
+    for key, skey in (('ga', 'sa'), ('gb', 'sb')):
+        gbit, slot = int(op[key]), int(op[skey])
+        if slot >= 0:
+            out.append(((j >> g[slot]) & 1)[None, :])
+        elif gbit != 0xFF:
+            out.append(_bit(tg, gbit))
+        else:
+            out.append(0)
+    return out[0], out[1]
+
+
+def _grad(a, b, gi, op, g, mats, L, high):
+    m0 = int(op['mat'])
+    pred = _pred(gi, op, g)
+    if int(op['s1']) == 1:
+        d = mats[m0:m0 + 4]
+        ba, bb = _diag_bits(gi, op, g, a.shape[1])
+        ga_ = d[ba + 2 * bb] * a
+    else:
+        m = mats[m0:m0 + 4].reshape(2, 2)
+        s0 = int(op['s0'])
+        tl = (s0 - 16) if s0 >= 16 else g[s0]
+        j = np.arange(a.shape[1])
+        bit = (j >> tl) & 1
+        p = a[:, j ^ (1 << tl)]
+        ga_ = np.where(bit[None, :] == 0, m[0, 0] * a + m[0, 1] * p, m[1, 0] * p + m[1, 1] * a)
+        cs = int(op['cslot'])
+        if cs >= 0:
+            pred = pred & (((j >> g[cs]) & 1)[None, :] == 1)
+    return float(np.real(np.sum(np.where(pred, np.conj(b) * ga_, 0))))
