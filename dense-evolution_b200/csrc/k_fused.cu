@@ -74,7 +74,7 @@ int fused_pass(void *sv, int dtype, const TileGeom &g, const desv_op *ops, int n
             case 9: return launch_fused<float2, 9, 4>(p, g, ops, nops, m, st);
             case 10: return launch_fused<float2, 10, 4>(p, g, ops, nops, m, st);
             case 11: return launch_fused<float2, 11, 4>(p, g, ops, nops, m, st);
-            case 12: return launch_fused<float2, 12, 4>(p, g, ops, nops, m, st);
+            case 12: return launch_fused<float2, 12, 3>(p, g, ops, nops, m, st);
             case 13: return launch_fused<float2, 13, 3>(p, g, ops, nops, m, st);
             default: return fail(DESV_EINVAL, "fused pass: complex64 tile_bits must be 9..13");
         }

@@ -31,14 +31,20 @@ template <typename T> __device__ __forceinline__ M22<T> load_m22(const T *p) {
     return m;
 }
 
-// 2x2 on register slot S (pairs j, j | 1<<S), optionally controlled by register slot `cs`.
-template <int S, int VAR, typename T>
-__device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m, int cs) {
+// 16-bit mask of the register indices j whose bit `slot` is set
+__device__ __forceinline__ uint32_t slot_mask(int slot) {
+    return slot == 0 ? 0xAAAAu : slot == 1 ? 0xCCCCu : slot == 2 ? 0xF0F0u : 0xFF00u;
+}
+
+// 2x2 on register slot S (pairs j, j | 1<<S).  CTRL: only pairs whose bit in
+// the 16-bit mask `act` is set are updated (control on a register slot).
+template <int S, int VAR, bool CTRL, typename T>
+__device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m, uint32_t act) {
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         if (j & (1 << S)) continue;
         const int j1 = j | (1 << S);
-        if (cs >= 0 && !((j >> cs) & 1)) continue;
+        if (CTRL && !((act >> j) & 1u)) continue;
         const T x0 = a[j], x1 = a[j1];
         if (VAR == V_DIAG) {
             a[j] = cmul(m.m00, x0);
@@ -58,15 +64,21 @@ __device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m, int cs) {
     }
 }
 
+template <int S, bool CTRL, typename T>
+__device__ __forceinline__ void m1_reg_var(T (&a)[16], const M22<T> &m, int var, uint32_t act) {
+    switch (var) {
+        case V_DIAG: m1_reg<S, V_DIAG, CTRL>(a, m, act); break;
+        case V_PHASE1: m1_reg<S, V_PHASE1, CTRL>(a, m, act); break;
+        case V_ANTI: m1_reg<S, V_ANTI, CTRL>(a, m, act); break;
+        case V_REAL: m1_reg<S, V_REAL, CTRL>(a, m, act); break;
+        default: m1_reg<S, V_GEN, CTRL>(a, m, act); break;
+    }
+}
+
 template <int S, typename T>
 __device__ __forceinline__ void m1_reg_dispatch(T (&a)[16], const M22<T> &m, int var, int cs) {
-    switch (var) {
-        case V_DIAG: m1_reg<S, V_DIAG>(a, m, cs); break;
-        case V_PHASE1: m1_reg<S, V_PHASE1>(a, m, cs); break;
-        case V_ANTI: m1_reg<S, V_ANTI>(a, m, cs); break;
-        case V_REAL: m1_reg<S, V_REAL>(a, m, cs); break;
-        default: m1_reg<S, V_GEN>(a, m, cs); break;
-    }
+    if (cs < 0) m1_reg_var<S, false>(a, m, var, 0xFFFFu);
+    else m1_reg_var<S, true>(a, m, var, slot_mask(cs));
 }
 
 // 2x2 on lane bit lb: the partner amplitude lives in lane ^ (1 << lb).
@@ -75,16 +87,17 @@ __device__ __forceinline__ void m1_lane(T (&a)[16], const M22<T> &m, int var, in
     const int mine = (lane >> lb) & 1;
     const T cself = mine ? m.m11 : m.m00;
     const T coth = mine ? m.m10 : m.m01;
+    const uint32_t act = cs < 0 ? 0xFFFFu : slot_mask(cs);
     if (var == V_DIAG || var == V_PHASE1) {
         if (!pred || (var == V_PHASE1 && !mine)) return;
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-            if (cs < 0 || ((j >> cs) & 1)) a[j] = cmul(cself, a[j]);
+            if ((act >> j) & 1u) a[j] = cmul(cself, a[j]);
         return;
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        if (cs >= 0 && !((j >> cs) & 1)) continue;  // uniform across the warp
+        if (!((act >> j) & 1u)) continue;  // uniform across the warp
         const T p = shfl_xor(a[j], 1 << lb);
         T r;
         if (var == V_ANTI) r = cmul(coth, p);
@@ -126,7 +139,9 @@ __device__ __forceinline__ void m2_dispatch(T (&a)[16], const T *mp, int s0, int
     }
 }
 
-// diagonal factor d[bit(ga) + 2 bit(gb)]; bits come from register slots sa/sb or the thread index
+// diagonal factor d[bit(ga) + 2 bit(gb)]; bits come from register slots sa/sb
+// or the thread index.  The per-amplitude selection uses 16-bit masks
+// computed once per op.
 template <typename T>
 __device__ __forceinline__ void diag_apply(T (&a)[16], const T *dp, int sa, int sb, int fa, int fb, bool sign_only) {
     const T d0 = dp[0], d1 = dp[1], d2 = dp[2], d3 = dp[3];
@@ -143,14 +158,21 @@ __device__ __forceinline__ void diag_apply(T (&a)[16], const T *dp, int sa, int 
         }
         return;
     }
+    const uint32_t A = sa >= 0 ? slot_mask(sa) : (fa ? 0xFFFFu : 0u);
+    const uint32_t B = sb >= 0 ? slot_mask(sb) : (fb ? 0xFFFFu : 0u);
+    const uint32_t m0 = ~A & ~B & 0xFFFFu, m1 = A & ~B & 0xFFFFu, m2 = ~A & B & 0xFFFFu, m3 = A & B;
+    if (sign_only) {
+        const uint32_t neg = (d0.x < 0 ? m0 : 0u) | (d1.x < 0 ? m1 : 0u) | (d2.x < 0 ? m2 : 0u) | (d3.x < 0 ? m3 : 0u);
+        if (neg)
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                if ((neg >> j) & 1u) a[j] = cneg(a[j]);
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        const int ba = sa >= 0 ? ((j >> sa) & 1) : fa;
-        const int bb = sb >= 0 ? ((j >> sb) & 1) : fb;
-        const int k = ba | (bb << 1);
-        const T f = k == 0 ? d0 : k == 1 ? d1 : k == 2 ? d2 : d3;
-        if (sign_only) a[j] = f.x < 0 ? cneg(a[j]) : a[j];
-        else a[j] = cmul(f, a[j]);
+        const T f = ((m3 >> j) & 1u) ? d3 : ((m2 >> j) & 1u) ? d2 : ((m1 >> j) & 1u) ? d1 : d0;
+        a[j] = cmul(f, a[j]);
     }
 }
 

@@ -9,9 +9,9 @@
 // consecutive tile ids are neighbours in memory.
 //
 // Each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... through a ring
-// of NBUF shared-memory slots.  Warp 0 issues one cp.async.bulk per 2^L-run
-// (loads complete on the slot's mbarrier, stores go into per-lane bulk
-// groups), every thread runs the body on the slot in shared memory.  Loads
+// of NBUF shared-memory slots.  Every thread issues cp.async.bulk copies for
+// its share of the 2^L-runs (loads complete on the slot's mbarrier, stores go
+// into per-thread bulk groups); every thread runs the body on the slot.  Loads
 // run D = NBUF-2 tiles ahead when the body's results are stored (one slot is
 // still draining its store), NBUF-1 tiles ahead otherwise.
 #pragma once
@@ -61,28 +61,37 @@ template <typename T, int NARR> struct PipeArrays {
 
 // Run `body(smem_slot_arrays, tile_base, tile_id)` over every tile.  Returns
 // false (after draining in-flight copies) if a bounded wait gave up.
+//
+// Every thread issues the bulk copies of the 2^L-runs c = threadIdx.x,
+// threadIdx.x + blockDim.x, ...; each warp announces its own byte count on the
+// slot's mbarrier (initialised with one arrival per warp), so no warp
+// serialises the copy issue of the whole tile.
 template <typename T, int K, int NBUF, int NARR, class Body>
 __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body &body, unsigned char *smem) {
     constexpr uint32_t TILE = 1u << K;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     T *bufs = reinterpret_cast<T *>(smem + 128);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const int lane = tid & 31;
     const uint32_t ntiles = 1u << (g.n - K);
     const uint32_t cnt = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
     const uint32_t chunk = 1u << g.L, nchunks = 1u << (K - g.L);
     const uint32_t chunk_bytes = chunk * sizeof(T);
 
     bool any_store = false;
-    uint32_t load_bytes = 0;
+    uint32_t nload = 0;
 #pragma unroll
     for (int a = 0; a < NARR; ++a) {
         any_store |= A.store[a];
-        if (A.load[a]) load_bytes += TILE * sizeof(T);
+        nload += A.load[a] ? 1u : 0u;
     }
     const uint32_t D = any_store ? (NBUF - 2) : (NBUF - 1);
+    // bytes this warp's copies deliver per tile
+    const uint32_t mine = tid < nchunks ? (nchunks - tid + nthr - 1) / nthr : 0u;
+    const uint32_t warp_bytes = __reduce_add_sync(0xffffffffu, mine) * chunk_bytes * nload;
 
-    if (threadIdx.x == 0) {
-        for (int b = 0; b < NBUF; ++b) mbar_init(&full[b], 1);
+    if (tid == 0) {
+        for (int b = 0; b < NBUF; ++b) mbar_init(&full[b], nthr / 32);
         fence_mbar_init();
     }
     __syncthreads();
@@ -91,9 +100,9 @@ __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body 
     auto issue_load = [&](uint32_t i) {
         const uint32_t slot = i % NBUF;
         const uint64_t base = tile_base(g, blockIdx.x + (uint64_t)i * gridDim.x);
-        if (lane == 0) mbar_arrive_expect_tx(&full[slot], load_bytes);
+        if (lane == 0) mbar_arrive_expect_tx(&full[slot], warp_bytes);
         __syncwarp();
-        for (uint32_t c = lane; c < nchunks; c += 32) {
+        for (uint32_t c = tid; c < nchunks; c += nthr) {
             const uint64_t off = base + chunk_offset(g, c);
 #pragma unroll
             for (int a = 0; a < NARR; ++a)
@@ -101,47 +110,41 @@ __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body 
         }
     };
 
-    if (warp == 0)
-        for (uint32_t i = 0; i < D && i < cnt; ++i) issue_load(i);
+    for (uint32_t i = 0; i < D && i < cnt; ++i) issue_load(i);
 
     bool ok = true;
     uint32_t i = 0;
     for (; i < cnt; ++i) {
         const uint32_t slot = i % NBUF;
-        if (warp == 0 && i + D < cnt) {
-            if (any_store) bulk_wait_read<1>();
-            __syncwarp();
-            issue_load(i + D);
-        }
         const bool waited = mbar_wait_bounded(&full[slot], (i / NBUF) & 1u);
+        if (any_store) bulk_wait_read<1>();  // this thread's stores older than the last group have left smem
         if (!__syncthreads_and(waited)) { ok = false; break; }
+        if (i + D < cnt) issue_load(i + D);  // into the slot of tile i+D-NBUF (drained above)
         T *sp[NARR];
 #pragma unroll
         for (int a = 0; a < NARR; ++a) sp[a] = slot_ptr(slot, a);
-        const uint64_t tid = blockIdx.x + (uint64_t)i * gridDim.x;
-        const uint64_t base = tile_base(g, tid);
-        body(sp, base, tid);
+        const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
+        const uint64_t base = tile_base(g, tix);
+        body(sp, base, tix);
         if (any_store) {
             fence_proxy_async_smem();
             __syncthreads();
-            if (warp == 0) {
-                for (uint32_t c = lane; c < nchunks; c += 32) {
-                    const uint64_t off = base + chunk_offset(g, c);
+            for (uint32_t c = tid; c < nchunks; c += nthr) {
+                const uint64_t off = base + chunk_offset(g, c);
 #pragma unroll
-                    for (int a = 0; a < NARR; ++a)
-                        if (A.store[a]) bulk_s2g(A.ptr[a] + off, sp[a] + (size_t)c * chunk, chunk_bytes);
-                }
-                bulk_commit();
+                for (int a = 0; a < NARR; ++a)
+                    if (A.store[a]) bulk_s2g(A.ptr[a] + off, sp[a] + (size_t)c * chunk, chunk_bytes);
             }
+            bulk_commit();
         } else {
             __syncthreads();
         }
     }
-    if (!ok && warp == 0) {
+    if (!ok) {
         // drain loads still in flight (bounded) so no copy targets freed shared memory
         for (uint32_t j = i; j < cnt && j < i + D + 1; ++j) mbar_wait_bounded(&full[j % NBUF], (j / NBUF) & 1u, 1u << 16);
     }
-    if (warp == 0 && any_store) bulk_wait_all();
+    if (any_store) bulk_wait_all();
     return ok;
 }
 
