@@ -57,6 +57,7 @@ _SIGS = {
     'desv_collapse': ([_vp, _i, _i, _i, _i, _d, _vp], _i),
     'desv_pauli_expect': ([_vp, _i, _i, _vp, _i, _vp, _vp, _vp, _sz, _vp], _i),
     'desv_pauli_matvec': ([_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _sz, _vp], _i),
+    'desv_pauli_expect_noalloc': ([_vp, _i, _i, _vp, _i, _vp, _vp, _vp], _i),
     'desv_adjoint_scratch_bytes': ([_i], _sz),
     'desv_adjoint_passes': ([_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp], _i),
 }

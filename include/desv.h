@@ -173,6 +173,19 @@ int desv_collapse(void *sv, int n, int dtype, int bit, int outcome, double scale
 int desv_pauli_expect(const void *psi, int n, int dtype, const desv_pauli_pass *passes, int npasses,
                       const desv_pauli_term *terms_dev, double *out_dev, void *scratch,
                       size_t scratch_bytes, void *stream);
+/* Allocation-free variant of desv_pauli_expect (no counterpart in the
+ * reference: an addition for callers that cannot allocate device memory or
+ * pass a scratch buffer, e.g. hosts whose allocator already owns all of HBM,
+ * plugins that may not allocate after load, latency-critical loops).  Same
+ * inputs and output minus the scratch: the per-CTA partial sums use a fixed
+ * 256 KiB device array inside the library, held by every GPU that loads it
+ * until exit.  At most 16384 / (8 x SMs) passes with terms (13 on a 148-SM
+ * B200); more are rejected with DESV_EINVAL before any launch.  The first
+ * call on a device looks the array up (cudaGetSymbolAddress): make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race and must be serialised. */
+int desv_pauli_expect_noalloc(const void *psi, int n, int dtype, const desv_pauli_pass *passes, int npasses,
+                              const desv_pauli_term *terms_dev, double *out_dev, void *stream);
 /* out = H psi (overwrites out); if expect_dev != NULL also accumulates
  * <psi|H psi> into expect_dev[0..1] like desv_pauli_expect. */
 int desv_pauli_matvec(const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes,
