@@ -282,6 +282,7 @@ def run_ours(args):
     torch.cuda.empty_cache()
 
     vqe = run_vqe(args) if not args.skip_vqe else None
+    batch = run_batch(args) if not args.skip_batch else None
     cpu = cpu_baseline() if (rank == 0 and ws == 1 and not args.skip_cpu) else None
     if rank == 0:
         line = {
@@ -307,6 +308,7 @@ def run_ours(args):
             'clocks': clk.summary(),
             'cpu_baseline': cpu,
             'vqe': vqe,
+            'batch': batch,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -347,6 +349,46 @@ def run_vqe(args):
             'backward_passes': int(len(prog.back.passes)), 'adjoint_ms': adj_s * 1e3, 'shift_ms': ps_s * 1e3}
 
 
+def run_batch(args, ncirc=4096, layers=6):
+    """Config 4: 4096 circuits, n ~ U{10..20}, HEA of 6 layers, XXZ chain with J_z ~ U[0.5, 1.5];
+    energy + adjoint gradient of every circuit from one persistent launch (CUDA graph replay)."""
+    import torch
+    from dense_evolution.batch import BatchVQE, hea_xxz_batch
+    rng = np.random.default_rng(SEED)
+    ns = rng.integers(10, 21, ncirc)
+    jz = rng.uniform(0.5, 1.5, ncirc)
+    t0 = time.perf_counter()
+    b = BatchVQE(hea_xxz_batch(ns, layers, jz), use_float32=True)
+    build_s = time.perf_counter() - t0
+    thetas = [rng.uniform(-np.pi, np.pi, 2 * n * layers) for n in ns]
+    b.set_theta(thetas)
+    b.capture()
+    for _ in range(max(1, args.warmup)):
+        b.graph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(2, args.steps)
+    e0.record()
+    for _ in range(reps):
+        b.graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    # end to end: host parameters in, energies + gradients out, every step
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        e, g = b.run(thetas, use_graph=True)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) / reps * 1e3
+    amps = float(np.sum(2.0 ** ns))
+    return {'workload': f'{ncirc} circuits, qubits uniform in 10..20, HEA {layers} layers (RY,RZ + CX ladder), '
+                        f'XXZ open chain J_xy=1, J_z~U[0.5,1.5]; energy + adjoint gradient per circuit',
+            'ms_per_batch': ms, 'circuits_per_s': ncirc / (ms / 1e3), 'grads_per_s': ncirc / (ms / 1e3),
+            'e2e_ms_per_batch': e2e_ms, 'plans': len(b.plans), 'launches_per_batch': 1,
+            'total_amplitudes': amps, 'resident_circuits': int(np.sum(ns <= 12)),
+            'plan_build_s': build_s, 'energy_mean': float(np.mean(e))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -355,6 +397,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--skip-vqe', action='store_true')
     ap.add_argument('--skip-cpu', action='store_true')
+    ap.add_argument('--skip-batch', action='store_true')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

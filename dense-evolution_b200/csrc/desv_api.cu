@@ -101,6 +101,7 @@ int desv_device_status(void *stream) {
         for (int k = 0; k < g_nreaders; ++k) h |= g_readers[k]();
     }
     if (h & DESV_DEV_TIMEOUT) return fail(DESV_ETIMEOUT, "a bounded wait inside a kernel gave up");
+    if (h & DESV_DEV_BADPLAN) return fail(DESV_EINVAL, "a kernel skipped a pass whose tile geometry it cannot run");
     return DESV_OK;
 }
 
@@ -293,6 +294,65 @@ int desv_pauli_matvec(const void *psi, void *out, int n, int dtype, const desv_p
                       const desv_pauli_term *terms, double *expect, void *scratch, size_t sb, void *stream) {
     if (psi == out) return fail(DESV_EINVAL, "matvec output must not alias the input");
     return pauli_common(psi, out, n, dtype, passes, npasses, terms, expect, scratch, sb, true, stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batched VQE
+namespace desv {
+int batch_vqe(int, const desv_batch_args &, int *, int, cudaStream_t);
+int batch_max_ctas(int);
+int batch_max_params();
+int batch_resident_bits();
+
+static void batch_layout(int dtype, int max_n, int max_pool, int ctas, size_t *ws_state, size_t *ws_pool,
+                         size_t *pool_stride, uint64_t *ws_amps) {
+    const size_t es = dtype == DESV_C64 ? 8 : 16;
+    *ws_amps = max_n > batch_resident_bits() ? (1ull << max_n) : 0ull;
+    *ws_state = (size_t)ctas * 2 * (size_t)(*ws_amps) * es;
+    *pool_stride = (((size_t)max_pool * es) + 255) / 256 * 256;
+    *ws_pool = (size_t)ctas * (*pool_stride);
+}
+}  // namespace desv
+
+extern "C" {
+
+size_t desv_batch_workspace_bytes(int dtype, int max_n, int max_pool_len) {
+    if ((dtype != DESV_C64 && dtype != DESV_C128) || max_n < 1 || max_n > 34 || max_pool_len < 0) return 0;
+    const int ctas = batch_max_ctas(dtype);
+    size_t st, pl, stride;
+    uint64_t amps;
+    batch_layout(dtype, max_n, max_pool_len, ctas, &st, &pl, &stride, &amps);
+    return 256 + st + pl;
+}
+
+int desv_batch_vqe(int dtype, int max_n, int max_pool_len, const desv_batch_args *args, void *workspace,
+                   size_t workspace_bytes, void *stream) {
+    if (dtype != DESV_C64 && dtype != DESV_C128) return fail(DESV_EINVAL, "batch: bad dtype");
+    if (!args || !workspace) return fail(DESV_EINVAL, "batch: null args or workspace");
+    if (max_n < 9 || max_n > 30) return fail(DESV_EINVAL, "batch: max_n must be in [9, 30]");
+    if (args->ncirc < 0) return fail(DESV_EINVAL, "batch: negative circuit count");
+    if (args->ncirc == 0) return DESV_OK;
+    if (!args->circuits || !args->plans || !args->passes || !args->ops || !args->recipes || !args->cpool ||
+        !args->theta || !args->energy || !args->grad)
+        return fail(DESV_EINVAL, "batch: null device array in args");
+    const int ctas = batch_max_ctas(dtype);
+    size_t st, pl, stride;
+    uint64_t amps;
+    batch_layout(dtype, max_n, max_pool_len, ctas, &st, &pl, &stride, &amps);
+    if (workspace_bytes < 256 + st + pl) return fail(DESV_EINVAL, "batch: workspace smaller than desv_batch_workspace_bytes");
+    if (reinterpret_cast<uintptr_t>(workspace) % 256) return fail(DESV_EINVAL, "batch: workspace must be 256-byte aligned");
+    desv_batch_args a = *args;
+    char *w = static_cast<char *>(workspace);
+    int *queue = reinterpret_cast<int *>(w);
+    a.workspace = w + 256;
+    a.ws_amps = amps;
+    a.pool_ws = w + 256 + st;
+    a.pool_stride_bytes = stride;
+    if (cudaMemsetAsync(queue, 0, sizeof(int), S(stream)) != cudaSuccess) return check_launch("batch queue reset");
+    int grid = ctas < args->ncirc ? ctas : args->ncirc;
+    return batch_vqe(dtype, a, queue, grid, S(stream));
 }
 
 }  // extern "C"

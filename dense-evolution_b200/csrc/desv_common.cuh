@@ -22,6 +22,7 @@ int sm_count();
 // translation unit has its own copy (no relocatable device code); every unit
 // registers a reader with the API layer at load time.
 #define DESV_DEV_TIMEOUT 1
+#define DESV_DEV_BADPLAN 2
 static __device__ int g_dev_status = 0;
 void register_status_reader(int (*reader)());
 static int tu_status_read_clear() {

@@ -1,0 +1,293 @@
+// Batched VQE: energy + adjoint gradient of thousands of independent circuits
+// of uneven qubit count in ONE persistent launch.
+//
+// The reference runs one parameter row at a time (run_batch_jit vmaps a single
+// circuit structure with one qubit count, backends/statevector.py:496-584;
+// energy + jax.grad per circuit, solvers/autodiff.py:92-169).  Here every CTA
+// takes the next circuit from an atomic queue (the host orders circuits by
+// decreasing cost) and runs, for that circuit alone:
+//   1. its matrix pool, computed on the device from theta (recipes),
+//   2. the fused forward passes (register-stage interpreter of the fused
+//      kernel) on |0...0>,
+//   3. lambda = H psi and E = <psi|lambda> (FP64),
+//   4. the fused adjoint passes over (psi, lambda) with GRAD probes,
+//      accumulating dE/dtheta per warp in FP64.
+// Circuits of <= 2^RES amplitudes keep psi and lambda resident in shared memory
+// for all four steps (no HBM traffic); larger ones stream tiles of a per-CTA
+// workspace in HBM through shared memory pass by pass.
+#include "desv_common.cuh"
+#include "stage_ops.cuh"
+#include "grad_ops.cuh"
+#include "tile_pipeline.cuh"
+
+namespace desv {
+
+constexpr int BATCH_THREADS = 256;  // 2^(12-4): one register stage over a 2^12 tile
+constexpr int BATCH_K = 12;         // tile bits of streamed circuits (and the largest resident state)
+constexpr int BATCH_MAXP = 320;     // parameters per circuit
+constexpr int BATCH_NW = BATCH_THREADS / 32;
+
+template <typename T> __device__ __forceinline__ T cpx(double re, double im) {
+    T r;
+    r.x = (decltype(r.x))re;
+    r.y = (decltype(r.y))im;
+    return r;
+}
+
+// one recipe entry -> the circuit's pool
+template <typename T>
+__device__ __forceinline__ void run_recipe(const desv_batch_recipe &r, const double *theta, const T *cpool, T *pool) {
+    T *o = pool + r.off;
+    const int kind = r.kind & 0xFF;
+    if (kind == DESV_RCP_CONST) {
+        for (int e = 0; e < r.count; ++e) o[e] = cpool[r.src + e];
+        return;
+    }
+    double th = theta[r.param];
+    if (r.kind & DESV_RCP_INVERSE) th = -th;
+    double s, c;
+    sincos(0.5 * th, &s, &c);
+    double s1, c1;
+    sincos(th, &s1, &c1);
+    switch (kind) {
+        case DESV_RCP_RX: o[0] = cpx<T>(c, 0); o[1] = cpx<T>(0, -s); o[2] = cpx<T>(0, -s); o[3] = cpx<T>(c, 0); break;
+        case DESV_RCP_RY: o[0] = cpx<T>(c, 0); o[1] = cpx<T>(-s, 0); o[2] = cpx<T>(s, 0); o[3] = cpx<T>(c, 0); break;
+        case DESV_RCP_RZ: o[0] = cpx<T>(c, -s); o[1] = cpx<T>(0, 0); o[2] = cpx<T>(0, 0); o[3] = cpx<T>(c, s); break;
+        case DESV_RCP_P: o[0] = cpx<T>(1, 0); o[1] = cpx<T>(0, 0); o[2] = cpx<T>(0, 0); o[3] = cpx<T>(c1, s1); break;
+        case DESV_RCP_RZ_TAB: o[0] = cpx<T>(c, -s); o[1] = cpx<T>(c, s); o[2] = cpx<T>(c, -s); o[3] = cpx<T>(c, s); break;
+        case DESV_RCP_P_TAB: o[0] = cpx<T>(1, 0); o[1] = cpx<T>(c1, s1); o[2] = cpx<T>(1, 0); o[3] = cpx<T>(c1, s1); break;
+        case DESV_RCP_CP_VEC: o[0] = cpx<T>(1, 0); o[1] = cpx<T>(1, 0); o[2] = cpx<T>(1, 0); o[3] = cpx<T>(c1, s1); break;
+        case DESV_RCP_CRZ_VEC: o[0] = cpx<T>(1, 0); o[1] = cpx<T>(c, -s); o[2] = cpx<T>(1, 0); o[3] = cpx<T>(c, s); break;
+        case DESV_RCP_PHASE_VEC: o[0] = o[1] = o[2] = o[3] = cpx<T>(c1, s1); break;
+        default: break;
+    }
+}
+
+// One register stage of a pass over a tile in shared memory (optionally two
+// arrays).  Threads >= 2^(K-4) only take part in the barriers.
+template <typename T, bool ADJ>
+__device__ __forceinline__ void batch_stage(T *s0, T *s1, const desv_op &st, const desv_op *ops, int cnt,
+                                            const T *mats, uint64_t tg_base, const TileGeom &g, int active,
+                                            double *acc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if ((int)threadIdx.x < active) {
+        const uint32_t idx = stage_base(threadIdx.x, st.g);
+        const uint32_t o0 = 1u << st.g[0], o1 = 1u << st.g[1], o2 = 1u << st.g[2], o3 = 1u << st.g[3];
+        T a[16], b[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const uint32_t off = idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) + ((j & 8) ? o3 : 0u);
+            a[j] = s0[off];
+            if (ADJ) b[j] = s1[off];
+        }
+        const uint64_t tg = tg_base | tile_local_to_global(g, idx);
+        if (!ADJ) {
+            run_stage_ops(a, ops, cnt, mats, tg, lane);
+        } else {
+#pragma unroll 1
+            for (int q = 0; q < cnt; ++q) {
+                const desv_op op = ops[q];
+                if (op.kind == DESV_OP_GRAD) {
+                    double v = grad_term(a, b, op, mats + op.mat, tg, lane);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0 && op.param >= 0 && op.param < BATCH_MAXP) acc[warp * BATCH_MAXP + op.param] += v;
+                } else {
+                    apply_one_op(a, op, mats, tg, lane);
+                    apply_one_op(b, op, mats, tg, lane);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const uint32_t off = idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) + ((j & 8) ? o3 : 0u);
+            s0[off] = a[j];
+            if (ADJ) s1[off] = b[j];
+        }
+    }
+    __syncthreads();
+}
+
+// All stages of one pass on one tile already in shared memory.
+template <typename T, bool ADJ>
+__device__ void batch_tile(T *s0, T *s1, const desv_op *ops, int nops, const T *mats, uint64_t base,
+                           const TileGeom &g, double *acc) {
+    const int active = 1 << (g.K - 4);
+    int k = 0;
+    while (k < nops) {
+        const desv_op st = ops[k];
+        const int cnt = (int)st.mat;
+        batch_stage<T, ADJ>(s0, s1, st, ops + k + 1, cnt, mats, base, g, active, acc);
+        k += 1 + cnt;
+    }
+}
+
+// one pass over a state (resident: the state is the single tile)
+template <typename T, bool ADJ>
+__device__ void batch_pass(T *gpsi, T *glam, T *spsi, T *slam, bool resident, const desv_pass &ps, int n,
+                           const desv_op *ops, const T *mats, double *acc) {
+    TileGeom g;
+    g.n = n;
+    g.K = ps.tile_bits;
+    g.L = ps.low_bits;
+    for (int i = 0; i < g.K - g.L; ++i) g.high[i] = ps.high[i];
+    {
+        uint64_t tmask = (1ull << g.L) - 1ull;
+        for (int i = 0; i < g.K - g.L; ++i) tmask |= 1ull << g.high[i];
+        int r = 0;
+        for (int b = 0; b < n; ++b)
+            if (!((tmask >> b) & 1ull)) g.rest[r++] = (uint8_t)b;
+        g.nrest = r;
+    }
+    const desv_op *pops = ops + ps.op_begin;
+    const int nops = ps.op_end - ps.op_begin;
+    // tiles must fit the shared-memory buffers and the 4-register-bit stages;
+    // a resident state must be exactly one tile (host plans guarantee both)
+    if (g.K < 9 || g.K > BATCH_K || (resident && g.K != n) || g.K > n) {
+        if (threadIdx.x == 0) atomicOr(&g_dev_status, DESV_DEV_BADPLAN);
+        return;
+    }
+    if (resident) {
+        batch_tile<T, ADJ>(spsi, slam, pops, nops, mats, 0, g, acc);
+        return;
+    }
+    const uint32_t ntiles = 1u << (n - g.K), TILE = 1u << g.K, chunk = 1u << g.L, nch = 1u << (g.K - g.L);
+    for (uint32_t t = 0; t < ntiles; ++t) {
+        const uint64_t base = tile_base(g, t);
+        for (uint32_t e = threadIdx.x; e < TILE; e += blockDim.x) {
+            const uint64_t gi = base + chunk_offset(g, e >> g.L) + (e & (chunk - 1));
+            spsi[e] = gpsi[gi];
+            if (ADJ) slam[e] = glam[gi];
+        }
+        __syncthreads();
+        batch_tile<T, ADJ>(spsi, slam, pops, nops, mats, base, g, acc);
+        for (uint32_t e = threadIdx.x; e < TILE; e += blockDim.x) {
+            const uint64_t gi = base + chunk_offset(g, e >> g.L) + (e & (chunk - 1));
+            gpsi[gi] = spsi[e];
+            if (ADJ) glam[gi] = slam[e];
+        }
+        __syncthreads();
+        (void)nch;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_vqe(desv_batch_args args, int *queue) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    T *sA = reinterpret_cast<T *>(smem);
+    T *sB = sA + (1u << BATCH_K);
+    double *acc = reinterpret_cast<double *>(sB + (1u << BATCH_K));
+    double *red = acc + BATCH_NW * BATCH_MAXP;
+    __shared__ int s_c;
+    const int tid = threadIdx.x;
+    T *wpsi = static_cast<T *>(args.workspace) + (size_t)blockIdx.x * 2 * args.ws_amps;
+    T *wlam = wpsi + args.ws_amps;
+    T *pool = reinterpret_cast<T *>(static_cast<char *>(args.pool_ws) + (size_t)blockIdx.x * args.pool_stride_bytes);
+    const desv_batch_circuit *circs = args.circuits;
+    for (;;) {
+        if (tid == 0) s_c = atomicAdd(queue, 1);
+        __syncthreads();
+        const int c = s_c;
+        __syncthreads();
+        if (c >= args.ncirc) break;
+        const desv_batch_circuit cd = circs[c];
+        const desv_batch_plan pl = args.plans[cd.plan];
+        const int n = pl.n;
+        const uint64_t dim = 1ull << n;
+        const bool resident = n <= BATCH_K;
+        const double *theta = args.theta + cd.theta_off;
+        // 1. matrices of this circuit
+        for (int r = pl.rec_begin + tid; r < pl.rec_end; r += blockDim.x)
+            run_recipe<T>(args.recipes[r], theta, static_cast<const T *>(args.cpool), pool);
+        for (int i = tid; i < BATCH_NW * BATCH_MAXP; i += blockDim.x) acc[i] = 0.0;
+        // 2. |0...0> and the forward passes
+        T *gpsi = resident ? sA : wpsi;
+        T *glam = resident ? sB : wlam;
+        for (uint64_t i = tid; i < dim; i += blockDim.x) gpsi[i] = cpx<T>(i == 0 ? 1.0 : 0.0, 0.0);
+        __threadfence_block();
+        __syncthreads();
+        for (int p = pl.fwd_begin; p < pl.fwd_end; ++p)
+            batch_pass<T, false>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc);
+        // 3. lambda = H psi, E = <psi|lambda>
+        double ere = 0;
+        for (uint64_t i = tid; i < dim; i += blockDim.x) {
+            T v = cpx<T>(0, 0);
+            for (int k = pl.term_begin; k < pl.term_end; ++k) {
+                const desv_pauli_term tm = args.terms[k];
+                const uint64_t src = i ^ tm.xmask;
+                const T pz = gpsi[src];
+                const double cr = tm.cre * args.coef[cd.coef_off + (k - pl.term_begin)];
+                const double ci = tm.cim * args.coef[cd.coef_off + (k - pl.term_begin)];
+                T cc = cpx<T>(cr, ci);
+                if (__popcll(src & tm.zmask) & 1) cc = cneg(cc);
+                v = cfma(cc, pz, v);
+            }
+            glam[i] = v;
+            const T a = gpsi[i];
+            ere += (double)a.x * (double)v.x + (double)a.y * (double)v.y;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ere += __shfl_xor_sync(0xffffffffu, ere, o);
+        if ((tid & 31) == 0) red[tid >> 5] = ere;
+        __threadfence_block();
+        __syncthreads();
+        if (tid == 0) {
+            double e = 0;
+            for (int w = 0; w < BATCH_NW; ++w) e += red[w];
+            args.energy[cd.out_index] = e;
+        }
+        // 4. adjoint sweep over (psi, lambda)
+        for (int p = pl.bwd_begin; p < pl.bwd_end; ++p)
+            batch_pass<T, true>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc);
+        __syncthreads();
+        for (int q = tid; q < pl.nparams; q += blockDim.x) {
+            double s = 0;
+            for (int w = 0; w < BATCH_NW; ++w) s += acc[w * BATCH_MAXP + q];
+            args.grad[cd.grad_off + q] = 2.0 * s;
+        }
+        __syncthreads();
+    }
+}
+
+static size_t batch_smem_bytes(int dtype) {
+    const size_t es = dtype == DESV_C64 ? 8 : 16;
+    return 2 * ((size_t)1 << BATCH_K) * es + (size_t)BATCH_NW * BATCH_MAXP * 8 + 32 * 8;
+}
+
+static void batch_attrs(int dtype) {
+    static bool done[2][64] = {{false}};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (done[dtype][dev & 63]) return;
+    const size_t smem = batch_smem_bytes(dtype);
+    if (dtype == DESV_C64) cudaFuncSetAttribute(k_batch_vqe<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else cudaFuncSetAttribute(k_batch_vqe<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    done[dtype][dev & 63] = true;
+}
+
+int batch_max_ctas(int dtype) {
+    static int cache[2][64] = {{0}};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cache[dtype][dev & 63]) return cache[dtype][dev & 63];
+    batch_attrs(dtype);
+    int b = 0;
+    const size_t smem = batch_smem_bytes(dtype);
+    if (dtype == DESV_C64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_vqe<float2>, BATCH_THREADS, smem);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_vqe<double2>, BATCH_THREADS, smem);
+    cache[dtype][dev & 63] = (b > 0 ? b : 1) * sm_count();
+    return cache[dtype][dev & 63];
+}
+
+int batch_vqe(int dtype, const desv_batch_args &args, int *queue, int grid, cudaStream_t st) {
+    batch_attrs(dtype);
+    const size_t smem = batch_smem_bytes(dtype);
+    if (dtype == DESV_C64) k_batch_vqe<float2><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
+    else k_batch_vqe<double2><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
+    return check_launch("batched VQE");
+}
+
+int batch_max_params() { return BATCH_MAXP; }
+int batch_resident_bits() { return BATCH_K; }
+
+}  // namespace desv

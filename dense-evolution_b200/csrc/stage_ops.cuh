@@ -36,15 +36,16 @@ __device__ __forceinline__ uint32_t slot_mask(int slot) {
     return slot == 0 ? 0xAAAAu : slot == 1 ? 0xCCCCu : slot == 2 ? 0xF0F0u : 0xFF00u;
 }
 
-// 2x2 on register slot S (pairs j, j | 1<<S).  CTRL: only pairs whose bit in
-// the 16-bit mask `act` is set are updated (control on a register slot).
-template <int S, int VAR, bool CTRL, typename T>
-__device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m, uint32_t act) {
+// 2x2 on register slot S (pairs j, j | 1<<S).  CS >= 0: only pairs whose
+// register bit CS is set are updated (control on a register slot); every
+// register index is a compile-time constant.
+template <int S, int VAR, int CS, typename T>
+__device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m) {
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         if (j & (1 << S)) continue;
+        if (CS >= 0 && !((j >> CS) & 1)) continue;
         const int j1 = j | (1 << S);
-        if (CTRL && !((act >> j) & 1u)) continue;
         const T x0 = a[j], x1 = a[j1];
         if (VAR == V_DIAG) {
             a[j] = cmul(m.m00, x0);
@@ -64,24 +65,58 @@ __device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m, uint32_t act
     }
 }
 
-template <int S, bool CTRL, typename T>
-__device__ __forceinline__ void m1_reg_var(T (&a)[16], const M22<T> &m, int var, uint32_t act) {
+template <int S, typename T>
+__device__ __forceinline__ void m1_reg_uncontrolled(T (&a)[16], const M22<T> &m, int var) {
     switch (var) {
-        case V_DIAG: m1_reg<S, V_DIAG, CTRL>(a, m, act); break;
-        case V_PHASE1: m1_reg<S, V_PHASE1, CTRL>(a, m, act); break;
-        case V_ANTI: m1_reg<S, V_ANTI, CTRL>(a, m, act); break;
-        case V_REAL: m1_reg<S, V_REAL, CTRL>(a, m, act); break;
-        default: m1_reg<S, V_GEN, CTRL>(a, m, act); break;
+        case V_DIAG: m1_reg<S, V_DIAG, -1>(a, m); break;
+        case V_PHASE1: m1_reg<S, V_PHASE1, -1>(a, m); break;
+        case V_ANTI: m1_reg<S, V_ANTI, -1>(a, m); break;
+        case V_REAL: m1_reg<S, V_REAL, -1>(a, m); break;
+        default: m1_reg<S, V_GEN, -1>(a, m); break;
     }
+}
+
+// controlled by register slot CS: anti-diagonal (CX-like) or general
+template <int S, int CS, typename T>
+__device__ __forceinline__ void m1_reg_ctl(T (&a)[16], const M22<T> &m, int var) {
+    if (var == V_ANTI) m1_reg<S, V_ANTI, CS>(a, m);
+    else m1_reg<S, V_GEN, CS>(a, m);
 }
 
 template <int S, typename T>
 __device__ __forceinline__ void m1_reg_dispatch(T (&a)[16], const M22<T> &m, int var, int cs) {
-    if (cs < 0) m1_reg_var<S, false>(a, m, var, 0xFFFFu);
-    else m1_reg_var<S, true>(a, m, var, slot_mask(cs));
+    switch (cs) {
+        case -1: m1_reg_uncontrolled<S>(a, m, var); break;
+        case 0: if (S != 0) m1_reg_ctl<S, (S != 0 ? 0 : 1)>(a, m, var); break;
+        case 1: if (S != 1) m1_reg_ctl<S, (S != 1 ? 1 : 0)>(a, m, var); break;
+        case 2: if (S != 2) m1_reg_ctl<S, (S != 2 ? 2 : 0)>(a, m, var); break;
+        default: if (S != 3) m1_reg_ctl<S, (S != 3 ? 3 : 0)>(a, m, var); break;
+    }
 }
 
 // 2x2 on lane bit lb: the partner amplitude lives in lane ^ (1 << lb).
+// Uncontrolled (no thread predicate, no register control): no selects.
+template <int VAR, typename T>
+__device__ __forceinline__ void m1_lane_free(T (&a)[16], const M22<T> &m, int lb, int lane) {
+    const int mine = (lane >> lb) & 1;
+    const T cself = mine ? m.m11 : m.m00;
+    const T coth = mine ? m.m10 : m.m01;
+    if (VAR == V_DIAG || VAR == V_PHASE1) {
+        if (VAR == V_PHASE1 && !mine) return;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) a[j] = cmul(cself, a[j]);
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const T p = shfl_xor(a[j], 1 << lb);
+        if (VAR == V_ANTI) a[j] = cmul(coth, p);
+        else if (VAR == V_REAL) a[j] = rfma(coth.x, p, rfma(cself.x, a[j], mk(decltype(p.x)(0), decltype(p.x)(0))));
+        else a[j] = cfma(coth, p, cmul(cself, a[j]));
+    }
+}
+
+// controlled variant: thread predicate `pred` and/or register control slot `cs`
 template <typename T>
 __device__ __forceinline__ void m1_lane(T (&a)[16], const M22<T> &m, int var, int cs, int lb, bool pred, int lane) {
     const int mine = (lane >> lb) & 1;
@@ -139,15 +174,49 @@ __device__ __forceinline__ void m2_dispatch(T (&a)[16], const T *mp, int s0, int
     }
 }
 
-// diagonal factor d[bit(ga) + 2 bit(gb)]; bits come from register slots sa/sb
-// or the thread index.  The per-amplitude selection uses 16-bit masks
-// computed once per op.
+// diagonal factor d[bit(ga) + 2 bit(gb)] per amplitude.  SA / SB: register
+// slot holding that bit (compile-time) or -1 when the bit is fixed for the
+// thread (values fa / fb); the factor of every amplitude is then picked at
+// compile time from four per-op registers.
+template <int SA, int SB, typename T>
+__device__ __forceinline__ void diag_slots(T (&a)[16], const T *dp, int fa, int fb, bool sign_only) {
+    const T d[4] = {dp[0], dp[1], dp[2], dp[3]};
+    if (sign_only) {
+        const bool n0 = d[0].x < 0, n1 = d[1].x < 0, n2 = d[2].x < 0, n3 = d[3].x < 0;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int ba = SA >= 0 ? ((j >> SA) & 1) : fa;
+            const int bb = SB >= 0 ? ((j >> SB) & 1) : fb;
+            const int k = ba | (bb << 1);
+            const bool neg = k == 0 ? n0 : k == 1 ? n1 : k == 2 ? n2 : n3;
+            if (neg) a[j] = cneg(a[j]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int ba = SA >= 0 ? ((j >> SA) & 1) : fa;
+        const int bb = SB >= 0 ? ((j >> SB) & 1) : fb;
+        a[j] = cmul(d[ba | (bb << 1)], a[j]);
+    }
+}
+
+template <int SA, typename T>
+__device__ __forceinline__ void diag_sb(T (&a)[16], const T *dp, int sb, int fa, int fb, bool sg) {
+    switch (sb) {
+        case -1: diag_slots<SA, -1>(a, dp, fa, fb, sg); break;
+        case 0: diag_slots<SA, 0>(a, dp, fa, fb, sg); break;
+        case 1: diag_slots<SA, 1>(a, dp, fa, fb, sg); break;
+        case 2: diag_slots<SA, 2>(a, dp, fa, fb, sg); break;
+        default: diag_slots<SA, 3>(a, dp, fa, fb, sg); break;
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void diag_apply(T (&a)[16], const T *dp, int sa, int sb, int fa, int fb, bool sign_only) {
-    const T d0 = dp[0], d1 = dp[1], d2 = dp[2], d3 = dp[3];
     if (sa < 0 && sb < 0) {
         const int k = fa | (fb << 1);
-        const T f = k == 0 ? d0 : k == 1 ? d1 : k == 2 ? d2 : d3;
+        const T f = dp[k];
         if (sign_only) {
             if (f.x < 0)
 #pragma unroll
@@ -158,21 +227,12 @@ __device__ __forceinline__ void diag_apply(T (&a)[16], const T *dp, int sa, int 
         }
         return;
     }
-    const uint32_t A = sa >= 0 ? slot_mask(sa) : (fa ? 0xFFFFu : 0u);
-    const uint32_t B = sb >= 0 ? slot_mask(sb) : (fb ? 0xFFFFu : 0u);
-    const uint32_t m0 = ~A & ~B & 0xFFFFu, m1 = A & ~B & 0xFFFFu, m2 = ~A & B & 0xFFFFu, m3 = A & B;
-    if (sign_only) {
-        const uint32_t neg = (d0.x < 0 ? m0 : 0u) | (d1.x < 0 ? m1 : 0u) | (d2.x < 0 ? m2 : 0u) | (d3.x < 0 ? m3 : 0u);
-        if (neg)
-#pragma unroll
-            for (int j = 0; j < 16; ++j)
-                if ((neg >> j) & 1u) a[j] = cneg(a[j]);
-        return;
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        const T f = ((m3 >> j) & 1u) ? d3 : ((m2 >> j) & 1u) ? d2 : ((m1 >> j) & 1u) ? d1 : d0;
-        a[j] = cmul(f, a[j]);
+    switch (sa) {
+        case -1: diag_sb<-1>(a, dp, sb, fa, fb, sign_only); break;
+        case 0: diag_sb<0>(a, dp, sb, fa, fb, sign_only); break;
+        case 1: diag_sb<1>(a, dp, sb, fa, fb, sign_only); break;
+        case 2: diag_sb<2>(a, dp, sb, fa, fb, sign_only); break;
+        default: diag_sb<3>(a, dp, sb, fa, fb, sign_only); break;
     }
 }
 
@@ -187,7 +247,18 @@ __device__ __forceinline__ void apply_one_op(T (&a)[16], const desv_op &op, cons
             const int var = m1_variant(op.flags);
             const M22<T> m = load_m22(mp);
             if (op.s0 >= 16) {
-                m1_lane(a, m, var, op.cslot, op.s0 - 16, pred, lane);
+                if (op.cmask == 0 && op.cslot < 0) {
+                    const int lb = op.s0 - 16;
+                    switch (var) {
+                        case V_DIAG: m1_lane_free<V_DIAG>(a, m, lb, lane); break;
+                        case V_PHASE1: m1_lane_free<V_PHASE1>(a, m, lb, lane); break;
+                        case V_ANTI: m1_lane_free<V_ANTI>(a, m, lb, lane); break;
+                        case V_REAL: m1_lane_free<V_REAL>(a, m, lb, lane); break;
+                        default: m1_lane_free<V_GEN>(a, m, lb, lane); break;
+                    }
+                } else {
+                    m1_lane(a, m, var, op.cslot, op.s0 - 16, pred, lane);
+                }
             } else if (pred) {
                 switch (op.s0) {
                     case 0: m1_reg_dispatch<0>(a, m, var, op.cslot); break;
@@ -208,16 +279,88 @@ __device__ __forceinline__ void apply_one_op(T (&a)[16], const desv_op &op, cons
     }
 }
 
+// Host-computed dispatch codes (desv_op bytes 13-14, see include/desv.h):
+//   1 + S*5 + VAR                        2x2 on register slot S, uncontrolled
+//   21 + (S*4 + CS)*2 + (VAR != ANTI)    2x2 on slot S controlled by slot CS
+//   53 + VAR                             2x2 on a lane bit, uncontrolled
+//   58 + (SA+1)*5 + (SB+1)               sign-only diagonal (slots SA/SB, -1 = thread bit)
+//   83 + (SA+1)*5 + (SB+1)               diagonal
+//   | 0x8000                             the thread predicate (cmask/cval) applies
+//   0                                    decode the fields (apply_one_op)
+#define DESV_CODE_PRED 0x8000u
+
+template <int S, int CS, typename T>
+__device__ __forceinline__ void m1_ctl_case(T (&a)[16], const M22<T> &m, bool anti) {
+    if (CS == S) return;
+    if (anti) m1_reg<S, V_ANTI, (CS == S ? -1 : CS)>(a, m);
+    else m1_reg<S, V_GEN, (CS == S ? -1 : CS)>(a, m);
+}
+
+template <int SA, int SB, typename T>
+__device__ __forceinline__ void diag_case(T (&a)[16], const T *mp, uint32_t w0y, uint64_t tg, bool sg) {
+    // thread-fixed bit values, read only when the bit is not in a register slot
+    const int fa = SA >= 0 ? 0 : (((w0y >> 8) & 0xFFu) == 0xFFu ? 0 : (int)((tg >> ((w0y >> 8) & 0xFFu)) & 1ull));
+    const int fb = SB >= 0 ? 0 : (((w0y >> 16) & 0xFFu) == 0xFFu ? 0 : (int)((tg >> ((w0y >> 16) & 0xFFu)) & 1ull));
+    diag_slots<SA, SB>(a, mp, fa, fb, sg);
+}
+
+#define DESV_M1U(S)                                                              \
+    case 1 + S * 5 + V_GEN: m1_reg<S, V_GEN, -1>(a, load_m22(mp)); break;        \
+    case 1 + S * 5 + V_REAL: m1_reg<S, V_REAL, -1>(a, load_m22(mp)); break;      \
+    case 1 + S * 5 + V_DIAG: m1_reg<S, V_DIAG, -1>(a, load_m22(mp)); break;      \
+    case 1 + S * 5 + V_PHASE1: m1_reg<S, V_PHASE1, -1>(a, load_m22(mp)); break;  \
+    case 1 + S * 5 + V_ANTI: m1_reg<S, V_ANTI, -1>(a, load_m22(mp)); break;
+#define DESV_M1C(S, CS)                                                                   \
+    case 21 + (S * 4 + CS) * 2: m1_ctl_case<S, CS>(a, load_m22(mp), true); break;         \
+    case 21 + (S * 4 + CS) * 2 + 1: m1_ctl_case<S, CS>(a, load_m22(mp), false); break;
+#define DESV_DG(SA, SB)                                                                     \
+    case 58 + (SA + 1) * 5 + (SB + 1): diag_case<SA, SB>(a, mp, w0y, tg, true); break;    \
+    case 83 + (SA + 1) * 5 + (SB + 1): diag_case<SA, SB>(a, mp, w0y, tg, false); break;
+#define DESV_DGROW(SA) DESV_DG(SA, -1) DESV_DG(SA, 0) DESV_DG(SA, 1) DESV_DG(SA, 2) DESV_DG(SA, 3)
+
 // Apply ops[0..nops) of one stage to the thread's registers.
 template <typename T>
 __device__ __forceinline__ void run_stage_ops(T (&a)[16], const desv_op *ops, int nops, const T *mats, uint64_t tg,
                                               int lane) {
 #pragma unroll 1
     for (int k = 0; k < nops; ++k) {
-        const desv_op op = ops[k];
-        apply_one_op(a, op, mats, tg, lane);
+        // desv_op is 40 bytes: records are only 8-byte aligned, so read bytes
+        // 0..15 as two 8-byte words (a 16-byte load would be misaligned for odd k)
+        const uint2 wlo = reinterpret_cast<const uint2 *>(ops + k)[0];
+        const uint2 whi = reinterpret_cast<const uint2 *>(ops + k)[1];
+        const uint4 w0 = make_uint4(wlo.x, wlo.y, whi.x, whi.y);
+        const uint32_t code = (w0.w >> 8) & 0xFFFFu;
+        if (code == 0) {
+            const desv_op op = ops[k];
+            apply_one_op(a, op, mats, tg, lane);
+            continue;
+        }
+        const T *mp = mats + reinterpret_cast<const uint32_t *>(ops + k)[4];
+        if (code & DESV_CODE_PRED) {
+            const uint64_t cm = ops[k].cmask, cv = ops[k].cval;
+            if ((tg & cm) != cv) continue;
+        }
+        const uint32_t w0y = w0.y;  // bytes 4..7: cslot, ga, gb, sa
+        switch (code & 0x7FFFu) {
+            DESV_M1U(0) DESV_M1U(1) DESV_M1U(2) DESV_M1U(3)
+            DESV_M1C(0, 1) DESV_M1C(0, 2) DESV_M1C(0, 3)
+            DESV_M1C(1, 0) DESV_M1C(1, 2) DESV_M1C(1, 3)
+            DESV_M1C(2, 0) DESV_M1C(2, 1) DESV_M1C(2, 3)
+            DESV_M1C(3, 0) DESV_M1C(3, 1) DESV_M1C(3, 2)
+            case 53 + V_GEN: m1_lane_free<V_GEN>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+            case 53 + V_REAL: m1_lane_free<V_REAL>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+            case 53 + V_DIAG: m1_lane_free<V_DIAG>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+            case 53 + V_PHASE1: m1_lane_free<V_PHASE1>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+            case 53 + V_ANTI: m1_lane_free<V_ANTI>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+            DESV_DGROW(-1) DESV_DGROW(0) DESV_DGROW(1) DESV_DGROW(2) DESV_DGROW(3)
+            default: break;
+        }
     }
 }
+#undef DESV_M1U
+#undef DESV_M1C
+#undef DESV_DG
+#undef DESV_DGROW
 
 // Thread's tile-local index with zeros at the 4 register bits g[0..3] (ascending).
 __device__ __forceinline__ uint32_t stage_base(uint32_t t, const uint8_t *g) {

@@ -24,7 +24,7 @@ F_REAL, F_DIAG, F_PHASE1, F_ANTI, F_SIGN, F_PARAM = 1, 2, 4, 8, 16, 32
 # numpy mirrors of the packed C structs (little-endian, no implicit padding)
 OP_DTYPE = np.dtype([
     ('kind', 'u1'), ('flags', 'u1'), ('s0', 'i1'), ('s1', 'i1'), ('cslot', 'i1'),
-    ('ga', 'u1'), ('gb', 'u1'), ('sa', 'i1'), ('sb', 'i1'), ('g', 'u1', (4,)), ('pad0', 'u1', (3,)),
+    ('ga', 'u1'), ('gb', 'u1'), ('sa', 'i1'), ('sb', 'i1'), ('g', 'u1', (4,)), ('code', '<u2'), ('pad0', 'u1'),
     ('mat', '<u4'), ('param', '<i4'), ('cmask', '<u8'), ('cval', '<u8')])
 assert OP_DTYPE.itemsize == 40
 PASS_DTYPE = np.dtype([('tile_bits', '<i4'), ('low_bits', '<i4'), ('op_begin', '<i4'), ('op_end', '<i4'),
@@ -59,6 +59,8 @@ _SIGS = {
     'desv_pauli_matvec': ([_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _sz, _vp], _i),
     'desv_pauli_expect_noalloc': ([_vp, _i, _i, _vp, _i, _vp, _vp, _vp], _i),
     'desv_adjoint_scratch_bytes': ([_i], _sz),
+    'desv_batch_workspace_bytes': ([_i, _i, _i], _sz),
+    'desv_batch_vqe': ([_i, _i, _i, _vp, _vp, _sz, _vp], _i),
     'desv_adjoint_passes': ([_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp], _i),
 }
 OPTIONAL = set()

@@ -1,0 +1,317 @@
+"""Batched VQE: energy and adjoint gradient of many independent circuits of
+uneven qubit count in one persistent GPU launch (``desv_batch_vqe``), optionally
+replayed from a captured CUDA graph.
+
+The reference evaluates one parameter row of one circuit shape at a time
+(``run_batch_jit`` vmaps a single structure at a single qubit count,
+``backends/statevector.py:496-584``; gradients come from ``jax.grad`` per
+circuit, ``solvers/autodiff.py:92-169``).  Here:
+
+* circuits sharing a structure (gate list + Pauli term structure) share one
+  plan -- forward fused passes and adjoint fused passes from the same fusion
+  pass as single circuits (1-qubit gates unmerged so that every op's matrix
+  can be rebuilt from theta on the device);
+* each circuit brings its theta and its real term coefficients (e.g. its own
+  J_z of an XXZ chain);
+* circuits are ordered by decreasing cost and pulled from an atomic queue, one
+  per CTA; states of <= 12 qubits never leave shared memory.
+
+Parameters are injected like the energy functions: into rx/ry/rz/u1/p/cp/crz
+in gate order (``solvers/autodiff.py:21,150-157``).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .circuits import fusion
+from .physics.observables import _normalize_terms
+from .solvers import adjoint
+from .solvers.autodiff import build_template
+
+RESIDENT_BITS = 12
+
+RCP = dict(CONST=0, RX=1, RY=2, RZ=3, P=4, RZ_TAB=5, P_TAB=6, CP_VEC=7, CRZ_VEC=8, PHASE_VEC=9)
+RCP_INVERSE = 0x100
+
+RECIPE_DTYPE = np.dtype([('off', '<u4'), ('param', '<i4'), ('kind', '<u2'), ('count', '<u2'), ('src', '<u4')])
+PLAN_DTYPE = np.dtype([(k, '<i4') for k in ('n', 'fwd_begin', 'fwd_end', 'bwd_begin', 'bwd_end', 'rec_begin',
+                                            'rec_end', 'term_begin', 'term_end', 'nparams', 'pool_len', 'pad')])
+CIRC_DTYPE = np.dtype([('plan', '<i4'), ('out_index', '<i4'), ('theta_off', '<i8'), ('coef_off', '<i8'),
+                       ('grad_off', '<i8')])
+assert RECIPE_DTYPE.itemsize == 16 and PLAN_DTYPE.itemsize == 48 and CIRC_DTYPE.itemsize == 32
+
+
+class BatchArgs(ctypes.Structure):
+    """ctypes mirror of desv_batch_args (include/desv.h)."""
+    _fields_ = [('ncirc', ctypes.c_int32), ('pad', ctypes.c_int32), ('circuits', ctypes.c_void_p),
+                ('plans', ctypes.c_void_p), ('passes', ctypes.c_void_p), ('ops', ctypes.c_void_p),
+                ('recipes', ctypes.c_void_p), ('cpool', ctypes.c_void_p), ('theta', ctypes.c_void_p),
+                ('coef', ctypes.c_void_p), ('terms', ctypes.c_void_p), ('energy', ctypes.c_void_p),
+                ('grad', ctypes.c_void_p), ('workspace', ctypes.c_void_p), ('ws_amps', ctypes.c_uint64),
+                ('pool_ws', ctypes.c_void_p), ('pool_stride_bytes', ctypes.c_uint64)]
+
+
+def _term_structure(terms, n):
+    """[(xmask, zmask, i^nY)] and real coefficients of a Pauli term list."""
+    st, coef = [], []
+    for c, p in terms:
+        t = _normalize_terms(p, None)
+        if t and max(t) >= n:
+            raise ValueError(f"term references qubit {max(t)}, but the circuit has {n} qubits")
+        x = z = ny = 0
+        for q, l in t.items():
+            b = 1 << (n - 1 - q)
+            if l in ('X', 'Y'):
+                x |= b
+            if l in ('Y', 'Z'):
+                z |= b
+            ny += l == 'Y'
+        ph = 1j ** ny
+        if complex(c).imag != 0:
+            raise ValueError('batched VQE takes real term coefficients')
+        st.append((x, z, ph.real, ph.imag))
+        coef.append(float(np.real(c)))
+    return tuple(st), coef
+
+
+class _Plan:
+    """Forward + adjoint passes and matrix recipes of one circuit structure."""
+
+    def __init__(self, rows, slots, n, term_struct, dtype, tile_bits=None):
+        if n < fusion.MIN_FUSED_QUBITS:
+            raise ValueError(f'batched VQE needs at least {fusion.MIN_FUSED_QUBITS} qubits per circuit')
+        self.n = n
+        self.nparams = 1 + max([s for s in slots if s >= 0], default=-1)
+        K = min(n, tile_bits or RESIDENT_BITS)
+        self.K = K
+        ir = fusion.lower(rows, n, slots)
+        fops = fusion.fuse_1q(ir, merge=False)
+        self.fwd = fusion.Packed(n, fops, fusion.schedule(fops, n, K))
+        bops = adjoint.backward_ops(ir)
+        self.bwd = fusion.Packed(n, bops, adjoint._split_params(fusion.schedule(bops, n, K), bops, 4096),
+                                 adjoint=True)
+        for p in list(self.fwd.passes) + list(self.bwd.passes):
+            if int(p['tile_bits']) != (n if n <= RESIDENT_BITS else K):
+                raise RuntimeError('batched plan: unexpected tile geometry')
+        cdt = np.complex64 if dtype == torch.complex64 else np.complex128
+        th0 = 0.37 + 0.0137 * np.arange(max(self.nparams, 1))   # generic angles: flags valid for every theta
+        fpool = self.fwd.materialize(th0, cdt)
+        bpool = self.bwd.materialize(th0, cdt)
+        self.fwd_len = len(fpool)
+        self.pool_len = len(fpool) + len(bpool)
+        self.cpool = np.concatenate([fpool, bpool])
+        # adjoint records: GRAD param -> theta index, matrices after the forward pool
+        bops_arr = self.bwd.ops
+        for ps in self.bwd.passes:
+            for r in range(int(ps['op_begin']), int(ps['op_end'])):
+                if bops_arr[r]['kind'] == N.OP_GRAD:
+                    bops_arr[r]['param'] = self.bwd.param_map[int(ps['map_begin']) + int(bops_arr[r]['param'])]
+        is_rec = bops_arr['kind'] != N.OP_STAGE
+        bops_arr['mat'][is_rec] += self.fwd_len
+        self.recipes = np.concatenate([self._recipes(self.fwd, 0), self._recipes(self.bwd, self.fwd_len)])
+        self.term_struct = term_struct
+
+    @staticmethod
+    def _recipes(packed, base):
+        V = packed._vec
+        out = np.zeros(V['R'], RECIPE_DTYPE)
+        for r, (rec_i, fi) in enumerate(packed.op_slots):
+            op = packed.fops[fi]
+            g = op.src[0]
+            kind_out, tf = int(V['out'][r]), int(V['tf'][r])
+            off = int(V['off'][r])
+            count = 16 if kind_out == 3 else 4
+            out[r]['off'] = base + off
+            out[r]['src'] = base + off
+            out[r]['count'] = count
+            out[r]['param'] = -1
+            if tf == 2 or g.slot < 0 or len(op.src) != 1:
+                out[r]['kind'] = RCP['CONST']
+                continue
+            name = g.name
+            if kind_out == 0:
+                k = {'rx': 'RX', 'ry': 'RY', 'rz': 'RZ', 'p': 'P', 'u1': 'P', 'phase': 'P'}[name]
+            elif kind_out == 1:
+                if int(V['ctl'][r]) != -1:
+                    raise RuntimeError('batched plan: controlled parametric diagonal')
+                k = {'rz': 'RZ_TAB', 'p': 'P_TAB', 'u1': 'P_TAB', 'phase': 'P_TAB'}[name]
+            elif kind_out == 2:
+                k = {'cp': 'CP_VEC', 'cphase': 'CP_VEC', 'crz': 'CRZ_VEC', 'gphase': 'PHASE_VEC'}[name]
+            else:
+                raise RuntimeError('batched plan: parametric dense 4x4')
+            out[r]['kind'] = RCP[k] | (RCP_INVERSE if tf == 1 else 0)
+            out[r]['param'] = g.slot
+        return out
+
+    @property
+    def cost(self):
+        return (1 << self.n) * (len(self.fwd.ops) + 2 * len(self.bwd.ops))
+
+
+class BatchVQE:
+    """Energies and adjoint gradients of many circuits in one launch.
+
+    items: sequence of (circuit, n_qubits, terms) -- circuit as gate tuples or
+    a QASMCircuit (parameters are ignored; theta is injected in gate order),
+    terms as (real coefficient, Pauli term) pairs.  Circuits whose gate list
+    and term structure coincide share a plan."""
+
+    def __init__(self, items: Sequence[Tuple], use_float32: bool = True, tile_bits=None):
+        self.dtype = torch.complex64 if use_float32 else torch.complex128
+        self.device = N.require_cuda()
+        N.lib()
+        plans: Dict[tuple, int] = {}
+        self.plans: List[_Plan] = []
+        self.circ = []          # (plan index, coefficients, nparams)
+        for circuit, n, terms in items:
+            rows, slots, n_params = build_template(circuit, n)
+            ts, coef = _term_structure(terms, n)
+            key = (tuple(rows), tuple(slots), n, ts)
+            if key not in plans:
+                plans[key] = len(self.plans)
+                self.plans.append(_Plan(rows, slots, n, ts, self.dtype, tile_bits))
+            self.circ.append((plans[key], coef, n_params))
+        self._pack()
+
+    def _pack(self):
+        pass_rows, op_rows, rec_rows, term_rows, plan_rows, cpools = [], [], [], [], [], []
+        nops = npass = nrec = nterm = ncp = 0
+        for p in self.plans:
+            prow = np.zeros((), PLAN_DTYPE)
+            prow['n'] = p.n
+            fwd = p.fwd.passes.copy()
+            bwd = np.zeros(len(p.bwd.passes), N.PASS_DTYPE)
+            for f in ('tile_bits', 'low_bits', 'op_begin', 'op_end', 'high'):
+                bwd[f] = p.bwd.passes[f]
+            fwd['op_begin'] += nops
+            fwd['op_end'] += nops
+            nf = len(p.fwd.ops)
+            bwd['op_begin'] += nops + nf
+            bwd['op_end'] += nops + nf
+            prow['fwd_begin'], prow['fwd_end'] = npass, npass + len(fwd)
+            prow['bwd_begin'], prow['bwd_end'] = npass + len(fwd), npass + len(fwd) + len(bwd)
+            pass_rows += [fwd, bwd]
+            npass += len(fwd) + len(bwd)
+            op_rows += [p.fwd.ops, p.bwd.ops]
+            nops += nf + len(p.bwd.ops)
+            rec = p.recipes.copy()
+            rec['src'] += ncp
+            rec_rows.append(rec)
+            prow['rec_begin'], prow['rec_end'] = nrec, nrec + len(rec)
+            nrec += len(rec)
+            cpools.append(p.cpool)
+            ncp += len(p.cpool)
+            prow['term_begin'], prow['term_end'] = nterm, nterm + len(p.term_struct)
+            term_rows += list(p.term_struct)
+            nterm += len(p.term_struct)
+            prow['nparams'], prow['pool_len'] = p.nparams, p.pool_len
+            plan_rows.append(prow)
+        dev = self.device
+        rdt = np.float32 if self.dtype == torch.complex64 else np.float64
+        cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
+
+        def up(a):
+            return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+
+        self.d_passes = up(np.concatenate(pass_rows))
+        self.d_ops = up(np.concatenate(op_rows))
+        self.d_recipes = up(np.concatenate(rec_rows))
+        self.d_cpool = torch.from_numpy(np.concatenate(cpools).astype(cdt).view(rdt).copy()).to(dev)
+        terms = np.zeros(max(len(term_rows), 1), N.TERM_DTYPE)
+        for i, (x, z, cr, ci) in enumerate(term_rows):
+            terms[i] = (x, z, cr, ci)
+        self.d_terms = up(terms)
+        self.d_plans = up(np.array(plan_rows, PLAN_DTYPE))
+        # circuits in decreasing cost; outputs stay in the caller's order
+        order = sorted(range(len(self.circ)), key=lambda i: -self.plans[self.circ[i][0]].cost)
+        crow = np.zeros(len(self.circ), CIRC_DTYPE)
+        theta_off, coef_off = [], []
+        t = c = 0
+        for i, (pi, coef, npar) in enumerate(self.circ):
+            theta_off.append(t)
+            coef_off.append(c)
+            t += max(npar, self.plans[pi].nparams, 1)
+            c += max(len(coef), 1)
+        self.theta_off = np.array(theta_off)
+        self.ntheta = t
+        coefs = np.zeros(max(c, 1))
+        for i, (pi, coef, npar) in enumerate(self.circ):
+            coefs[coef_off[i]:coef_off[i] + len(coef)] = coef
+        for k, i in enumerate(order):
+            pi = self.circ[i][0]
+            crow[k] = (pi, i, theta_off[i], coef_off[i], theta_off[i])
+        self.d_circ = up(crow)
+        self.d_coef = torch.from_numpy(coefs).to(dev)
+        self.d_theta = torch.zeros(max(t, 1), dtype=torch.float64, device=dev)
+        self.d_energy = torch.zeros(len(self.circ), dtype=torch.float64, device=dev)
+        self.d_grad = torch.zeros(max(t, 1), dtype=torch.float64, device=dev)
+        self.max_n = max(p.n for p in self.plans)
+        self.max_pool = max(p.pool_len for p in self.plans)
+        code = N.DESV_C64 if self.dtype == torch.complex64 else N.DESV_C128
+        self.code = code
+        wsb = int(N.lib().desv_batch_workspace_bytes(code, max(self.max_n, 9), self.max_pool))
+        self.d_ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        a = BatchArgs()
+        a.ncirc = len(self.circ)
+        for f, t_ in (('circuits', self.d_circ), ('plans', self.d_plans), ('passes', self.d_passes),
+                      ('ops', self.d_ops), ('recipes', self.d_recipes), ('cpool', self.d_cpool),
+                      ('theta', self.d_theta), ('coef', self.d_coef), ('terms', self.d_terms),
+                      ('energy', self.d_energy), ('grad', self.d_grad)):
+            setattr(a, f, t_.data_ptr())
+        self.args = a
+        self.graph = None
+
+    # ------------------------------------------------------------------ run
+    def set_theta(self, thetas: Sequence[np.ndarray]):
+        """Copy every circuit's parameters (gate order) into the device buffer."""
+        host = np.zeros(self.ntheta)
+        for i, th in enumerate(thetas):
+            th = np.asarray(th, dtype=np.float64).reshape(-1)
+            host[self.theta_off[i]:self.theta_off[i] + th.size] = th
+        self.d_theta.copy_(torch.from_numpy(host))
+
+    def launch(self, stream=None):
+        st = ctypes.c_void_p(N.stream_ptr(stream))
+        N.check(N.lib().desv_batch_vqe(self.code, max(self.max_n, 9), self.max_pool, ctypes.byref(self.args),
+                                       ctypes.c_void_p(self.d_ws.data_ptr()), self.d_ws.numel(), st),
+                'batched VQE')
+
+    def capture(self):
+        """Capture the launch in a CUDA graph (after one eager warm-up launch)."""
+        self.launch()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.launch(stream=s)
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = g
+        return g
+
+    def run(self, thetas, use_graph: bool = False):
+        """(energies [ncirc], list of gradients) for the given parameters."""
+        self.set_theta(thetas)
+        if use_graph:
+            if self.graph is None:
+                self.capture()
+            self.graph.replay()
+        else:
+            self.launch()
+        e = self.d_energy.cpu().numpy()
+        g = self.d_grad.cpu().numpy()
+        grads = [g[self.theta_off[i]:self.theta_off[i] + self.circ[i][2]].copy() for i in range(len(self.circ))]
+        return e, grads
+
+
+def hea_xxz_batch(ns: Sequence[int], layers: int, jz: Sequence[float], jxy: float = 1.0):
+    """Items for BatchVQE: hardware-efficient ansatz (RY, RZ per qubit + CX ladder)
+    with an open-chain XXZ Hamiltonian per circuit."""
+    from .workloads import hea_circuit, xxz_terms
+    return [(hea_circuit(n, layers), n, xxz_terms(n, z, jxy)) for n, z in zip(ns, jz)]

@@ -499,45 +499,228 @@ class Packed:
         rec['cmask'], rec['cval'] = cmask, cval
         return rec
 
-    def materialize(self, theta=None, dtype=np.complex64):
-        """Matrix pool and per-op flags for the given parameters."""
-        pool = []
-        ops = self.ops
-        for rec_i, fi in self.op_slots:
+    # ------------------------------------------------------------------ matrices
+    def _prepare(self):
+        """Vectorised recipe of every record's matrix (built once per plan)."""
+        gates, gidx = [], {}
+
+        def gi(g):
+            k = id(g)
+            if k not in gidx:
+                gidx[k] = len(gates)
+                gates.append(g)
+            return gidx[k]
+
+        R = len(self.op_slots)
+        recipes, out, tf, ctl, isgen, gen_m = [], np.zeros(R, np.int8), np.zeros(R, np.int8), \
+            np.full(R, -2, np.int8), np.zeros(R, bool), np.zeros((R, 2, 2), np.complex128)
+        gen_v = np.zeros((R, 4), np.complex128)
+        m2_rec = []
+        off = np.zeros(R, np.int64)
+        pos = 0
+        for r, (rec_i, fi) in enumerate(self.op_slots):
             op = self.fops[fi]
-            m = _clean(op.matrix(theta))
-            ops[rec_i]['mat'] = sum(len(x) for x in pool)
-            if rec_i in self.diag1:
-                # 1-bit diagonal as a table over (target, control): off-control rows are the
-                # identity for gates and zero for generators
-                ctl = self.diag1[rec_i]
-                d = np.array([m[0, 0], m[1, 1]], dtype=np.complex128)
-                off = np.zeros(2) if op.kind == 'g1' else np.ones(2)
-                if ctl is None:
-                    tab = np.concatenate([d, d])
-                elif ctl == 1:
-                    tab = np.concatenate([off, d])
+            kind = op.kind
+            srcs = [gi(g) for g in op.src]
+            recipes.append(srcs)
+            bwd = type(op).__name__ == 'BOp'
+            if kind in ('g1', 'gd'):
+                tf[r] = 2
+                isgen[r] = True
+                m = op.matrix(None)
+                if kind == 'g1':
+                    gen_m[r] = m
                 else:
-                    tab = np.concatenate([d, off])
-                if op.kind == 'm1':
-                    ops[rec_i]['flags'] = N.F_SIGN if (not np.any(tab.imag) and np.all(np.abs(tab.real) == 1)) else 0
-                pool.append(tab.astype(np.complex128))
-            elif op.kind == 'm1':
-                ops[rec_i]['flags'] = _m1_flags(m)
-                pool.append(m.reshape(-1))
-            elif op.kind in ('g1', 'gd'):
-                pool.append(m.reshape(-1))
-            elif op.kind in ('d2', 'scalar'):
-                ops[rec_i]['flags'] = N.F_SIGN if (not np.any(m.imag) and np.all(np.abs(m.real) == 1)) else 0
-                pool.append(m.reshape(-1))
+                    gen_v[r] = m
+            elif bwd:
+                tf[r] = 1
+            if rec_i in self.diag1:
+                out[r] = 1
+                c = self.diag1[rec_i]
+                ctl[r] = -1 if c is None else int(c)
+            elif kind in ('m1', 'g1'):
+                out[r] = 0
+            elif kind in ('d2', 'scalar', 'gd'):
+                out[r] = 2
             else:
-                # kernel row index = 2*bit(s1) + bit(s0); m is indexed 2*bit(t2) + bit(t)
-                if self.m2_swap[rec_i]:
-                    perm = [0, 2, 1, 3]
-                    m = m[np.ix_(perm, perm)]
-                pool.append(m.reshape(-1))
-        mats = np.concatenate(pool).astype(dtype) if pool else np.zeros(4, dtype=dtype)
-        return mats
+                out[r] = 3
+                m2_rec.append(r)
+            off[r] = pos
+            pos += 16 if out[r] == 3 else 4
+            self.ops[rec_i]['mat'] = off[r]
+        D = max([len(x) for x in recipes], default=1) or 1
+        src = np.full((R, D), -1, np.int64)
+        for r, x in enumerate(recipes):
+            src[r, :len(x)] = x
+        G = len(gates)
+        code = np.zeros(G, np.int8)
+        slot = np.full(G, -1, np.int64)
+        value = np.zeros(G)
+        cmat = np.tile(np.eye(2, dtype=np.complex128), (G, 1, 1))
+        cvec = np.ones((G, 4), np.complex128)
+        names = {'rx': 1, 'ry': 2, 'rz': 3, 'p': 4, 'u1': 4, 'phase': 4}
+        for i, g in enumerate(gates):
+            slot[i], value[i] = g.slot, g.value
+            if g.kind == 'scalar':
+                code[i] = 5
+            elif g.kind == 'm1':
+                if g.const is not None:
+                    cmat[i] = g.const
+                else:
+                    code[i] = names[g.name]
+            elif g.kind == 'd2':
+                if g.const is not None:
+                    cvec[i] = g.const
+                else:
+                    code[i] = 11 if g.name in ('cp', 'cphase') else 12
+            else:
+                code[i] = 20   # m2: handled per record
+        self._vec = dict(R=R, D=D, src=src, out=out, tf=tf, ctl=ctl, isgen=isgen, gen_m=gen_m, gen_v=gen_v,
+                         off=off, pool_len=pos, code=code, slot=slot, value=value, cmat=cmat, cvec=cvec,
+                         rec_index=np.array([ri for ri, _ in self.op_slots], np.int64), m2_rec=m2_rec,
+                         gates=gates)
+
+    def materialize(self, theta=None, dtype=np.complex64):
+        """Matrix pool (and per-op flags in self.ops) for the given parameters."""
+        if getattr(self, '_vec', None) is None:
+            self._prepare()
+        V = self._vec
+        R = V['R']
+        if R == 0:
+            return np.zeros(4, dtype=dtype)
+        slot, code = V['slot'], V['code']
+        v = V['value'].copy()
+        if theta is not None:
+            th = np.asarray(theta, dtype=np.float64)
+            has = slot >= 0
+            v[has] = th[slot[has]]
+        # every gate as a 2x2 (1-qubit kinds) and as a 4-vector (diagonal kinds)
+        mat = V['cmat'].copy()
+        vec = V['cvec'].copy()
+        c, s = np.cos(v / 2), np.sin(v / 2)
+        em, ep, e1 = np.exp(-0.5j * v), np.exp(0.5j * v), np.exp(1j * v)
+        k = code == 1
+        mat[k] = np.stack([np.stack([c[k], -1j * s[k]], -1), np.stack([-1j * s[k], c[k]], -1)], -2)
+        k = code == 2
+        mat[k] = np.stack([np.stack([c[k], -s[k]], -1), np.stack([s[k], c[k]], -1)], -2).astype(np.complex128)
+        k = code == 3
+        mat[k] = 0
+        mat[k, 0, 0], mat[k, 1, 1] = em[k], ep[k]
+        k = code == 4
+        mat[k] = 0
+        mat[k, 0, 0], mat[k, 1, 1] = 1.0, e1[k]
+        k = code == 5
+        mat[k] = 0
+        mat[k, 0, 0], mat[k, 1, 1] = e1[k], e1[k]
+        vec[k] = e1[k][:, None]
+        k = code == 11
+        vec[k, 3] = e1[k]
+        k = code == 12
+        vec[k, 1], vec[k, 3] = em[k], ep[k]
+        # record products (in application order: later gates multiply from the left)
+        src = V['src']
+        M = np.tile(np.eye(2, dtype=np.complex128), (R, 1, 1))
+        Vv = np.ones((R, 4), np.complex128)
+        for d in range(V['D']):
+            sel = src[:, d] >= 0
+            if not sel.any():
+                continue
+            ids = src[sel, d]
+            M[sel] = mat[ids] @ M[sel]
+            Vv[sel] = Vv[sel] * vec[ids]
+        tf = V['tf']
+        dag = tf == 1
+        M[dag] = np.conj(np.swapaxes(M[dag], -1, -2))
+        Vv[dag] = np.conj(Vv[dag])
+        gen = tf == 2
+        M[gen] = V['gen_m'][gen]
+        Vv[gen] = V['gen_v'][gen]
+        out = V['out']
+        pool = np.zeros(V['pool_len'], np.complex128)
+        flags = np.zeros(R, np.uint8)
+        # 2x2 records
+        k = out == 0
+        if k.any():
+            m = _clean_batch(M[k].reshape(-1, 4))
+            idx = V['off'][k][:, None] + np.arange(4)
+            pool[idx] = m
+            diag = (m[:, 1] == 0) & (m[:, 2] == 0)
+            f = np.where(diag, N.F_DIAG, 0) | np.where(diag & (m[:, 0] == 1), N.F_PHASE1, 0) | \
+                np.where(~diag & (m[:, 0] == 0) & (m[:, 3] == 0), N.F_ANTI, 0) | \
+                np.where(~np.any(m.imag != 0, axis=1), N.F_REAL, 0)
+            flags[k] = np.where(V['isgen'][k], 0, f)
+        # 1-bit diagonal tables over (target, first control)
+        k = out == 1
+        if k.any():
+            m = _clean_batch(M[k].reshape(-1, 4))
+            d0, d1 = m[:, 0], m[:, 3]
+            offv = np.where(V['isgen'][k], 0.0, 1.0).astype(np.complex128)
+            ctl = V['ctl'][k]
+            tab = np.stack([d0, d1, d0, d1], -1)
+            c1 = ctl == 1
+            tab[c1] = np.stack([offv[c1], offv[c1], d0[c1], d1[c1]], -1)
+            c0 = ctl == 0
+            tab[c0] = np.stack([d0[c0], d1[c0], offv[c0], offv[c0]], -1)
+            pool[V['off'][k][:, None] + np.arange(4)] = tab
+            sign = (~np.any(tab.imag != 0, axis=1)) & np.all(np.abs(tab.real) == 1, axis=1)
+            flags[k] = np.where(V['isgen'][k], 0, np.where(sign, N.F_SIGN, 0))
+        # diagonal records
+        k = out == 2
+        if k.any():
+            m = _clean_batch(Vv[k])
+            pool[V['off'][k][:, None] + np.arange(4)] = m
+            sign = (~np.any(m.imag != 0, axis=1)) & np.all(np.abs(m.real) == 1, axis=1)
+            flags[k] = np.where(V['isgen'][k], 0, np.where(sign, N.F_SIGN, 0))
+        # dense 4x4 records (rare): one by one
+        for r in V['m2_rec']:
+            rec_i, fi = self.op_slots[r]
+            m = _clean(self.fops[fi].matrix(theta))
+            if self.m2_swap[rec_i]:
+                perm = [0, 2, 1, 3]
+                m = m[np.ix_(perm, perm)]
+            pool[V['off'][r]:V['off'][r] + 16] = m.reshape(-1)
+        self.ops['flags'][V['rec_index']] = flags
+        self.ops['code'][V['rec_index']] = self._dispatch_codes(flags)
+        return pool.astype(dtype)
+
+    def _dispatch_codes(self, flags: np.ndarray) -> np.ndarray:
+        """Per-record dispatch codes of the stage interpreter (include/desv.h, desv_op.code)."""
+        recs = self.ops[self._vec['rec_index']]
+        kind = recs['kind'].astype(np.int64)
+        s0 = recs['s0'].astype(np.int64)
+        cs = recs['cslot'].astype(np.int64)
+        sa = recs['sa'].astype(np.int64)
+        sb = recs['sb'].astype(np.int64)
+        pred = recs['cmask'] != 0
+        f = flags.astype(np.int64)
+        var = np.where(f & N.F_PHASE1, 3, np.where(f & N.F_DIAG, 2, np.where(f & N.F_ANTI, 4,
+                                                                        np.where(f & N.F_REAL, 1, 0))))
+        code = np.zeros(len(recs), np.int64)
+        m1 = kind == N.OP_M1
+        lane = m1 & (s0 >= 16)
+        reg = m1 & (s0 < 16)
+        free_lane = lane & ~pred & (cs < 0)
+        code[free_lane] = 53 + var[free_lane]
+        u = reg & (cs < 0)
+        code[u] = 1 + s0[u] * 5 + var[u]
+        c = reg & (cs >= 0)
+        code[c] = 21 + (s0[c] * 4 + cs[c]) * 2 + (var[c] != 4)
+        code[reg & pred] |= 0x8000
+        d = kind == N.OP_DIAG
+        sign = (f & N.F_SIGN) != 0
+        base = np.where(sign, 58, 83)
+        code[d] = base[d] + (sa[d] + 1) * 5 + (sb[d] + 1)
+        code[d & pred] |= 0x8000
+        return code.astype(np.uint16)
+
+
+def _clean_batch(m: np.ndarray) -> np.ndarray:
+    """Zero real / imaginary parts below 1e-15 x max(1, max |entry|) per row."""
+    scale = np.maximum(1.0, np.abs(m).max(axis=1, keepdims=True))
+    re, im = m.real.copy(), m.imag.copy()
+    re[np.abs(re) < 1e-15 * scale] = 0.0
+    im[np.abs(im) < 1e-15 * scale] = 0.0
+    return re + 1j * im
 
 
 def build(target: Sequence[tuple], n: int, kmax: int, slots=None, merge_1q: bool = True):

@@ -67,7 +67,13 @@ typedef struct desv_op {
     uint8_t ga, gb;  /* DIAG: global bit positions (0xFF: absent) */
     int8_t sa, sb;   /* DIAG: register slot holding ga / gb in this stage, -1 if thread-fixed */
     uint8_t g[4];    /* STAGE: tile-local bit positions of register slots 0..3 (ascending, >= 5) */
-    uint8_t pad0[3];
+    uint8_t code[2]; /* host-computed dispatch code, little-endian (0: decode the fields):
+                        1+S*5+V register slot S uncontrolled; 21+(S*4+CS)*2+(V!=ANTI) slot S
+                        controlled by slot CS; 53+V lane bit uncontrolled; 58+(SA+1)*5+(SB+1)
+                        sign-only diagonal; 83+(SA+1)*5+(SB+1) diagonal; |0x8000: cmask/cval
+                        predicate applies.  V: 0 general, 1 real, 2 diagonal, 3 phase-on-|1>,
+                        4 anti-diagonal (same priority as the flags PHASE1 > DIAG > ANTI > REAL) */
+    uint8_t pad0;
     uint32_t mat;    /* first complex element of this op's matrix in the matrix pool */
     int32_t param;   /* adjoint plans: gradient slot of this op (-1: none) */
     uint64_t cmask;  /* thread-level control: apply iff (index & cmask) == cval */
@@ -150,6 +156,75 @@ size_t desv_adjoint_scratch_bytes(int max_params_per_pass);
 int desv_adjoint_passes(void *phi, void *lam, int n, int dtype, const desv_adj_pass *passes, int npasses,
                         const desv_op *ops_dev, const void *mats_dev, const int32_t *map_dev, double *grad_dev,
                         void *scratch, size_t scratch_bytes, void *stream);
+
+/* ---- batched VQE (replaces run_batch_jit's vmap over one circuit shape,
+ *      backends/statevector.py:496-584, plus energy_fn + jax.grad per circuit,
+ *      solvers/autodiff.py:92-169): energy and adjoint gradient of thousands of
+ *      circuits of different qubit counts in one persistent launch. ------------ */
+
+/* recipe kinds: how a record's matrix is made from theta on the device */
+#define DESV_RCP_CONST 0     /* copy `count` complex values from cpool[src] */
+#define DESV_RCP_RX 1        /* 2x2 RX(theta) */
+#define DESV_RCP_RY 2        /* 2x2 RY(theta) */
+#define DESV_RCP_RZ 3        /* 2x2 RZ(theta) */
+#define DESV_RCP_P 4         /* 2x2 diag(1, e^{i theta}) */
+#define DESV_RCP_RZ_TAB 5    /* 1-bit diagonal table of RZ(theta) */
+#define DESV_RCP_P_TAB 6     /* 1-bit diagonal table of P(theta) */
+#define DESV_RCP_CP_VEC 7    /* diagonal (1, 1, 1, e^{i theta}) */
+#define DESV_RCP_CRZ_VEC 8   /* diagonal (1, e^{-i theta/2}, 1, e^{i theta/2}) */
+#define DESV_RCP_PHASE_VEC 9 /* scalar e^{i theta} as a 4-entry diagonal */
+#define DESV_RCP_INVERSE 0x100 /* use -theta (inverse gate) */
+
+typedef struct desv_batch_recipe {
+    uint32_t off;   /* destination in the circuit's pool (complex elements) */
+    int32_t param;  /* theta index within the circuit (-1 for constants) */
+    uint16_t kind;  /* DESV_RCP_* (| DESV_RCP_INVERSE) */
+    uint16_t count; /* complex values written (constants) */
+    uint32_t src;   /* constants: first value in cpool */
+} desv_batch_recipe;
+
+/* one circuit structure: forward passes, adjoint passes, recipes, Hamiltonian terms */
+typedef struct desv_batch_plan {
+    int32_t n;                   /* qubits, 9..34 */
+    int32_t fwd_begin, fwd_end;  /* desv_pass rows of the forward circuit */
+    int32_t bwd_begin, bwd_end;  /* desv_pass rows of the adjoint sweep (GRAD param = theta index) */
+    int32_t rec_begin, rec_end;  /* recipes filling the circuit's pool */
+    int32_t term_begin, term_end;/* Pauli terms (coefficient = cre/cim x the circuit's coef[k]) */
+    int32_t nparams, pool_len, pad;
+} desv_batch_plan;
+
+typedef struct desv_batch_circuit {
+    int32_t plan, out_index;     /* plan row; energy index */
+    int64_t theta_off;           /* first parameter in theta */
+    int64_t coef_off;            /* first term coefficient in coef */
+    int64_t grad_off;            /* first gradient entry in grad */
+} desv_batch_circuit;
+
+/* device pointers of one batch; workspace fields are filled by desv_batch_vqe */
+typedef struct desv_batch_args {
+    int32_t ncirc, pad;
+    const desv_batch_circuit *circuits; /* processed in array order: sort by decreasing cost */
+    const desv_batch_plan *plans;
+    const desv_pass *passes;
+    const desv_op *ops;
+    const desv_batch_recipe *recipes;
+    const void *cpool;                  /* float2 / double2 constants */
+    const double *theta, *coef;
+    const desv_pauli_term *terms;
+    double *energy, *grad;
+    void *workspace;
+    uint64_t ws_amps;
+    void *pool_ws;
+    uint64_t pool_stride_bytes;
+} desv_batch_args;
+
+size_t desv_batch_workspace_bytes(int dtype, int max_n, int max_pool_len);
+/* One persistent launch over every circuit of `args` (host struct of device
+ * pointers).  Circuits of <= 12 qubits run in shared memory; larger ones
+ * stream a per-CTA slice of `workspace`.  Capturable in a CUDA graph after a
+ * first (warm-up) call. */
+int desv_batch_vqe(int dtype, int max_n, int max_pool_len, const desv_batch_args *args, void *workspace,
+                   size_t workspace_bytes, void *stream);
 
 /* ---- reductions (FP64 accumulation; statevector.py:141-147,272-358,599-607,
  *      utils/measurement.py:71-94) ------------------------------------------ */

@@ -60,9 +60,10 @@ def run_passes(sv, n, passes, ops, mats, lam=None, grad=None, param_map=None):
                     v = _grad(a, b, tg, op, g, mats, L, high)
                     grad[param_map[int(ps['map_begin']) + int(op['param'])]] += 2.0 * v
                     continue
-                a = _apply(a, tg, op, g, mats)
+                code = int(op['code'])
+                a = _apply_coded(a, tg, op, g, mats, code) if code else _apply(a, tg, op, g, mats)
                 if b is not None:
-                    b = _apply(b, tg, op, g, mats)
+                    b = _apply_coded(b, tg, op, g, mats, code) if code else _apply(b, tg, op, g, mats)
             k += 1 + cnt
         sv[gi] = a
         if lam is not None:
@@ -150,3 +151,59 @@ def _grad(a, b, gi, op, g, mats, L, high):
         if cs >= 0:
             pred = pred & (((j >> g[cs]) & 1)[None, :] == 1)
     return float(np.real(np.sum(np.where(pred, np.conj(b) * ga_, 0))))
+
+
+def _variant_pair(m, var, x0, x1):
+    """The kernel's per-variant 2x2 formulas (a wrong variant gives a wrong result here too)."""
+    if var == 2:                      # diagonal
+        return m[0, 0] * x0, m[1, 1] * x1
+    if var == 3:                      # phase on |1>
+        return x0, m[1, 1] * x1
+    if var == 4:                      # anti-diagonal
+        return m[0, 1] * x1, m[1, 0] * x0
+    if var == 1:                      # real
+        return m[0, 0].real * x0 + m[0, 1].real * x1, m[1, 0].real * x0 + m[1, 1].real * x1
+    return m[0, 0] * x0 + m[0, 1] * x1, m[1, 0] * x0 + m[1, 1] * x1
+
+
+def _apply_coded(a, tg, op, g, mats, code):
+    """Follow the dispatch code exactly as the kernel's switch does."""
+    m0 = int(op['mat'])
+    pred = _pred(tg, op, g) if code & 0x8000 else np.ones_like(tg, dtype=bool)
+    c = code & 0x7FFF
+    j = np.arange(a.shape[1])
+    if 1 <= c <= 57:
+        m = mats[m0:m0 + 4].reshape(2, 2)
+        if c <= 20:
+            S, var, cs = (c - 1) // 5, (c - 1) % 5, -1
+            tl = g[S]
+        elif c <= 52:
+            k = c - 21
+            var = 4 if k % 2 == 0 else 0
+            S, cs = (k // 2) // 4, (k // 2) % 4
+            tl = g[S]
+        else:
+            var, cs = c - 53, -1
+            tl = int(op['s0']) - 16
+        bit = (j >> tl) & 1
+        lo = j[bit == 0]
+        hi = lo | (1 << tl)
+        n0, n1 = _variant_pair(m, var, a[:, lo], a[:, hi])
+        out = a.copy()
+        out[:, lo], out[:, hi] = n0, n1
+        ok = pred
+        if cs >= 0:
+            ok = ok & (((j >> g[cs]) & 1)[None, :] == 1)
+        return np.where(ok, out, a)
+    if 58 <= c <= 107:
+        sign = c < 83
+        k = c - (58 if sign else 83)
+        SA, SB = k // 5 - 1, k % 5 - 1
+        d = mats[m0:m0 + 4]
+        ba = ((j >> g[SA]) & 1)[None, :] if SA >= 0 else (_bit(tg, int(op['ga'])) if int(op['ga']) != 0xFF else 0)
+        bb = ((j >> g[SB]) & 1)[None, :] if SB >= 0 else (_bit(tg, int(op['gb'])) if int(op['gb']) != 0xFF else 0)
+        f = d[ba + 2 * bb]
+        if sign:
+            f = np.where(np.real(f) < 0, -1.0, 1.0)
+        return np.where(pred, a * f, a)
+    raise AssertionError(f'unknown dispatch code {code}')

@@ -1,0 +1,54 @@
+"""Batched VQE (one persistent launch over circuits of different qubit counts)
+against the single-circuit adjoint path and the oracle."""
+import numpy as np
+import pytest
+
+from oracle import sv_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize('f32', [False, True])
+def test_batch_matches_single_circuit_adjoint(f32):
+    import dense_evolution as de
+    from dense_evolution.batch import BatchVQE, hea_xxz_batch
+    rng = np.random.default_rng(3)
+    ns = [9, 14, 10, 12, 13, 9, 11]
+    jz = rng.uniform(0.5, 1.5, len(ns))
+    items = hea_xxz_batch(ns, 2, jz)
+    b = BatchVQE(items, use_float32=f32)
+    thetas = [rng.uniform(-np.pi, np.pi, 2 * n * 2) for n in ns]
+    e, g = b.run(thetas)
+    for i, (circ, n, terms) in enumerate(items):
+        fn, npar = de.circuit_to_energy_fn(circ, n, use_float32=f32)
+        e1, g1, _ = fn.program.value_and_grad(thetas[i], terms)
+        tol = 1e-5 if f32 else 1e-10
+        assert e[i] == pytest.approx(e1, abs=tol)
+        assert np.allclose(g[i], g1, atol=tol)
+    # oracle for the two smallest
+    for i in (0, 5):
+        circ, n, terms = items[i]
+        rows, _ = O.energy_template([{'name': c[0], 'qubits': [q for q in c[1:] if isinstance(q, int)]}
+                                     for c in circ], n)
+        e_ref, _ = O.energy(thetas[i], rows, n, terms)
+        assert e[i] == pytest.approx(e_ref, abs=1e-5 if f32 else 1e-10)
+        fd = O.fd_gradient(thetas[i], rows, n, terms, h=1e-5, indices=[0, 7, 20])
+        assert np.allclose(g[i][[0, 7, 20]], fd, atol=1e-4 if f32 else 1e-7)
+    from dense_evolution import _native as N
+    N.device_status()
+
+
+def test_batch_cuda_graph_replay():
+    from dense_evolution.batch import BatchVQE, hea_xxz_batch
+    rng = np.random.default_rng(5)
+    ns = [10, 13, 12, 9]
+    b = BatchVQE(hea_xxz_batch(ns, 3, rng.uniform(0.5, 1.5, len(ns))))
+    th = [rng.uniform(-np.pi, np.pi, 6 * n) for n in ns]
+    e0, g0 = b.run(th)
+    e1, g1 = b.run(th, use_graph=True)
+    th2 = [t + 0.1 for t in th]
+    e2, g2 = b.run(th2, use_graph=True)
+    e3, g3 = b.run(th2)
+    assert np.allclose(e0, e1) and all(np.allclose(x, y) for x, y in zip(g0, g1))
+    assert np.allclose(e2, e3) and all(np.allclose(x, y) for x, y in zip(g2, g3))
+    assert not np.allclose(e0, e2)
