@@ -278,11 +278,15 @@ def run_ours(args):
     e2e_step = _max_over_ranks(float(np.mean(e2e_times)), ws)
     e2e_passes = npasses
     e2e_value = ws * e2e_passes * pass_bytes / e2e_step / 1e9
-    del sim
-    torch.cuda.empty_cache()
 
+    del sv, sim, ops_t, mats_t
+    torch.cuda.empty_cache()
     vqe = run_vqe(args) if not args.skip_vqe else None
+    torch.cuda.empty_cache()
     batch = run_batch(args) if not args.skip_batch else None
+    torch.cuda.empty_cache()
+    large = run_large(args) if not args.skip_large else None
+    torch.cuda.empty_cache()
     cpu = cpu_baseline() if (rank == 0 and ws == 1 and not args.skip_cpu) else None
     if rank == 0:
         line = {
@@ -309,6 +313,7 @@ def run_ours(args):
             'cpu_baseline': cpu,
             'vqe': vqe,
             'batch': batch,
+            'large': large,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -389,6 +394,48 @@ def run_batch(args, ncirc=4096, layers=6):
             'plan_build_s': build_s, 'energy_mean': float(np.mean(e))}
 
 
+def run_large(args, n=32, n_ref=30, layers=4):
+    """Config 5: 32-qubit complex64 adjoint gradient (psi, lambda, mu: 3 x 32 GiB), HEA 4 layers
+    (256 parameters), Heisenberg XXX open chain; accuracy from the same structure at 30 qubits,
+    complex64 against complex128."""
+    import torch
+    import dense_evolution as de
+    from dense_evolution.workloads import hea_circuit, xxx_terms
+    out = {'workload': f'{n}-qubit complex64 HEA {layers} layers, XXX open chain; adjoint gradient'}
+    free = torch.cuda.mem_get_info()[0]
+    if free < 3.2 * (1 << n) * 8:
+        out['skipped'] = f'needs {3 * (1 << n) * 8 / 2**30:.0f} GiB of free HBM, {free / 2**30:.0f} GiB free'
+        return out
+    fn, npar = de.circuit_to_energy_fn(hea_circuit(n, layers), n, use_float32=True)
+    op = de.PauliSumOperator(xxx_terms(n), n)
+    theta = np.random.default_rng(SEED).uniform(-np.pi, np.pi, npar)
+    e, g, psi = fn.program.value_and_grad(theta, op)       # warm-up (plans, scratch)
+    del psi
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e, g, psi = fn.program.value_and_grad(theta, op)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    peak = torch.cuda.max_memory_allocated() / 2**30
+    del psi
+    torch.cuda.empty_cache()
+    out.update({'energy': e, 'grad_norm': float(np.linalg.norm(g)), 'seconds_per_gradient': dt,
+                'grads_per_s': 1.0 / dt, 'params': npar, 'peak_hbm_gib': peak,
+                'forward_passes': len(fn.program.forward.packed.passes), 'backward_passes': len(fn.program.back.passes)})
+    # accuracy of complex64 against complex128, same structure at 30 qubits
+    th = np.random.default_rng(SEED).uniform(-np.pi, np.pi, 2 * n_ref * layers)
+    r = {}
+    for f32 in (True, False):
+        f, _ = de.circuit_to_energy_fn(hea_circuit(n_ref, layers), n_ref, use_float32=f32)
+        ee, gg, pp = f.program.value_and_grad(th, de.PauliSumOperator(xxx_terms(n_ref), n_ref))
+        r[f32] = (ee, gg)
+        del pp
+        torch.cuda.empty_cache()
+    out.update({'ref_qubits': n_ref, 'abs_energy_error_c64_vs_c128': abs(r[True][0] - r[False][0]),
+                'max_abs_grad_error_c64_vs_c128': float(np.max(np.abs(r[True][1] - r[False][1])))})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -398,6 +445,7 @@ def main():
     ap.add_argument('--skip-vqe', action='store_true')
     ap.add_argument('--skip-cpu', action='store_true')
     ap.add_argument('--skip-batch', action='store_true')
+    ap.add_argument('--skip-large', action='store_true')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

@@ -56,8 +56,8 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, T
                     v = warp_sum_d(v);
                     if (lane == 0) acc[warp * nparams + op.param] += v;
                 } else {
-                    apply_one_op(a, op, mats, tg, lane);
-                    apply_one_op(b, op, mats, tg, lane);
+                    apply_op_at(a, ops + k + q, mats, tg, lane);
+                    apply_op_at(b, ops + k + q, mats, tg, lane);
                 }
             }
 #pragma unroll
@@ -111,18 +111,21 @@ template <typename T, int K, int NBUF> static size_t adj_smem(int nparams) {
 template <typename T, int K, int NBUF>
 static int launch_adj(T *phi, T *lam, const TileGeom &g, const desv_op *ops, int nops, const T *mats, int nparams,
                       double *part, int *grid_out, cudaStream_t st) {
-    static int bps[64] = {0};
+    static bool attr[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     const size_t smax = adj_smem<T, K, NBUF>(ADJ_MAX_PARAMS);
-    if (bps[dev & 63] == 0) {
+    if (!attr[dev & 63]) {
         cudaFuncSetAttribute(k_adjoint_pass<T, K, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
-        int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_adjoint_pass<T, K, NBUF>, 1 << (K - 4), smax);
-        bps[dev & 63] = b > 0 ? b : 1;
+        attr[dev & 63] = true;
     }
+    // resident CTAs for the shared memory this launch really uses
+    int bps = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_adjoint_pass<T, K, NBUF>, 1 << (K - 4),
+                                                  adj_smem<T, K, NBUF>(nparams));
+    if (bps < 1) bps = 1;
     const uint64_t ntiles = 1ull << (g.n - K);
-    uint64_t cap = (uint64_t)sm_count() * bps[dev & 63];
+    uint64_t cap = (uint64_t)sm_count() * bps;
     if (cap > ADJ_MAX_ROWS) cap = ADJ_MAX_ROWS;
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     *grid_out = grid;
@@ -140,7 +143,7 @@ int adjoint_pass(void *phi, void *lam, int dtype, const TileGeom &g, const desv_
         switch (g.K) {
             case 9: return launch_adj<float2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
             case 10: return launch_adj<float2, 10, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
-            case 11: return launch_adj<float2, 11, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+            case 11: return launch_adj<float2, 11, 3>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
             default: return fail(DESV_EINVAL, "adjoint pass: complex64 tile_bits must be 9..11");
         }
     }
@@ -148,7 +151,7 @@ int adjoint_pass(void *phi, void *lam, int dtype, const TileGeom &g, const desv_
     const double2 *m = static_cast<const double2 *>(mats);
     switch (g.K) {
         case 9: return launch_adj<double2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
-        case 10: return launch_adj<double2, 10, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+        case 10: return launch_adj<double2, 10, 3>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
         default: return fail(DESV_EINVAL, "adjoint pass: complex128 tile_bits must be 9..10");
     }
 }

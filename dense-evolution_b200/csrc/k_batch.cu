@@ -211,20 +211,19 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_vqe(desv_batch_args arg
         // 3. lambda = H psi, E = <psi|lambda>
         double ere = 0;
         for (uint64_t i = tid; i < dim; i += blockDim.x) {
-            T v = cpx<T>(0, 0);
+            double2 v = make_double2(0.0, 0.0);
             for (int k = pl.term_begin; k < pl.term_end; ++k) {
                 const desv_pauli_term tm = args.terms[k];
                 const uint64_t src = i ^ tm.xmask;
                 const T pz = gpsi[src];
-                const double cr = tm.cre * args.coef[cd.coef_off + (k - pl.term_begin)];
-                const double ci = tm.cim * args.coef[cd.coef_off + (k - pl.term_begin)];
-                T cc = cpx<T>(cr, ci);
+                const double w = args.coef[cd.coef_off + (k - pl.term_begin)];
+                double2 cc = make_double2(tm.cre * w, tm.cim * w);
                 if (__popcll(src & tm.zmask) & 1) cc = cneg(cc);
-                v = cfma(cc, pz, v);
+                v = cfma(cc, make_double2((double)pz.x, (double)pz.y), v);
             }
-            glam[i] = v;
+            glam[i] = cpx<T>(v.x, v.y);
             const T a = gpsi[i];
-            ere += (double)a.x * (double)v.x + (double)a.y * (double)v.y;
+            ere += (double)a.x * v.x + (double)a.y * v.y;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) ere += __shfl_xor_sync(0xffffffffu, ere, o);

@@ -6,8 +6,9 @@
 // tile passes: every term whose flip mask lies inside a pass's tile bits is
 // evaluated from the shared-memory tile, so all terms of a pass cost one read
 // of psi.  (P_k psi)[i] = psi[i ^ x_k] * c_k * (-1)^popcount((i ^ x_k) & z_k),
-// where c_k already carries the i^(#Y) factor.  Per amplitude the term sum is
-// formed in the state's precision; the expectation is accumulated in FP64.
+// where c_k already carries the i^(#Y) factor.  The per-amplitude term sum and
+// the expectation are accumulated in FP64 (only H psi is stored in the state's
+// precision).
 #include "desv_common.cuh"
 #include "tile_pipeline.cuh"
 
@@ -19,7 +20,7 @@ constexpr int PAULI_MAX_TERMS = 512;
 template <typename T> struct TermTab {
     uint32_t xl[PAULI_MAX_TERMS];
     uint32_t zl[PAULI_MAX_TERMS];
-    T c[PAULI_MAX_TERMS];
+    double2 c[PAULI_MAX_TERMS];
     uint8_t pb[PAULI_MAX_TERMS];
 };
 
@@ -41,10 +42,7 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
         const desv_pauli_term tm = terms[k];
         tab->xl[k] = global_to_tile_local(g, tm.xmask);
         tab->zl[k] = global_to_tile_local(g, tm.zmask);
-        T c;
-        c.x = (decltype(c.x))tm.cre;
-        c.y = (decltype(c.y))tm.cim;
-        tab->c[k] = c;
+        tab->c[k] = make_double2(tm.cre, tm.cim);
     }
     PipeArrays<T, NARR> A;
     A.ptr[0] = const_cast<T *>(psi);
@@ -64,30 +62,31 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
         const T *s = sp[0];
 #pragma unroll 1
         for (uint32_t j = threadIdx.x; j < (1u << K); j += PAULI_THREADS) {
-            T v = mk(decltype(s[0].x)(0), decltype(s[0].x)(0));
+            double2 v = make_double2(0.0, 0.0);
             uint32_t last_x = 0xFFFFFFFFu;
-            T p = s[j];
+            double2 p = make_double2(0.0, 0.0);
 #pragma unroll 4
             for (int k = 0; k < nterms; ++k) {
                 const uint32_t xl = tab->xl[k];
                 if (xl != last_x) {
-                    p = s[j ^ xl];
+                    const T q = s[j ^ xl];
+                    p = make_double2((double)q.x, (double)q.y);
                     last_x = xl;
                 }
                 const int sg = (__popc((j ^ xl) & tab->zl[k]) ^ tab->pb[k]) & 1;
-                const T c = tab->c[k];
+                const double2 c = tab->c[k];
                 v = sg ? cfma(cneg(c), p, v) : cfma(c, p, v);
             }
             if (MODE != 0 || want_e) {
                 const T a = s[j];
-                ere += (double)a.x * (double)v.x + (double)a.y * (double)v.y;
-                eim += (double)a.x * (double)v.y - (double)a.y * (double)v.x;
+                ere += (double)a.x * v.x + (double)a.y * v.y;
+                eim += (double)a.x * v.y - (double)a.y * v.x;
             }
-            if (MODE == 1) sp[NARR - 1][j] = v;
+            if (MODE == 1) sp[NARR - 1][j] = mk((decltype(s[0].x))v.x, (decltype(s[0].x))v.y);
             if (MODE == 2) {
                 T o = sp[NARR - 1][j];
-                o.x += v.x;
-                o.y += v.y;
+                o.x = (decltype(o.x))((double)o.x + v.x);
+                o.y = (decltype(o.y))((double)o.y + v.y);
                 sp[NARR - 1][j] = o;
             }
         }
@@ -153,26 +152,25 @@ __global__ void __launch_bounds__(256) k_pauli_direct(const T *psi, T *out, uint
                                                       double *part) {
     double ere = 0, eim = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
-        T v = mk(decltype(psi[0].x)(0), decltype(psi[0].x)(0));
+        double2 v = make_double2(0.0, 0.0);
         for (int k = 0; k < nterms; ++k) {
             const desv_pauli_term tm = terms[k];
             const uint64_t src = i ^ tm.xmask;
-            const T p = psi[src];
-            T c;
-            c.x = (decltype(c.x))tm.cre;
-            c.y = (decltype(c.y))tm.cim;
+            const T q = psi[src];
+            const double2 p = make_double2((double)q.x, (double)q.y);
+            const double2 c = make_double2(tm.cre, tm.cim);
             v = (__popcll(src & tm.zmask) & 1) ? cfma(cneg(c), p, v) : cfma(c, p, v);
         }
         if (want_e) {
             const T a = psi[i];
-            ere += (double)a.x * (double)v.x + (double)a.y * (double)v.y;
-            eim += (double)a.x * (double)v.y - (double)a.y * (double)v.x;
+            ere += (double)a.x * v.x + (double)a.y * v.y;
+            eim += (double)a.x * v.y - (double)a.y * v.x;
         }
-        if (MODE == 1) out[i] = v;
+        if (MODE == 1) out[i] = mk((decltype(psi[0].x))v.x, (decltype(psi[0].x))v.y);
         if (MODE == 2) {
             T o = out[i];
-            o.x += v.x;
-            o.y += v.y;
+            o.x = (decltype(o.x))((double)o.x + v.x);
+            o.y = (decltype(o.y))((double)o.y + v.y);
             out[i] = o;
         }
     }

@@ -318,44 +318,47 @@ __device__ __forceinline__ void diag_case(T (&a)[16], const T *mp, uint32_t w0y,
     case 83 + (SA + 1) * 5 + (SB + 1): diag_case<SA, SB>(a, mp, w0y, tg, false); break;
 #define DESV_DGROW(SA) DESV_DG(SA, -1) DESV_DG(SA, 0) DESV_DG(SA, 1) DESV_DG(SA, 2) DESV_DG(SA, 3)
 
+// Apply the op at `opp` (dispatch code or field decode) to the thread's registers.
+template <typename T>
+__device__ __forceinline__ void apply_op_at(T (&a)[16], const desv_op *opp, const T *mats, uint64_t tg, int lane) {
+    // desv_op is 40 bytes: records are only 8-byte aligned, so read bytes
+    // 0..15 as two 8-byte words (a 16-byte load would be misaligned for odd k)
+    const uint2 wlo = reinterpret_cast<const uint2 *>(opp)[0];
+    const uint2 whi = reinterpret_cast<const uint2 *>(opp)[1];
+    const uint4 w0 = make_uint4(wlo.x, wlo.y, whi.x, whi.y);
+    const uint32_t code = (w0.w >> 8) & 0xFFFFu;
+    if (code == 0) {
+        const desv_op op = *opp;
+        apply_one_op(a, op, mats, tg, lane);
+        return;
+    }
+    const T *mp = mats + reinterpret_cast<const uint32_t *>(opp)[4];
+    if (code & DESV_CODE_PRED) {
+        if ((tg & opp->cmask) != opp->cval) return;
+    }
+    const uint32_t w0y = w0.y;  // bytes 4..7: cslot, ga, gb, sa
+    switch (code & 0x7FFFu) {
+        DESV_M1U(0) DESV_M1U(1) DESV_M1U(2) DESV_M1U(3)
+        DESV_M1C(0, 1) DESV_M1C(0, 2) DESV_M1C(0, 3)
+        DESV_M1C(1, 0) DESV_M1C(1, 2) DESV_M1C(1, 3)
+        DESV_M1C(2, 0) DESV_M1C(2, 1) DESV_M1C(2, 3)
+        DESV_M1C(3, 0) DESV_M1C(3, 1) DESV_M1C(3, 2)
+        case 53 + V_GEN: m1_lane_free<V_GEN>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+        case 53 + V_REAL: m1_lane_free<V_REAL>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+        case 53 + V_DIAG: m1_lane_free<V_DIAG>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+        case 53 + V_PHASE1: m1_lane_free<V_PHASE1>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+        case 53 + V_ANTI: m1_lane_free<V_ANTI>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
+        DESV_DGROW(-1) DESV_DGROW(0) DESV_DGROW(1) DESV_DGROW(2) DESV_DGROW(3)
+        default: break;
+    }
+}
+
 // Apply ops[0..nops) of one stage to the thread's registers.
 template <typename T>
 __device__ __forceinline__ void run_stage_ops(T (&a)[16], const desv_op *ops, int nops, const T *mats, uint64_t tg,
                                               int lane) {
 #pragma unroll 1
-    for (int k = 0; k < nops; ++k) {
-        // desv_op is 40 bytes: records are only 8-byte aligned, so read bytes
-        // 0..15 as two 8-byte words (a 16-byte load would be misaligned for odd k)
-        const uint2 wlo = reinterpret_cast<const uint2 *>(ops + k)[0];
-        const uint2 whi = reinterpret_cast<const uint2 *>(ops + k)[1];
-        const uint4 w0 = make_uint4(wlo.x, wlo.y, whi.x, whi.y);
-        const uint32_t code = (w0.w >> 8) & 0xFFFFu;
-        if (code == 0) {
-            const desv_op op = ops[k];
-            apply_one_op(a, op, mats, tg, lane);
-            continue;
-        }
-        const T *mp = mats + reinterpret_cast<const uint32_t *>(ops + k)[4];
-        if (code & DESV_CODE_PRED) {
-            const uint64_t cm = ops[k].cmask, cv = ops[k].cval;
-            if ((tg & cm) != cv) continue;
-        }
-        const uint32_t w0y = w0.y;  // bytes 4..7: cslot, ga, gb, sa
-        switch (code & 0x7FFFu) {
-            DESV_M1U(0) DESV_M1U(1) DESV_M1U(2) DESV_M1U(3)
-            DESV_M1C(0, 1) DESV_M1C(0, 2) DESV_M1C(0, 3)
-            DESV_M1C(1, 0) DESV_M1C(1, 2) DESV_M1C(1, 3)
-            DESV_M1C(2, 0) DESV_M1C(2, 1) DESV_M1C(2, 3)
-            DESV_M1C(3, 0) DESV_M1C(3, 1) DESV_M1C(3, 2)
-            case 53 + V_GEN: m1_lane_free<V_GEN>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
-            case 53 + V_REAL: m1_lane_free<V_REAL>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
-            case 53 + V_DIAG: m1_lane_free<V_DIAG>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
-            case 53 + V_PHASE1: m1_lane_free<V_PHASE1>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
-            case 53 + V_ANTI: m1_lane_free<V_ANTI>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
-            DESV_DGROW(-1) DESV_DGROW(0) DESV_DGROW(1) DESV_DGROW(2) DESV_DGROW(3)
-            default: break;
-        }
-    }
+    for (int k = 0; k < nops; ++k) apply_op_at(a, ops + k, mats, tg, lane);
 }
 #undef DESV_M1U
 #undef DESV_M1C
