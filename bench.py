@@ -210,8 +210,8 @@ def run_ours(args):
 
     dev = torch.device('cuda', torch.cuda.current_device())
     st = torch.cuda.current_stream()
-    n = N_QUBITS
-    circ = brick_u3_circuit(n, LAYERS, SEED)
+    n, layers = args.qubits, args.layers
+    circ = brick_u3_circuit(n, layers, SEED)
     t_c = time.perf_counter()
     plan = CompiledCircuit(de.QuantumTranspiler.transpile(circ), n, torch.complex64)
     compile_s = time.perf_counter() - t_c
@@ -221,7 +221,7 @@ def run_ours(args):
     N.check(lib.desv_init_basis(ctypes.c_void_p(sv.data_ptr()), n, N.DESV_C64, 0, ctypes.c_void_p(st.cuda_stream)),
             'init')
     ops_t, mats_t = plan.device_arrays(dev)
-    passes = plan.packed.passes
+    passes = plan.device_passes
     pass_bytes = 2 * (1 << n) * 8
 
     def one_pass(i):
@@ -262,7 +262,7 @@ def run_ours(args):
     sim = de.DenseSVSimulator(n, use_float32=True)
     e2e_times, h2d = [], 0
     for i in range(args.warmup + args.steps):
-        c = brick_u3_circuit(n, LAYERS, SEED + 1 + i)
+        c = brick_u3_circuit(n, layers, SEED + 1 + i)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sim.set_initial_state(None)
@@ -273,7 +273,8 @@ def run_ours(args):
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)
-            h2d = int(plan_i.packed.ops.nbytes + plan_i.device_arrays(dev)[1].numel() * 4)
+            ops_i, mats_i = plan_i.device_arrays(dev)
+            h2d = int(ops_i.numel() + mats_i.numel() * 4)
         sim._plans.clear()
     e2e_step = _max_over_ranks(float(np.mean(e2e_times)), ws)
     e2e_passes = npasses
@@ -293,15 +294,17 @@ def run_ours(args):
             'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'complex64 (fp32 gate math)', 'data': 'synthetic',
-            'config': {'workload': f'{n}-qubit complex64 random circuit, {LAYERS} layers of U3 on every qubit + '
+            'config': {'workload': f'{n}-qubit complex64 random circuit, {layers} layers of U3 on every qubit + '
                                    f'brick-wall CZ, fused into tile passes', 'seed': SEED, 'qubits': n,
-                       'layers': LAYERS, 'fused_passes': npasses, 'tile_bits': plan.tile_bits,
-                       'l2': 'state (8 GiB) far larger than L2; no flush needed', 'parallelism': f'replicas x{ws}'},
-            'passes_per_step': npasses, 'layers_per_s': ws * LAYERS / (ms_step / 1e3),
-            'ms_per_layer': ms_step / LAYERS, 'compile_s': compile_s,
+                       'layers': layers, 'fused_passes': npasses, 'tile_bits': plan.tile_bits,
+                       'l2': f'state ({(1 << n) * 8 / 2**30:.2f} GiB) larger than L2 (126 MB); no flush needed',
+                       'parallelism': f'replicas x{ws}'},
+            'passes_per_step': npasses, 'layers_per_s': ws * layers / (ms_step / 1e3),
+            'ms_per_layer': ms_step / layers, 'compile_s': compile_s,
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_src,
-                         'kernel': 'k_fused_pass<float2,12,4>', 'algorithmic_bytes_per_launch': pass_bytes,
+                         'kernel': f'k_fused_pass<float2,{plan.tile_bits},3>',
+                         'algorithmic_bytes_per_launch': pass_bytes,
                          'avg_launch_ms': avg_pass_ms, 'min_launch_ms': float(per_pass.min()),
                          'max_launch_ms': float(per_pass.max())},
             'e2e': {'value': e2e_value, 'unit': 'GB/s', 'h2d_bytes_per_step': h2d,
@@ -446,6 +449,8 @@ def main():
     ap.add_argument('--skip-cpu', action='store_true')
     ap.add_argument('--skip-batch', action='store_true')
     ap.add_argument('--skip-large', action='store_true')
+    ap.add_argument('--qubits', type=int, default=N_QUBITS, help='headline circuit width (default 30)')
+    ap.add_argument('--layers', type=int, default=LAYERS, help='headline circuit depth (default 40)')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

@@ -288,6 +288,9 @@ __device__ __forceinline__ void apply_one_op(T (&a)[16], const desv_op &op, cons
 //   | 0x8000                             the thread predicate (cmask/cval) applies
 //   0                                    decode the fields (apply_one_op)
 #define DESV_CODE_PRED 0x8000u
+#define DESV_CODE_MULTI 120u      // + slot mask 1..15: general 2x2 on each slot in the mask
+#define DESV_CODE_MULTI_REAL 136u // + slot mask: real 2x2 on each slot in the mask
+#define DESV_CODE_SIGNS 152u      // group of +-1 diagonals, s0 entries at the op's matrix offset
 
 template <int S, int CS, typename T>
 __device__ __forceinline__ void m1_ctl_case(T (&a)[16], const M22<T> &m, bool anti) {
@@ -318,21 +321,91 @@ __device__ __forceinline__ void diag_case(T (&a)[16], const T *mp, uint32_t w0y,
     case 83 + (SA + 1) * 5 + (SB + 1): diag_case<SA, SB>(a, mp, w0y, tg, false); break;
 #define DESV_DGROW(SA) DESV_DG(SA, -1) DESV_DG(SA, 0) DESV_DG(SA, 1) DESV_DG(SA, 2) DESV_DG(SA, 3)
 
-// Apply the op at `opp` (dispatch code or field decode) to the thread's registers.
+// 2x2 gates on every register slot in the compile-time set M (ascending slot
+// order, commuting: the slots are distinct); matrices are consecutive in the pool.
+template <int M, int VAR, typename T>
+__device__ __forceinline__ void multi_reg(T (&a)[16], const T *mp) {
+    constexpr int k1 = (M & 1) ? 1 : 0;
+    constexpr int k2 = k1 + ((M & 2) ? 1 : 0);
+    constexpr int k3 = k2 + ((M & 4) ? 1 : 0);
+    if (M & 1) m1_reg<0, VAR, -1>(a, load_m22(mp));
+    if (M & 2) m1_reg<1, VAR, -1>(a, load_m22(mp + 4 * k1));
+    if (M & 4) m1_reg<2, VAR, -1>(a, load_m22(mp + 4 * k2));
+    if (M & 8) m1_reg<3, VAR, -1>(a, load_m22(mp + 4 * k3));
+}
+
+// 16-bit mask of the register indices j whose selected bit is 1: x < 4 is a
+// register slot, 0x40 | b is global index bit b (fixed for the thread), 0xFF
+// is an absent bit (always 0).
+__device__ __forceinline__ uint32_t sign_bit_mask(uint32_t x, uint64_t tg) {
+    if (x < 4u) return (uint32_t)(0xFF00F0F0CCCCAAAAull >> (16u * x)) & 0xFFFFu;
+    if (x == 0xFFu) return 0u;
+    return ((tg >> (x & 63u)) & 1ull) ? 0xFFFFu : 0u;
+}
+
+__device__ __forceinline__ void flip_sign(float2 &v, uint32_t s) {
+    v.x = __uint_as_float(__float_as_uint(v.x) ^ s);
+    v.y = __uint_as_float(__float_as_uint(v.y) ^ s);
+}
+__device__ __forceinline__ void flip_sign(double2 &v, uint32_t s) {
+    const unsigned long long t = (unsigned long long)s << 32;
+    v.x = __longlong_as_double(__double_as_longlong(v.x) ^ (long long)t);
+    v.y = __longlong_as_double(__double_as_longlong(v.y) ^ (long long)t);
+}
+
+// A group of +-1 diagonals (cz, and cp / crz at angles that give signs): entry
+// i = a | b << 8 | pattern << 16, where pattern bit k negates the amplitudes
+// with bit(a) + 2 bit(b) == k.  The group's signs are folded into one 16-bit
+// mask per thread and applied once, as sign-bit flips.
 template <typename T>
-__device__ __forceinline__ void apply_op_at(T (&a)[16], const desv_op *opp, const T *mats, uint64_t tg, int lane) {
-    // desv_op is 40 bytes: records are only 8-byte aligned, so read bytes
-    // 0..15 as two 8-byte words (a 16-byte load would be misaligned for odd k)
-    const uint2 wlo = reinterpret_cast<const uint2 *>(opp)[0];
-    const uint2 whi = reinterpret_cast<const uint2 *>(opp)[1];
-    const uint4 w0 = make_uint4(wlo.x, wlo.y, whi.x, whi.y);
+__device__ __forceinline__ void signs_group(T (&a)[16], const uint32_t *e, int cnt, uint64_t tg) {
+    uint32_t neg = 0;
+#pragma unroll 1
+    for (int i = 0; i < cnt; ++i) {
+        const uint32_t w = e[i];
+        const uint32_t ma1 = sign_bit_mask(w & 0xFFu, tg), mb1 = sign_bit_mask((w >> 8) & 0xFFu, tg);
+        const uint32_t ma0 = ~ma1 & 0xFFFFu, mb0 = ~mb1 & 0xFFFFu;
+        const uint32_t p = w >> 16;
+        neg ^= (ma0 & mb0 & (0u - (p & 1u))) ^ (ma1 & mb0 & (0u - ((p >> 1) & 1u))) ^
+               (ma0 & mb1 & (0u - ((p >> 2) & 1u))) ^ (ma1 & mb1 & (0u - ((p >> 3) & 1u)));
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) flip_sign(a[j], (neg << (31 - j)) & 0x80000000u);
+}
+
+#define DESV_MULTI(M)                                              \
+    case DESV_CODE_MULTI + M: multi_reg<M, V_GEN>(a, mp); break;   \
+    case DESV_CODE_MULTI_REAL + M: multi_reg<M, V_REAL>(a, mp); break;
+
+// First 24 bytes of an op record: bytes 0..15 (kinds, slots, code) and the
+// matrix offset (bytes 16..19).  Records are 40 bytes, so only 8-byte loads
+// are aligned for every record.
+struct OpHead {
+    uint4 w;
+    uint32_t mat;
+};
+
+__device__ __forceinline__ OpHead load_head(const desv_op *opp) {
+    const uint2 *p = reinterpret_cast<const uint2 *>(opp);
+    const uint2 lo = p[0], hi = p[1], m = p[2];
+    OpHead h;
+    h.w = make_uint4(lo.x, lo.y, hi.x, hi.y);
+    h.mat = m.x;
+    return h;
+}
+
+// Apply the op whose header is `h` (record at `opp`) to the thread's registers.
+template <typename T>
+__device__ __forceinline__ void apply_op_head(T (&a)[16], const OpHead &h, const desv_op *opp, const T *mats,
+                                              uint64_t tg, int lane) {
+    const uint4 w0 = h.w;
     const uint32_t code = (w0.w >> 8) & 0xFFFFu;
     if (code == 0) {
         const desv_op op = *opp;
         apply_one_op(a, op, mats, tg, lane);
         return;
     }
-    const T *mp = mats + reinterpret_cast<const uint32_t *>(opp)[4];
+    const T *mp = mats + h.mat;
     if (code & DESV_CODE_PRED) {
         if ((tg & opp->cmask) != opp->cval) return;
     }
@@ -349,17 +422,36 @@ __device__ __forceinline__ void apply_op_at(T (&a)[16], const desv_op *opp, cons
         case 53 + V_PHASE1: m1_lane_free<V_PHASE1>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
         case 53 + V_ANTI: m1_lane_free<V_ANTI>(a, load_m22(mp), (int)((w0.x >> 16) & 0xFFu) - 16, lane); break;
         DESV_DGROW(-1) DESV_DGROW(0) DESV_DGROW(1) DESV_DGROW(2) DESV_DGROW(3)
+        DESV_MULTI(1) DESV_MULTI(2) DESV_MULTI(3) DESV_MULTI(4) DESV_MULTI(5) DESV_MULTI(6) DESV_MULTI(7)
+        DESV_MULTI(8) DESV_MULTI(9) DESV_MULTI(10) DESV_MULTI(11) DESV_MULTI(12) DESV_MULTI(13) DESV_MULTI(14)
+        DESV_MULTI(15)
+        case DESV_CODE_SIGNS:
+            signs_group(a, reinterpret_cast<const uint32_t *>(mp), (int)((w0.x >> 16) & 0xFFu), tg);
+            break;
         default: break;
     }
 }
 
-// Apply ops[0..nops) of one stage to the thread's registers.
+template <typename T>
+__device__ __forceinline__ void apply_op_at(T (&a)[16], const desv_op *opp, const T *mats, uint64_t tg, int lane) {
+    apply_op_head(a, load_head(opp), opp, mats, tg, lane);
+}
+
+// Apply ops[0..nops) of one stage to the thread's registers; the next op's
+// header is loaded while the current op runs.
 template <typename T>
 __device__ __forceinline__ void run_stage_ops(T (&a)[16], const desv_op *ops, int nops, const T *mats, uint64_t tg,
                                               int lane) {
+    if (nops <= 0) return;
+    OpHead h = load_head(ops);
 #pragma unroll 1
-    for (int k = 0; k < nops; ++k) apply_op_at(a, ops + k, mats, tg, lane);
+    for (int k = 0; k < nops; ++k) {
+        const OpHead hn = load_head(ops + (k + 1 < nops ? k + 1 : k));
+        apply_op_head(a, h, ops + k, mats, tg, lane);
+        h = hn;
+    }
 }
+#undef DESV_MULTI
 #undef DESV_M1U
 #undef DESV_M1C
 #undef DESV_DG

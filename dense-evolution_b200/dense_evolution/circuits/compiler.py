@@ -108,13 +108,19 @@ class CompiledCircuit:
     def _np_dtype(self):
         return np.complex64 if self.dtype == torch.complex64 else np.complex128
 
+    @property
+    def device_passes(self):
+        """desv_pass rows of the grouped op stream that device_arrays() uploaded."""
+        return self._passes
+
     def device_arrays(self, device, theta=None):
         """(ops, mats) device tensors for `theta` (cached for constant circuits)."""
         key = None if theta is None else np.asarray(theta, dtype=np.float64).tobytes()
         if self._dev_cache is not None and self._dev_cache[0] == device and self._dev_theta_key == key:
             return self._dev_cache[1], self._dev_cache[2]
         mats = self.packed.materialize(theta, self._np_dtype())
-        ops_t = torch.from_numpy(self.packed.ops.view(np.uint8).copy()).to(device)
+        ops, self._passes, mats = self.packed.compact(mats)
+        ops_t = torch.from_numpy(ops.view(np.uint8).copy()).to(device)
         rdt = np.float32 if self.dtype == torch.complex64 else np.float64
         mats_t = torch.from_numpy(mats.view(rdt).copy()).to(device)
         self._dev_cache = (device, ops_t, mats_t)
@@ -135,7 +141,7 @@ class CompiledCircuit:
         if len(self.packed.passes) == 0:
             return sv
         ops_t, mats_t = self.device_arrays(sv.device, theta)
-        passes = self.packed.passes
+        passes = self._passes
         N.check(lib.desv_apply_passes(ctypes.c_void_p(sv.data_ptr()), self.n, code,
                                       ctypes.c_void_p(passes.ctypes.data), len(passes),
                                       ctypes.c_void_p(ops_t.data_ptr()), ctypes.c_void_p(mats_t.data_ptr()), st),

@@ -714,6 +714,187 @@ class Packed:
         return code.astype(np.uint16)
 
 
+    # ------------------------------------------------------------ grouping
+    def compact(self, pool: np.ndarray):
+        """Forward-pass op stream with runs of ops grouped (desv.h grouped codes).
+
+        Inside a stage, a run of uncontrolled general / real 2x2 ops on distinct
+        register slots becomes one multi-slot op (the gates commute), and a run
+        of +-1 diagonals becomes one sign group, so the kernel dispatches once
+        per run.  Ops are first reordered inside the stage (never across a
+        non-commuting pair) to make the runs long.  Call after `materialize`
+        (codes and flags are set there).  Returns (ops, passes, pool) for
+        desv_apply_passes; the canonical records in self.ops are left untouched.
+        """
+        codes = self.ops['code']
+        c = codes & 0x7FFF
+        sg = np.nonzero((c >= 58) & (c <= 82))[0]
+        tabs = pool[self.ops['mat'][sg].astype(np.int64)[:, None] + np.arange(4)] if len(sg) else pool[:0]
+        key = codes.tobytes() + np.signbit(tabs.real).tobytes()
+        cache = getattr(self, '_compact_cache', None)
+        if cache is None or cache[0] != key or cache[5] != len(pool):
+            cache = (key,) + self._compact_structure(pool) + (len(pool),)
+            self._compact_cache = cache
+        _, ops, passes, gather, words, _ = cache
+        if words is None and not len(gather):
+            return ops, passes, pool
+        ext = [pool, pool[gather]]
+        if words is not None:
+            # sign entries: raw uint32 words stored in whole pool elements
+            wpe = pool.dtype.itemsize // 4
+            w = np.zeros((len(words) + wpe - 1) // wpe * wpe, np.uint32)
+            w[:len(words)] = words
+            ext.append(np.frombuffer(w.tobytes(), dtype=pool.dtype))
+        return ops, passes, np.concatenate(ext)
+
+    def _compact_structure(self, pool):
+        recs = self.ops
+        wpe = pool.dtype.itemsize // 4
+        out, rows, gather, words = [], [], [], []
+        base = len(pool)
+        nsign_words = 0
+        # sign-entry words go after the gathered matrices: offsets are fixed up
+        # once the gather length is known
+        sign_recs = []
+        for ps in self.passes:
+            begin = len(out)
+            k, end = int(ps['op_begin']), int(ps['op_end'])
+            while k < end:
+                st = recs[k].copy()
+                cnt = int(st['mat'])
+                body = recs[self._group_order(k + 1, cnt)]
+                new = []
+                i = 0
+                while i < cnt:
+                    r = body[i]
+                    c = int(r['code'])
+                    if not c & 0x8000 and 1 <= c <= 20 and (c - 1) % 5 in (0, 1):
+                        run, slots = [i], {(c - 1) // 5}
+                        j = i + 1
+                        while j < cnt:
+                            cj = int(body[j]['code'])
+                            if cj & 0x8000 or not 1 <= cj <= 20 or (cj - 1) % 5 not in (0, 1) or \
+                                    (cj - 1) // 5 in slots:
+                                break
+                            run.append(j)
+                            slots.add((cj - 1) // 5)
+                            j += 1
+                        if len(run) >= 2:
+                            by_slot = sorted(run, key=lambda x: (int(body[x]['code']) - 1) // 5)
+                            real = all((int(body[x]['code']) - 1) % 5 == 1 for x in run)
+                            mask = sum(1 << ((int(body[x]['code']) - 1) // 5) for x in run)
+                            g = r.copy()
+                            g['code'] = (136 if real else 120) + mask
+                            g['mat'] = base + len(gather)
+                            for x in by_slot:
+                                m0 = int(body[x]['mat'])
+                                gather.extend(range(m0, m0 + 4))
+                            new.append(g)
+                        else:
+                            new.append(r.copy())
+                        i = j
+                    elif not c & 0x8000 and 58 <= c <= 82:
+                        j = i
+                        ents = []
+                        while j < cnt:
+                            cj = int(body[j]['code'])
+                            if cj & 0x8000 or not 58 <= cj <= 82 or len(ents) == 127:
+                                break
+                            ents.append(self._sign_word(body[j], pool))
+                            j += 1
+                        g = r.copy()
+                        g['code'] = 152
+                        g['s0'] = len(ents)
+                        sign_recs.append((g, nsign_words))
+                        words.extend(ents)
+                        nsign_words += len(ents)
+                        # keep every group's words whole-element aligned
+                        pad = (-nsign_words) % wpe
+                        words.extend([0] * pad)
+                        nsign_words += pad
+                        new.append(g)
+                        i = j
+                    else:
+                        new.append(r.copy())
+                        i += 1
+                st['mat'] = len(new)
+                out.append(st)
+                out.extend(new)
+                k += 1 + cnt
+            row = ps.copy()
+            row['op_begin'], row['op_end'] = begin, len(out)
+            rows.append(row)
+        wbase = base + len(gather)
+        for g, w0 in sign_recs:
+            g['mat'] = wbase + w0 // wpe
+        ops = np.array(out, dtype=N.OP_DTYPE) if out else np.zeros(0, N.OP_DTYPE)
+        passes = np.array(rows, dtype=self.passes.dtype) if rows else np.zeros(0, self.passes.dtype)
+        return ops, passes, np.array(gather, np.int64), (np.array(words, np.uint32) if words else None)
+
+    def _group_order(self, first: int, cnt: int) -> np.ndarray:
+        """Record indices of one stage, reordered (respecting every non-commuting
+        pair) so that mergeable ops sit next to each other: uncontrolled
+        general / real 2x2 ops on distinct register slots, and +-1 diagonals."""
+        idx = list(range(first, first + cnt))
+        if cnt < 3:
+            return np.array(idx, np.int64)
+        if not hasattr(self, '_fop_of'):
+            self._fop_of = {ri: fi for ri, fi in self.op_slots}
+        codes = [int(c) for c in self.ops['code'][first:first + cnt]]
+
+        def cls(c):
+            if c & 0x8000:
+                return 'o'
+            if 1 <= c <= 20 and (c - 1) % 5 in (0, 1):
+                return 'r'
+            if 58 <= c <= 82:
+                return 's'
+            return 'o'
+        kinds = [cls(c) for c in codes]
+        fo = [self.fops[self._fop_of[i]] for i in idx]
+        preds = []
+        for j in range(cnt):
+            pj = set()
+            for i in range(j):
+                if (fo[i].nd & (fo[j].nd | fo[j].d)) or (fo[i].d & fo[j].nd):
+                    pj.add(i)
+            preds.append(pj)
+        done, order = set(), []
+        cur, slots = None, set()
+        while len(order) < cnt:
+            ready = [j for j in range(cnt) if j not in done and preds[j] <= done]
+            pick = None
+            if cur == 'r':
+                pick = next((j for j in ready if kinds[j] == 'r' and (codes[j] - 1) // 5 not in slots), None)
+            elif cur == 's':
+                pick = next((j for j in ready if kinds[j] == 's'), None)
+            if pick is None:
+                slots = set()
+                for want in ('r', 's', 'o'):
+                    pick = next((j for j in ready if kinds[j] == want), None)
+                    if pick is not None:
+                        break
+                cur = kinds[pick]
+            if cur == 'r':
+                slots.add((codes[pick] - 1) // 5)
+            done.add(pick)
+            order.append(pick)
+        return np.array([idx[j] for j in order], np.int64)
+
+    @staticmethod
+    def _sign_word(r, pool) -> int:
+        def sel(gkey, skey):
+            s = int(r[skey])
+            if s >= 0:
+                return s
+            g = int(r[gkey])
+            return 0xFF if g == 0xFF else 0x40 | g
+        m0 = int(r['mat'])
+        d = pool[m0:m0 + 4]
+        pattern = sum(1 << k for k in range(4) if d[k].real < 0)
+        return sel('ga', 'sa') | sel('gb', 'sb') << 8 | pattern << 16
+
+
 def _clean_batch(m: np.ndarray) -> np.ndarray:
     """Zero real / imaginary parts below 1e-15 x max(1, max |entry|) per row."""
     scale = np.maximum(1.0, np.abs(m).max(axis=1, keepdims=True))

@@ -72,7 +72,13 @@ typedef struct desv_op {
                         controlled by slot CS; 53+V lane bit uncontrolled; 58+(SA+1)*5+(SB+1)
                         sign-only diagonal; 83+(SA+1)*5+(SB+1) diagonal; |0x8000: cmask/cval
                         predicate applies.  V: 0 general, 1 real, 2 diagonal, 3 phase-on-|1>,
-                        4 anti-diagonal (same priority as the flags PHASE1 > DIAG > ANTI > REAL) */
+                        4 anti-diagonal (same priority as the flags PHASE1 > DIAG > ANTI > REAL).
+                        Grouped ops (forward passes): 120+M general 2x2 on every register slot in
+                        the 4-bit mask M, 136+M the same with real matrices (matrices consecutive,
+                        ascending slot); 152 a group of s0 +-1 diagonals whose entries are uint32
+                        words at the matrix offset: a | b << 8 | pattern << 16 with a, b = register
+                        slot 0..3, 0x40 | global bit, or 0xFF (absent), pattern bit k negating
+                        amplitudes with bit(a) + 2*bit(b) == k */
     uint8_t pad0;
     uint32_t mat;    /* first complex element of this op's matrix in the matrix pool */
     int32_t param;   /* adjoint plans: gradient slot of this op (-1: none) */

@@ -206,4 +206,38 @@ def _apply_coded(a, tg, op, g, mats, code):
         if sign:
             f = np.where(np.real(f) < 0, -1.0, 1.0)
         return np.where(pred, a * f, a)
+    if 120 <= c <= 151:
+        real, mask = c >= 136, c - (136 if c >= 136 else 120)
+        out = a
+        k = 0
+        for S in range(4):
+            if not (mask >> S) & 1:
+                continue
+            m = mats[m0 + 4 * k:m0 + 4 * k + 4].reshape(2, 2)
+            k += 1
+            tl = g[S]
+            lo = j[((j >> tl) & 1) == 0]
+            hi = lo | (1 << tl)
+            n0, n1 = _variant_pair(m, 1 if real else 0, out[:, lo], out[:, hi])
+            out = out.copy()
+            out[:, lo], out[:, hi] = n0, n1
+        return np.where(pred, out, a)
+    if c == 152:
+        cnt = int(op['s0'])
+        wpe = mats.dtype.itemsize // 4
+        words = np.ascontiguousarray(mats).view(np.uint32)[m0 * wpe:m0 * wpe + cnt]
+        neg = np.zeros(a.shape, dtype=bool)
+
+        def bit(x):
+            if x < 4:
+                return ((j >> g[x]) & 1)[None, :]
+            if x == 0xFF:
+                return np.zeros((1, a.shape[1]), np.int64)
+            return _bit(tg, x & 63)
+        for w in words:
+            w = int(w)
+            ba, bb = bit(w & 0xFF), bit((w >> 8) & 0xFF)
+            pat = (w >> 16) & 0xF
+            neg ^= ((pat >> (ba + 2 * bb)) & 1).astype(bool)
+        return np.where(pred & neg, -a, a)
     raise AssertionError(f'unknown dispatch code {code}')

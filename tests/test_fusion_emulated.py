@@ -16,7 +16,12 @@ def _emulate(circ, n, kmax, theta=None, slots=None, merge=True):
     target = QuantumTranspiler.transpile(circ)
     ir, fops, packed = fusion.build(target, n, kmax, slots, merge)
     mats = packed.materialize(theta, np.complex128)
-    return run_passes(O.zero_state(n), n, packed.passes, packed.ops, mats), packed
+    got = run_passes(O.zero_state(n), n, packed.passes, packed.ops, mats)
+    # the grouped stream the forward kernels run must give the same state
+    ops, passes, pool = packed.compact(mats)
+    grouped = run_passes(O.zero_state(n), n, passes, ops, pool)
+    assert np.max(np.abs(grouped - got)) < 1e-12
+    return got, packed
 
 
 @pytest.mark.parametrize('n,kmax', [(9, 9), (10, 9), (11, 10), (12, 12), (13, 11)])
