@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, T
                                                                 int nops, const T *mats, int nparams, double *part) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
-    double *acc = reinterpret_cast<double *>(smem + 128 + (size_t)NBUF * 2 * (1u << K) * sizeof(T));
+    double *acc = reinterpret_cast<double *>(smem + PIPE_HDR_BYTES + (size_t)NBUF * 2 * (1u << K) * sizeof(T));
     for (int i = threadIdx.x; i < NW * nparams; i += blockDim.x) acc[i] = 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     PipeArrays<T, 2> A;
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, T
                 a[j] = sphi[off];
                 b[j] = slam[off];
             }
-            const uint64_t tg = base | tile_local_to_global(g, idx);
+            const uint64_t tg = base | tl2g(pipe_ctab(smem), g.L, idx);
 #pragma unroll 1
             for (int q = 1; q <= cnt; ++q) {
                 const desv_op op = ops[k + q];
@@ -105,7 +105,7 @@ constexpr int ADJ_MAX_ROWS = 1184;  // partial-sum rows per pass (= grid bound)
 
 template <typename T, int K, int NBUF> static size_t adj_smem(int nparams) {
     constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
-    return 128 + (size_t)NBUF * 2 * (1u << K) * sizeof(T) + (size_t)NW * nparams * sizeof(double);
+    return PIPE_HDR_BYTES + (size_t)NBUF * 2 * (1u << K) * sizeof(T) + (size_t)NW * nparams * sizeof(double);
 }
 
 template <typename T, int K, int NBUF>

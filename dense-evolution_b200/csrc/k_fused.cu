@@ -10,30 +10,52 @@
 namespace desv {
 
 template <typename T, int K>
-__device__ __forceinline__ void fused_tile_body(T *s, uint64_t base, const TileGeom &g, const desv_op *ops, int nops,
-                                                const T *mats) {
+__device__ __forceinline__ void fused_tile_body(T *s, T *sv, uint64_t base, const uint64_t *ctab, int L,
+                                                const desv_op *ops, int nops, const T *mats) {
     const int lane = threadIdx.x & 31;
     int k = 0;
 #pragma unroll 1
     while (k < nops) {
-        const desv_op st = ops[k];
-        const int cnt = (int)st.mat;
-        const uint32_t idx = stage_base(threadIdx.x, st.g);
-        const uint32_t o0 = 1u << st.g[0], o1 = 1u << st.g[1], o2 = 1u << st.g[2], o3 = 1u << st.g[3];
+        // stage record: register bit positions g[0..3] (bytes 9..12), op count (mat)
+        const OpHead sh = load_head(ops + k);
+        const int cnt = (int)sh.mat;
+        const uint32_t g0 = (sh.w.z >> 8) & 0xFFu, g1 = (sh.w.z >> 16) & 0xFFu, g2 = sh.w.z >> 24,
+                       g3 = sh.w.w & 0xFFu;
+        const uint8_t gs8[4] = {(uint8_t)g0, (uint8_t)g1, (uint8_t)g2, (uint8_t)g3};
+        const uint32_t idx = stage_base(threadIdx.x, gs8);
+        const uint32_t o0 = 1u << g0, o1 = 1u << g1, o2 = 1u << g2, o3 = 1u << g3;
         T a[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j)
             a[j] = s[idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) + ((j & 8) ? o3 : 0u)];
-        const uint64_t tg = base | tile_local_to_global(g, idx);
+        const uint64_t tg = base | tl2g(ctab, L, idx);
         run_stage_ops(a, ops + k + 1, cnt, mats, tg, lane);
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
-            s[idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) + ((j & 8) ? o3 : 0u)] = a[j];
-        __syncthreads();
         k += 1 + cnt;
+        if (k >= nops) {
+            // last stage: straight from registers to HBM.  Lanes are index bits
+            // 0..4, so every store instruction of a warp writes 32 consecutive
+            // amplitudes.
+            const uint64_t q0 = tl_bit(ctab, L, g0), q1 = tl_bit(ctab, L, g1), q2 = tl_bit(ctab, L, g2),
+                           q3 = tl_bit(ctab, L, g3);
+            T *out = sv + tg;
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                out[((j & 1) ? q0 : 0ull) + ((j & 2) ? q1 : 0ull) + ((j & 4) ? q2 : 0ull) + ((j & 8) ? q3 : 0ull)] =
+                    a[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                s[idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) + ((j & 8) ? o3 : 0u)] = a[j];
+            __syncthreads();
+            // the next bulk load into this slot (async proxy) must follow these writes
+            fence_proxy_async_smem();
+        }
     }
 }
 
+// Loads run NBUF-1 tiles ahead (bulk copies into the shared-memory ring); the
+// last register stage of every tile writes its amplitudes straight to HBM, so
+// no ring slot waits for a store to drain.
 template <typename T, int K, int NBUF>
 __global__ void __launch_bounds__(1 << (K - 4)) k_fused_pass(T *sv, TileGeom g, const desv_op *ops, int nops,
                                                               const T *mats) {
@@ -41,8 +63,10 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_fused_pass(T *sv, TileGeom g, 
     PipeArrays<T, 1> A;
     A.ptr[0] = sv;
     A.load[0] = true;
-    A.store[0] = true;
-    auto body = [&](T *const *sp, uint64_t base, uint64_t) { fused_tile_body<T, K>(sp[0], base, g, ops, nops, mats); };
+    A.store[0] = false;
+    auto body = [&](T *const *sp, uint64_t base, uint64_t) {
+        fused_tile_body<T, K>(sp[0], sv, base, pipe_ctab(smem), g.L, ops, nops, mats);
+    };
     run_tiles<T, K, NBUF, 1>(g, A, body, smem);
 }
 
@@ -51,7 +75,7 @@ static int launch_fused(T *sv, const TileGeom &g, const desv_op *ops, int nops, 
     static int bps[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
-    const size_t smem = 128 + (size_t)NBUF * (1u << K) * sizeof(T);
+    const size_t smem = PIPE_HDR_BYTES + (size_t)NBUF * (1u << K) * sizeof(T);
     if (bps[dev & 63] == 0) {
         cudaFuncSetAttribute(k_fused_pass<T, K, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int b = 0;

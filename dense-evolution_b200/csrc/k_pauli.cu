@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
                                                          int nterms, int want_e, double *part) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NARR = MODE == 0 ? 1 : 2;
-    TermTab<T> *tab = reinterpret_cast<TermTab<T> *>(smem + 128 + (size_t)NBUF * NARR * (1u << K) * sizeof(T));
+    TermTab<T> *tab = reinterpret_cast<TermTab<T> *>(smem + PIPE_HDR_BYTES + (size_t)NBUF * NARR * (1u << K) * sizeof(T));
     for (int k = threadIdx.x; k < nterms; k += blockDim.x) {
         const desv_pauli_term tm = terms[k];
         tab->xl[k] = global_to_tile_local(g, tm.xmask);
@@ -128,7 +128,7 @@ static int launch_pauli(const T *psi, T *out, const TileGeom &g, const desv_paul
     int dev = 0;
     cudaGetDevice(&dev);
     constexpr int NARR = MODE == 0 ? 1 : 2;
-    const size_t smem = 128 + (size_t)NBUF * NARR * (1u << K) * sizeof(T) + sizeof(TermTab<T>);
+    const size_t smem = PIPE_HDR_BYTES + (size_t)NBUF * NARR * (1u << K) * sizeof(T) + sizeof(TermTab<T>);
     if (bps[dev & 63] == 0) {
         cudaFuncSetAttribute(k_pauli<T, K, NBUF, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int b = 0;

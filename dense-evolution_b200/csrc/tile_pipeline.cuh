@@ -52,6 +52,27 @@ __device__ __forceinline__ uint64_t chunk_offset(const TileGeom &g, uint32_t c) 
     return o;
 }
 
+// Shared-memory header of a pipelined kernel: 128 bytes of mbarriers, then
+// the chunk table ctab[c] = global offset of the tile's 2^L-run c (built when
+// the tile has at most PIPE_CTAB_MAX runs), then the NBUF x NARR tile slots.
+constexpr uint32_t PIPE_CTAB_MAX = 256;
+constexpr size_t PIPE_HDR_BYTES = 128 + 8 * PIPE_CTAB_MAX;
+
+__device__ __forceinline__ const uint64_t *pipe_ctab(const unsigned char *smem) {
+    return reinterpret_cast<const uint64_t *>(smem + 128);
+}
+
+// tile-local index j -> global offset inside the tile (table lookup; valid when
+// the tile has at most PIPE_CTAB_MAX runs)
+__device__ __forceinline__ uint64_t tl2g(const uint64_t *ctab, int L, uint32_t j) {
+    return ctab[j >> L] | (uint64_t)(j & ((1u << L) - 1u));
+}
+
+// global offset of tile-local bit position p (a single set bit)
+__device__ __forceinline__ uint64_t tl_bit(const uint64_t *ctab, int L, uint32_t p) {
+    return p < (uint32_t)L ? (1ull << p) : ctab[1u << (p - L)];
+}
+
 // Arrays taking part in a pipelined sweep.  Array 0 is always loaded.
 template <typename T, int NARR> struct PipeArrays {
     T *ptr[NARR];
@@ -70,7 +91,8 @@ template <typename T, int K, int NBUF, int NARR, class Body>
 __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body &body, unsigned char *smem) {
     constexpr uint32_t TILE = 1u << K;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-    T *bufs = reinterpret_cast<T *>(smem + 128);
+    uint64_t *ctab = reinterpret_cast<uint64_t *>(smem + 128);
+    T *bufs = reinterpret_cast<T *>(smem + PIPE_HDR_BYTES);
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const int lane = tid & 31;
     const uint32_t ntiles = 1u << (g.n - K);
@@ -94,16 +116,32 @@ __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body 
         for (int b = 0; b < NBUF; ++b) mbar_init(&full[b], nthr / 32);
         fence_mbar_init();
     }
+    // geometry, once per CTA: the chunk table, this thread's run offsets and the
+    // tile bases.  Tile t's base deposits the bits of t into the rest bits;
+    // consecutive tiles of this CTA differ by a constant deposited stride, added
+    // with carries running through the non-rest bits ((b | ~M) + s) & M.
+    if (nchunks <= PIPE_CTAB_MAX)
+        for (uint32_t c = tid; c < nchunks; c += nthr) ctab[c] = chunk_offset(g, c);
+    const uint64_t my_off = tid < nchunks ? chunk_offset(g, tid) : 0ull;
+    uint64_t rmask = 0;
+#pragma unroll 1
+    for (int r = 0; r < g.nrest; ++r) rmask |= 1ull << g.rest[r];
+    const uint64_t tstride = tile_base(g, gridDim.x);
+    const uint64_t base0 = tile_base(g, blockIdx.x);
     __syncthreads();
+    uint64_t lbase = base0;  // base of the next tile to load
+    uint64_t cbase = base0;  // base of the next tile to process
+    auto next_base = [&](uint64_t b) { return ((b | ~rmask) + tstride) & rmask; };
 
     auto slot_ptr = [&](uint32_t slot, int a) { return bufs + (size_t)(slot * NARR + a) * TILE; };
     auto issue_load = [&](uint32_t i) {
         const uint32_t slot = i % NBUF;
-        const uint64_t base = tile_base(g, blockIdx.x + (uint64_t)i * gridDim.x);
+        const uint64_t base = lbase;
+        lbase = next_base(lbase);
         if (lane == 0) mbar_arrive_expect_tx(&full[slot], warp_bytes);
         __syncwarp();
         for (uint32_t c = tid; c < nchunks; c += nthr) {
-            const uint64_t off = base + chunk_offset(g, c);
+            const uint64_t off = base + (c == tid ? my_off : chunk_offset(g, c));
 #pragma unroll
             for (int a = 0; a < NARR; ++a)
                 if (A.load[a]) bulk_g2s(slot_ptr(slot, a) + (size_t)c * chunk, A.ptr[a] + off, chunk_bytes, &full[slot]);
@@ -124,13 +162,14 @@ __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body 
 #pragma unroll
         for (int a = 0; a < NARR; ++a) sp[a] = slot_ptr(slot, a);
         const uint64_t tix = blockIdx.x + (uint64_t)i * gridDim.x;
-        const uint64_t base = tile_base(g, tix);
+        const uint64_t base = cbase;
+        cbase = next_base(cbase);
         body(sp, base, tix);
         if (any_store) {
             fence_proxy_async_smem();
             __syncthreads();
             for (uint32_t c = tid; c < nchunks; c += nthr) {
-                const uint64_t off = base + chunk_offset(g, c);
+                const uint64_t off = base + (c == tid ? my_off : chunk_offset(g, c));
 #pragma unroll
                 for (int a = 0; a < NARR; ++a)
                     if (A.store[a]) bulk_s2g(A.ptr[a] + off, sp[a] + (size_t)c * chunk, chunk_bytes);
