@@ -286,11 +286,14 @@ __device__ __forceinline__ void apply_one_op(T (&a)[16], const desv_op &op, cons
 //   58 + (SA+1)*5 + (SB+1)               sign-only diagonal (slots SA/SB, -1 = thread bit)
 //   83 + (SA+1)*5 + (SB+1)               diagonal
 //   | 0x8000                             the thread predicate (cmask/cval) applies
-//   0                                    decode the fields (apply_one_op)
+//   0                                    invalid in a plan (sets DESV_DEV_BADPLAN)
 #define DESV_CODE_PRED 0x8000u
 #define DESV_CODE_MULTI 120u      // + slot mask 1..15: general 2x2 on each slot in the mask
 #define DESV_CODE_MULTI_REAL 136u // + slot mask: real 2x2 on each slot in the mask
 #define DESV_CODE_SIGNS 152u      // group of +-1 diagonals, s0 entries at the op's matrix offset
+#define DESV_CODE_LAYER 160u      // + slot mask 0..15: general 2x2 on those slots and on the lane bits in s1
+#define DESV_CODE_LAYER_REAL 176u // + slot mask: the same with real matrices
+#define DESV_CODE_LANE_CTL 192u   // 2x2 on lane bit s0-16 with a register control (cslot) and/or predicate
 
 template <int S, int CS, typename T>
 __device__ __forceinline__ void m1_ctl_case(T (&a)[16], const M22<T> &m, bool anti) {
@@ -373,6 +376,32 @@ __device__ __forceinline__ void signs_group(T (&a)[16], const uint32_t *e, int c
     for (int j = 0; j < 16; ++j) flip_sign(a[j], (neg << (31 - j)) & 0x80000000u);
 }
 
+// 2x2 gates on the lane bits in `lmask` (bit b: lane bit b), commuting,
+// matrices consecutive (ascending lane bit).
+template <int VAR, typename T>
+__device__ __forceinline__ void multi_lane(T (&a)[16], const T *mp, uint32_t lmask, int lane) {
+#pragma unroll 1
+    while (lmask) {
+        const int lb = __ffs(lmask) - 1;
+        lmask &= lmask - 1u;
+        m1_lane_free<VAR>(a, load_m22(mp), lb, lane);
+        mp += 4;
+    }
+}
+
+// One layer of commuting uncontrolled 2x2 gates of a stage: register slots in
+// M (compile time), then the lane bits in lmask.
+template <int M, int VAR, typename T>
+__device__ __forceinline__ void layer_op(T (&a)[16], const T *mp, uint32_t lmask, int lane) {
+    constexpr int nreg = ((M & 1) ? 1 : 0) + ((M & 2) ? 1 : 0) + ((M & 4) ? 1 : 0) + ((M & 8) ? 1 : 0);
+    if (M) multi_reg<M, VAR>(a, mp);
+    multi_lane<VAR>(a, mp + 4 * nreg, lmask, lane);
+}
+
+#define DESV_LAYER(M)                                                                        \
+    case DESV_CODE_LAYER + M: layer_op<M, V_GEN>(a, mp, (w0.x >> 24) & 0x1Fu, lane); break;   \
+    case DESV_CODE_LAYER_REAL + M: layer_op<M, V_REAL>(a, mp, (w0.x >> 24) & 0x1Fu, lane); break;
+
 #define DESV_MULTI(M)                                              \
     case DESV_CODE_MULTI + M: multi_reg<M, V_GEN>(a, mp); break;   \
     case DESV_CODE_MULTI_REAL + M: multi_reg<M, V_REAL>(a, mp); break;
@@ -400,11 +429,6 @@ __device__ __forceinline__ void apply_op_head(T (&a)[16], const OpHead &h, const
                                               uint64_t tg, int lane) {
     const uint4 w0 = h.w;
     const uint32_t code = (w0.w >> 8) & 0xFFFFu;
-    if (code == 0) {
-        const desv_op op = *opp;
-        apply_one_op(a, op, mats, tg, lane);
-        return;
-    }
     const T *mp = mats + h.mat;
     if (code & DESV_CODE_PRED) {
         if ((tg & opp->cmask) != opp->cval) return;
@@ -425,10 +449,17 @@ __device__ __forceinline__ void apply_op_head(T (&a)[16], const OpHead &h, const
         DESV_MULTI(1) DESV_MULTI(2) DESV_MULTI(3) DESV_MULTI(4) DESV_MULTI(5) DESV_MULTI(6) DESV_MULTI(7)
         DESV_MULTI(8) DESV_MULTI(9) DESV_MULTI(10) DESV_MULTI(11) DESV_MULTI(12) DESV_MULTI(13) DESV_MULTI(14)
         DESV_MULTI(15)
+        DESV_LAYER(0) DESV_LAYER(1) DESV_LAYER(2) DESV_LAYER(3) DESV_LAYER(4) DESV_LAYER(5) DESV_LAYER(6)
+        DESV_LAYER(7) DESV_LAYER(8) DESV_LAYER(9) DESV_LAYER(10) DESV_LAYER(11) DESV_LAYER(12) DESV_LAYER(13)
+        DESV_LAYER(14) DESV_LAYER(15)
         case DESV_CODE_SIGNS:
             signs_group(a, reinterpret_cast<const uint32_t *>(mp), (int)((w0.x >> 16) & 0xFFu), tg);
             break;
-        default: break;
+        case DESV_CODE_LANE_CTL:
+            m1_lane(a, load_m22(mp), m1_variant((int)((w0.x >> 8) & 0xFFu)), (int)(int8_t)(w0.y & 0xFFu),
+                    (int)((w0.x >> 16) & 0xFFu) - 16, (tg & opp->cmask) == opp->cval, lane);
+            break;
+        default: atomicOr(&g_dev_status, DESV_DEV_BADPLAN); break;
     }
 }
 
@@ -452,6 +483,7 @@ __device__ __forceinline__ void run_stage_ops(T (&a)[16], const desv_op *ops, in
     }
 }
 #undef DESV_MULTI
+#undef DESV_LAYER
 #undef DESV_M1U
 #undef DESV_M1C
 #undef DESV_DG

@@ -701,6 +701,7 @@ class Packed:
         reg = m1 & (s0 < 16)
         free_lane = lane & ~pred & (cs < 0)
         code[free_lane] = 53 + var[free_lane]
+        code[lane & ~free_lane] = 192
         u = reg & (cs < 0)
         code[u] = 1 + s0[u] * 5 + var[u]
         c = reg & (cs >= 0)
@@ -711,6 +712,8 @@ class Packed:
         base = np.where(sign, 58, 83)
         code[d] = base[d] + (sa[d] + 1) * 5 + (sb[d] + 1)
         code[d & pred] |= 0x8000
+        if np.any(kind == N.OP_M2):
+            raise RuntimeError('fusion: dense 4x4 records are not supported by the pass kernels')
         return code.astype(np.uint16)
 
 
@@ -719,7 +722,7 @@ class Packed:
         """Forward-pass op stream with runs of ops grouped (desv.h grouped codes).
 
         Inside a stage, a run of uncontrolled general / real 2x2 ops on distinct
-        register slots becomes one multi-slot op (the gates commute), and a run
+        register slots and lane bits becomes one layer op (the gates commute), and a run
         of +-1 diagonals becomes one sign group, so the kernel dispatches once
         per run.  Ops are first reordered inside the stage (never across a
         non-commuting pair) to make the runs long.  Call after `materialize`
@@ -768,25 +771,26 @@ class Packed:
                 while i < cnt:
                     r = body[i]
                     c = int(r['code'])
-                    if not c & 0x8000 and 1 <= c <= 20 and (c - 1) % 5 in (0, 1):
-                        run, slots = [i], {(c - 1) // 5}
+                    if _layer_target(r) is not None:
+                        run, seen = [i], {_layer_target(r)}
                         j = i + 1
                         while j < cnt:
-                            cj = int(body[j]['code'])
-                            if cj & 0x8000 or not 1 <= cj <= 20 or (cj - 1) % 5 not in (0, 1) or \
-                                    (cj - 1) // 5 in slots:
+                            t = _layer_target(body[j])
+                            if t is None or t in seen:
                                 break
                             run.append(j)
-                            slots.add((cj - 1) // 5)
+                            seen.add(t)
                             j += 1
                         if len(run) >= 2:
-                            by_slot = sorted(run, key=lambda x: (int(body[x]['code']) - 1) // 5)
-                            real = all((int(body[x]['code']) - 1) % 5 == 1 for x in run)
-                            mask = sum(1 << ((int(body[x]['code']) - 1) // 5) for x in run)
+                            by_t = sorted(run, key=lambda x: _layer_target(body[x]))
+                            real = all(_layer_real(body[x]) for x in run)
+                            mask = sum(1 << t for t in seen if t < 4)
+                            lmask = sum(1 << (t - 4) for t in seen if t >= 4)
                             g = r.copy()
-                            g['code'] = (136 if real else 120) + mask
+                            g['code'] = (176 if real else 160) + mask
+                            g['s1'] = lmask
                             g['mat'] = base + len(gather)
-                            for x in by_slot:
+                            for x in by_t:
                                 m0 = int(body[x]['mat'])
                                 gather.extend(range(m0, m0 + 4))
                             new.append(g)
@@ -842,15 +846,17 @@ class Packed:
             self._fop_of = {ri: fi for ri, fi in self.op_slots}
         codes = [int(c) for c in self.ops['code'][first:first + cnt]]
 
-        def cls(c):
-            if c & 0x8000:
-                return 'o'
-            if 1 <= c <= 20 and (c - 1) % 5 in (0, 1):
+        recs = self.ops[first:first + cnt]
+        tgt = [_layer_target(r) for r in recs]
+
+        def cls(j):
+            if tgt[j] is not None:
                 return 'r'
-            if 58 <= c <= 82:
+            c = codes[j]
+            if not c & 0x8000 and 58 <= c <= 82:
                 return 's'
             return 'o'
-        kinds = [cls(c) for c in codes]
+        kinds = [cls(j) for j in range(cnt)]
         fo = [self.fops[self._fop_of[i]] for i in idx]
         preds = []
         for j in range(cnt):
@@ -865,7 +871,7 @@ class Packed:
             ready = [j for j in range(cnt) if j not in done and preds[j] <= done]
             pick = None
             if cur == 'r':
-                pick = next((j for j in ready if kinds[j] == 'r' and (codes[j] - 1) // 5 not in slots), None)
+                pick = next((j for j in ready if kinds[j] == 'r' and tgt[j] not in slots), None)
             elif cur == 's':
                 pick = next((j for j in ready if kinds[j] == 's'), None)
             if pick is None:
@@ -876,7 +882,7 @@ class Packed:
                         break
                 cur = kinds[pick]
             if cur == 'r':
-                slots.add((codes[pick] - 1) // 5)
+                slots.add(tgt[pick])
             done.add(pick)
             order.append(pick)
         return np.array([idx[j] for j in order], np.int64)
@@ -893,6 +899,24 @@ class Packed:
         d = pool[m0:m0 + 4]
         pattern = sum(1 << k for k in range(4) if d[k].real < 0)
         return sel('ga', 'sa') | sel('gb', 'sb') << 8 | pattern << 16
+
+
+def _layer_target(r):
+    """Target of an op that can join a layer op (uncontrolled general / real
+    2x2 without a thread predicate): register slot 0..3, or 4 + lane bit; else None."""
+    c = int(r['code'])
+    if c & 0x8000:
+        return None
+    if 1 <= c <= 20 and (c - 1) % 5 in (0, 1):
+        return (c - 1) // 5
+    if c in (53, 54):
+        return 4 + int(r['s0']) - 16
+    return None
+
+
+def _layer_real(r) -> bool:
+    c = int(r['code'])
+    return c == 54 or (1 <= c <= 20 and (c - 1) % 5 == 1)
 
 
 def _clean_batch(m: np.ndarray) -> np.ndarray:

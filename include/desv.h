@@ -43,7 +43,8 @@ extern "C" {
 /* fused-pass op kinds (desv_op.kind) */
 #define DESV_OP_STAGE 0 /* start of a register stage: g[0..3] = tile-local bit positions */
 #define DESV_OP_M1 1    /* 2x2 on register slot s0 (0..3) or lane bit (s0 = 16 + bit, bit < 5) */
-#define DESV_OP_M2 2    /* 4x4 on register slots s0 < s1; row index = 2*bit(s1) + bit(s0) */
+#define DESV_OP_M2 2    /* 4x4 on register slots s0 < s1 (reserved: the host lowers every two-qubit
+                           gate to 2x2 / diagonal ops, and the pass kernels reject this kind) */
 #define DESV_OP_DIAG 3  /* diagonal on global bits ga, gb: factor d[bit(ga) + 2*bit(gb)] */
 #define DESV_OP_GRAD 4  /* adjoint passes only: add Re<lambda|G|phi> to gradient slot `param`;
                            s1 == 0: G = 2x2 generator on s0 (controls as M1),
@@ -78,7 +79,12 @@ typedef struct desv_op {
                         ascending slot); 152 a group of s0 +-1 diagonals whose entries are uint32
                         words at the matrix offset: a | b << 8 | pattern << 16 with a, b = register
                         slot 0..3, 0x40 | global bit, or 0xFF (absent), pattern bit k negating
-                        amplitudes with bit(a) + 2*bit(b) == k */
+                        amplitudes with bit(a) + 2*bit(b) == k; 160+M general 2x2 on the register
+                        slots in M and on the lane bits in the 5-bit mask s1, 176+M the same with
+                        real matrices (matrices: slots ascending, then lane bits ascending);
+                        192 2x2 on lane bit s0-16 with a register control (cslot) and/or the
+                        cmask/cval predicate.  Code 0 is invalid: the kernels skip the op and
+                        set the bad-plan device status. */
     uint8_t pad0;
     uint32_t mat;    /* first complex element of this op's matrix in the matrix pool */
     int32_t param;   /* adjoint plans: gradient slot of this op (-1: none) */

@@ -222,6 +222,22 @@ def _apply_coded(a, tg, op, g, mats, code):
             out = out.copy()
             out[:, lo], out[:, hi] = n0, n1
         return np.where(pred, out, a)
+    if 160 <= c <= 191:
+        real, mask = c >= 176, c - (176 if c >= 176 else 160)
+        lmask = int(op['s1']) & 0x1F
+        out = a.copy()
+        k = 0
+        tls = [g[S] for S in range(4) if (mask >> S) & 1] + [b for b in range(5) if (lmask >> b) & 1]
+        for tl in tls:
+            m = mats[m0 + 4 * k:m0 + 4 * k + 4].reshape(2, 2)
+            k += 1
+            lo = j[((j >> tl) & 1) == 0]
+            hi = lo | (1 << tl)
+            n0, n1 = _variant_pair(m, 1 if real else 0, out[:, lo], out[:, hi])
+            out[:, lo], out[:, hi] = n0, n1
+        return np.where(pred, out, a)
+    if c == 192:
+        return _apply(a, tg, op, g, mats)
     if c == 152:
         cnt = int(op['s0'])
         wpe = mats.dtype.itemsize // 4
