@@ -146,44 +146,70 @@ def _barrier(ws):
 # CPU baseline: the oracle (a NumPy restatement of the reference's eager path)
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(n=N_QUBITS, gates=3):
-    """Time `gates` single-gate passes of the workload at full size on the host
-    (complex64, like the workload); returns GB/s by the same algorithmic-byte rule."""
+def _fused_schedule(n, layers):
+    """(transpiled gate count, fused pass count) of the headline circuit -- host
+    code only (lowering + fusion), used to put both arms on one byte rule."""
+    import torch
+    from dense_evolution.circuits import fusion
+    from dense_evolution.circuits.compiler import QuantumTranspiler, default_tile_bits
+    from dense_evolution.workloads import brick_u3_circuit
+    target = QuantumTranspiler.transpile(brick_u3_circuit(n, layers, SEED))
+    _, _, packed = fusion.build(target, n, default_tile_bits(n, torch.complex64))
+    return len(target), len(packed.passes)
+
+
+def cpu_baseline(n=N_QUBITS, layers=LAYERS, gates=2, npasses=None):
+    """The CPU path of the reference algorithm (the NumPy oracle, complex64 like
+    the workload) on a bounded sample: `gates` transpiled gates of the headline
+    circuit, one full-state pass each.  The whole-circuit time is extrapolated
+    as (mean time per gate) x (transpiled gate count), and the value uses the
+    same rule as the GPU arm: fused passes x 2 x 2^n x 8 B / circuit time, so
+    the ratio of the two values is the speed-up on the same circuit.  `cores`
+    is measured: process CPU time / wall time over the sample."""
     from oracle import sv_oracle as O
     from dense_evolution.workloads import brick_u3_circuit
+    ngates, nfused = _fused_schedule(n, layers)
+    if npasses is not None:
+        nfused = npasses
     circ = O.transpile(brick_u3_circuit(n, 1, SEED))[:gates]
     sv = np.zeros(1 << n, dtype=np.complex64)
     sv[0] = 1
-    t0 = time.perf_counter()
+    c0, t0 = time.process_time(), time.perf_counter()
     for cmd in circ:
         sv = O.run_circuit(sv, n, [cmd], do_transpile=False)
     dt = time.perf_counter() - t0
-    gbs = len(circ) * 2 * (1 << n) * 8 / dt / 1e9
-    return {'value': gbs, 'unit': 'GB/s', 'cores': 1, 'kind': 'port',
-            'sample': f'{len(circ)} single-gate passes (first gates of layer 0) of the {n}-qubit complex64 '
-                      f'circuit through the NumPy oracle, {dt:.1f} s'}
+    cores = (time.process_time() - c0) / dt
+    per_gate = dt / len(circ)
+    est = per_gate * ngates
+    gbs = nfused * 2 * (1 << n) * 8 / est / 1e9
+    return {'value': gbs, 'unit': 'GB/s', 'cores': round(cores, 2), 'kind': 'port',
+            'sample': f'{len(circ)} transpiled gates ({", ".join(c[0] for c in circ)}) of the {n}-qubit complex64 '
+                      f'circuit through the NumPy oracle, {per_gate:.2f} s per gate, extrapolated to all '
+                      f'{ngates} gates ({est:.0f} s per circuit); bytes counted as {nfused} fused passes',
+            'est_circuit_s': est}
 
 
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    res = None
     t0 = time.perf_counter()
-    vals = []
+    vals, cores, last = [], [], None
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(N_QUBITS, gates=1)
+        r = cpu_baseline(args.qubits, args.layers, gates=1)
         if i >= args.warmup:
             vals.append(r['value'])
-        res = r
+            cores.append(r['cores'])
+        last = r
     v = float(np.mean(vals))
     line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'GB/s', 'n_gpus': args.gpus,
             'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'complex64', 'data': 'synthetic',
-            'config': {'workload': f'{N_QUBITS}-qubit complex64 random circuit, {LAYERS} layers of U3 + brick CZ '
-                                   f'(one reference pass per gate)', 'seed': SEED},
-            'cpu_baseline': {'value': v, 'unit': 'GB/s', 'cores': 1, 'kind': 'port',
-                             'sample': 'one single-gate pass per step at 30 qubits, NumPy oracle'},
+            'config': {'workload': f'{args.qubits}-qubit complex64 random circuit, {args.layers} layers of U3 on every '
+                                   f'qubit + brick-wall CZ', 'seed': SEED, 'qubits': args.qubits,
+                       'layers': args.layers},
+            'cpu_baseline': {'value': v, 'unit': 'GB/s', 'cores': float(np.mean(cores)), 'kind': 'port',
+                             'sample': 'per step: ' + last['sample']},
             'e2e': {'value': v, 'unit': 'GB/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
             'wall_s': time.perf_counter() - t0}
     print(json.dumps(line), flush=True)
@@ -288,7 +314,7 @@ def run_ours(args):
     torch.cuda.empty_cache()
     large = run_large(args) if not args.skip_large else None
     torch.cuda.empty_cache()
-    cpu = cpu_baseline() if (rank == 0 and ws == 1 and not args.skip_cpu) else None
+    cpu = cpu_baseline(n, layers, gates=2, npasses=npasses) if (rank == 0 and ws == 1 and not args.skip_cpu) else None
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,

@@ -315,3 +315,47 @@ def hea_xxz_batch(ns: Sequence[int], layers: int, jz: Sequence[float], jxy: floa
     with an open-chain XXZ Hamiltonian per circuit."""
     from .workloads import hea_circuit, xxz_terms
     return [(hea_circuit(n, layers), n, xxz_terms(n, z, jxy)) for n, z in zip(ns, jz)]
+
+
+# ---------------------------------------------------------------------------
+# several GPUs: circuits are independent, so a batch shards by circuit
+# ---------------------------------------------------------------------------
+
+def shard_items(qubits: Sequence[int], rank: int, world: int) -> List[int]:
+    """Indices of the circuits that `rank` of `world` runs.  Circuits are dealt
+    by decreasing cost (2^n amplitudes) to the rank with the least work so far,
+    ties to the lowest rank, so every rank computes the same partition without
+    communicating."""
+    if not 0 <= rank < world:
+        raise ValueError(f'rank {rank} not in [0, {world})')
+    order = sorted(range(len(qubits)), key=lambda i: (-(1 << int(qubits[i])), i))
+    load = [0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += 1 << int(qubits[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def gather_results(indices: Sequence[int], energies: Sequence[float], grads: Sequence[np.ndarray], total: int,
+                   group=None):
+    """Collect every rank's (index, energy, gradient) on all ranks through
+    torch.distributed (any backend with object collectives: gloo, nccl) and
+    return (energies, grads) in circuit order.  The only exchange of a sharded
+    batch: one gather of results after the launch."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    parts = [None] * world
+    dist.all_gather_object(parts, (list(indices), [float(e) for e in energies], [np.asarray(g) for g in grads]),
+                           group=group)
+    e_all = np.zeros(total)
+    g_all: List[np.ndarray] = [None] * total
+    for idx, es, gs in parts:
+        for i, e, g in zip(idx, es, gs):
+            e_all[i] = e
+            g_all[i] = g
+    if any(g is None for g in g_all):
+        raise RuntimeError('gather_results: some circuits were run by no rank')
+    return e_all, g_all
