@@ -13,7 +13,18 @@
 
 namespace desv {
 
-enum : int { V_GEN = 0, V_REAL, V_DIAG, V_PHASE1, V_ANTI };
+enum : int { V_GEN = 0, V_REAL, V_DIAG, V_PHASE1, V_ANTI, V_BREAL };
+
+// Element-wise products for real matrices stored duplicated as (v, v): one
+// packed FP32 instruction per complex amplitude on sm_100 (fma.rn.f32x2).
+__device__ __forceinline__ float2 bmul(const float2 &m, const float2 &x) { return __fmul2_rn(m, x); }
+__device__ __forceinline__ float2 bfma(const float2 &m, const float2 &x, const float2 &c) {
+    return __ffma2_rn(m, x, c);
+}
+__device__ __forceinline__ double2 bmul(const double2 &m, const double2 &x) { return make_double2(m.x * x.x, m.y * x.y); }
+__device__ __forceinline__ double2 bfma(const double2 &m, const double2 &x, const double2 &c) {
+    return make_double2(fma(m.x, x.x, c.x), fma(m.y, x.y, c.y));
+}
 
 __device__ __forceinline__ int m1_variant(int flags) {
     if (flags & DESV_F_PHASE1) return V_PHASE1;
@@ -58,6 +69,9 @@ __device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m) {
         } else if (VAR == V_REAL) {
             a[j] = rfma(m.m01.x, x1, rfma(m.m00.x, x0, mk(decltype(x0.x)(0), decltype(x0.x)(0))));
             a[j1] = rfma(m.m11.x, x1, rfma(m.m10.x, x0, mk(decltype(x0.x)(0), decltype(x0.x)(0))));
+        } else if (VAR == V_BREAL) {
+            a[j] = bfma(m.m01, x1, bmul(m.m00, x0));
+            a[j1] = bfma(m.m11, x1, bmul(m.m10, x0));
         } else {
             a[j] = cfma(m.m01, x1, cmul(m.m00, x0));
             a[j1] = cfma(m.m11, x1, cmul(m.m10, x0));
@@ -110,6 +124,7 @@ __device__ __forceinline__ void m1_lane_free(T (&a)[16], const M22<T> &m, int lb
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const T p = shfl_xor(a[j], 1 << lb);
+        if (VAR == V_BREAL) { a[j] = bfma(coth, p, bmul(cself, a[j])); continue; }
         if (VAR == V_ANTI) a[j] = cmul(coth, p);
         else if (VAR == V_REAL) a[j] = rfma(coth.x, p, rfma(cself.x, a[j], mk(decltype(p.x)(0), decltype(p.x)(0))));
         else a[j] = cfma(coth, p, cmul(cself, a[j]));
@@ -291,8 +306,10 @@ __device__ __forceinline__ void apply_one_op(T (&a)[16], const desv_op &op, cons
 #define DESV_CODE_MULTI 120u      // + slot mask 1..15: general 2x2 on each slot in the mask
 #define DESV_CODE_MULTI_REAL 136u // + slot mask: real 2x2 on each slot in the mask
 #define DESV_CODE_SIGNS 152u      // group of +-1 diagonals, s0 entries at the op's matrix offset
-#define DESV_CODE_LAYER 160u      // + slot mask 0..15: general 2x2 on those slots and on the lane bits in s1
-#define DESV_CODE_LAYER_REAL 176u // + slot mask: the same with real matrices
+#define DESV_CODE_DIAG_GROUP 154u // group of diagonals, s0 entries of 5 elements at the op's matrix offset
+#define DESV_CODE_LAYER 160u      // + slot mask 0..15: general 2x2 on those slots (packed form, 8 elements
+                                  // per matrix) and on the lane bits in s1 (plain form)
+#define DESV_CODE_LAYER_REAL 176u // + slot mask: the same with real matrices stored as (v, v) pairs
 #define DESV_CODE_LANE_CTL 192u   // 2x2 on lane bit s0-16 with a register control (cslot) and/or predicate
 
 template <int S, int CS, typename T>
@@ -376,6 +393,35 @@ __device__ __forceinline__ void signs_group(T (&a)[16], const uint32_t *e, int c
     for (int j = 0; j < 16; ++j) flip_sign(a[j], (neg << (31 - j)) & 0x80000000u);
 }
 
+// 2x2 on register slot S with the matrix in packed form: for every entry m the
+// pool holds A = (re m, re m) and B = (-im m, im m), so that
+// m x = A * x + B * swap(x) element-wise -- four packed FP32 instructions per
+// output amplitude (fma.rn.f32x2), the swapped inputs shared by both outputs.
+template <int S, typename T> __device__ __forceinline__ void m1_reg_packed(T (&a)[16], const T *mp) {
+    const T A00 = mp[0], B00 = mp[1], A01 = mp[2], B01 = mp[3], A10 = mp[4], B10 = mp[5], A11 = mp[6],
+            B11 = mp[7];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if (j & (1 << S)) continue;
+        const int j1 = j | (1 << S);
+        const T x0 = a[j], x1 = a[j1];
+        const T s0 = mk(x0.y, x0.x), s1 = mk(x1.y, x1.x);
+        a[j] = bfma(B01, s1, bfma(A01, x1, bfma(B00, s0, bmul(A00, x0))));
+        a[j1] = bfma(B11, s1, bfma(A11, x1, bfma(B10, s0, bmul(A10, x0))));
+    }
+}
+
+// packed-form gates on every register slot in M (8 elements per matrix)
+template <int M, typename T> __device__ __forceinline__ void multi_reg_packed(T (&a)[16], const T *mp) {
+    constexpr int k1 = (M & 1) ? 1 : 0;
+    constexpr int k2 = k1 + ((M & 2) ? 1 : 0);
+    constexpr int k3 = k2 + ((M & 4) ? 1 : 0);
+    if (M & 1) m1_reg_packed<0>(a, mp);
+    if (M & 2) m1_reg_packed<1>(a, mp + 8 * k1);
+    if (M & 4) m1_reg_packed<2>(a, mp + 8 * k2);
+    if (M & 8) m1_reg_packed<3>(a, mp + 8 * k3);
+}
+
 // 2x2 gates on the lane bits in `lmask` (bit b: lane bit b), commuting,
 // matrices consecutive (ascending lane bit).
 template <int VAR, typename T>
@@ -398,9 +444,116 @@ __device__ __forceinline__ void layer_op(T (&a)[16], const T *mp, uint32_t lmask
     multi_lane<VAR>(a, mp + 4 * nreg, lmask, lane);
 }
 
+// ---- diagonal groups (code DESV_CODE_DIAG_GROUP) ----------------------------
+// Entry i: element 5i holds the header word a | b << 8 | kind << 16 | sign
+// pattern << 20; elements 5i+1..5i+4 hold d[bit(a) + 2 bit(b)].  Entries with a
+// register slot are normalised on the host so that d[0] == 1.
+enum : uint32_t { DG_SIGN = 0, DG_THREAD = 1, DG_SLOT_A = 2, DG_SLOT_B = 3, DG_TWO = 4 };
+
+__device__ __forceinline__ uint32_t dg_bit(uint32_t x, uint64_t tg) {
+    return x == 0xFFu ? 0u : (uint32_t)((tg >> (x & 63u)) & 1ull);
+}
+
+template <typename T> __device__ __forceinline__ T cdiv(const T &x, const T &y) {
+    const auto inv = decltype(y.x)(1) / (y.x * y.x + y.y * y.y);
+    return mk((x.x * y.x + x.y * y.y) * inv, (x.y * y.x - x.x * y.y) * inv);
+}
+
+// amplitudes with register bit S == 0 times g0, == 1 times g1
+template <int S, typename T> __device__ __forceinline__ void dg_slot16(T (&a)[16], const T &g0, const T &g1) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) a[j] = cmul((j >> S) & 1 ? g1 : g0, a[j]);
+}
+// amplitudes with register bit S == 1 times r
+template <int S, typename T> __device__ __forceinline__ void dg_slot8(T (&a)[16], const T &r) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if ((j >> S) & 1) a[j] = cmul(r, a[j]);
+}
+template <typename T>
+__device__ __forceinline__ void dg_slot(T (&a)[16], uint32_t s, bool full, const T &g0, const T &g1) {
+    switch (s) {
+        case 0: if (full) dg_slot16<0>(a, g0, g1); else dg_slot8<0>(a, g1); break;
+        case 1: if (full) dg_slot16<1>(a, g0, g1); else dg_slot8<1>(a, g1); break;
+        case 2: if (full) dg_slot16<2>(a, g0, g1); else dg_slot8<2>(a, g1); break;
+        default: if (full) dg_slot16<3>(a, g0, g1); else dg_slot8<3>(a, g1); break;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void diag_group(T (&a)[16], const T *e, int cnt, uint64_t tg) {
+    using R = decltype(a[0].x);
+    const T one = mk(R(1), R(0));
+    T ps = one;
+    uint32_t neg = 0;
+    // thread-fixed factors (and the thread-dependent normalisation of slot entries)
+#pragma unroll 1
+    for (int i = 0; i < cnt; ++i) {
+        const uint32_t h = *reinterpret_cast<const uint32_t *>(e + 5 * i);
+        const uint32_t sa = h & 0xFFu, sb = (h >> 8) & 0xFFu, kind = (h >> 16) & 0xFu;
+        if (kind == DG_SIGN) {
+            const uint32_t ma1 = sign_bit_mask(sa, tg), mb1 = sign_bit_mask(sb, tg);
+            const uint32_t ma0 = ~ma1 & 0xFFFFu, mb0 = ~mb1 & 0xFFFFu;
+            const uint32_t p = h >> 20;
+            neg ^= (ma0 & mb0 & (0u - (p & 1u))) ^ (ma1 & mb0 & (0u - ((p >> 1) & 1u))) ^
+                   (ma0 & mb1 & (0u - ((p >> 2) & 1u))) ^ (ma1 & mb1 & (0u - ((p >> 3) & 1u)));
+        } else if (kind == DG_THREAD) {
+            ps = cmul(ps, e[5 * i + 1 + dg_bit(sa, tg) + 2 * dg_bit(sb, tg)]);
+        } else if (kind == DG_SLOT_A) {
+            if (dg_bit(sb, tg)) ps = cmul(ps, e[5 * i + 3]);
+        } else if (kind == DG_SLOT_B) {
+            if (dg_bit(sa, tg)) ps = cmul(ps, e[5 * i + 2]);
+        }
+    }
+    // register-slot factors; the first one also carries ps
+    bool first = true;
+#pragma unroll 1
+    for (int i = 0; i < cnt; ++i) {
+        const uint32_t h = *reinterpret_cast<const uint32_t *>(e + 5 * i);
+        const uint32_t sa = h & 0xFFu, sb = (h >> 8) & 0xFFu, kind = (h >> 16) & 0xFu;
+        if (kind == DG_SLOT_A || kind == DG_SLOT_B) {
+            const bool isa = kind == DG_SLOT_A;
+            const uint32_t v = dg_bit(isa ? sb : sa, tg);
+            const T *d = e + 5 * i + 1;
+            // factor for slot bit 0 / 1 at this thread's other bit v (f0 == 1 when v == 0)
+            const T f0 = v ? d[isa ? 2 : 1] : one;
+            const T f1 = v ? d[3] : d[isa ? 1 : 2];
+            const T r = v ? cdiv(f1, f0) : f1;
+            if (first) dg_slot(a, isa ? sa : sb, true, ps, cmul(ps, r));
+            else dg_slot(a, isa ? sa : sb, false, one, r);
+            first = false;
+        } else if (kind == DG_TWO) {
+            // two register slots (rare: a non-sign diagonal inside the register set);
+            // d[0] == 1, so only amplitudes with a slot bit set change
+            const T *d = e + 5 * i + 1;
+            const T d1 = d[1], d2 = d[2], d3 = d[3];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const uint32_t ba = (j >> sa) & 1u, bb = (j >> sb) & 1u;
+                if (ba | bb) a[j] = cmul(bb ? (ba ? d3 : d2) : d1, a[j]);
+            }
+        }
+    }
+    if (first) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) a[j] = cmul(ps, a[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) flip_sign(a[j], (neg << (31 - j)) & 0x80000000u);
+}
+
+// general layer with the register-slot matrices in packed form, then the lane
+// gates in plain form
+template <int M, typename T>
+__device__ __forceinline__ void layer_packed(T (&a)[16], const T *mp, uint32_t lmask, int lane) {
+    constexpr int nreg = ((M & 1) ? 1 : 0) + ((M & 2) ? 1 : 0) + ((M & 4) ? 1 : 0) + ((M & 8) ? 1 : 0);
+    if (M) multi_reg_packed<M>(a, mp);
+    multi_lane<V_GEN>(a, mp + 8 * nreg, lmask, lane);
+}
+
 #define DESV_LAYER(M)                                                                        \
-    case DESV_CODE_LAYER + M: layer_op<M, V_GEN>(a, mp, (w0.x >> 24) & 0x1Fu, lane); break;   \
-    case DESV_CODE_LAYER_REAL + M: layer_op<M, V_REAL>(a, mp, (w0.x >> 24) & 0x1Fu, lane); break;
+    case DESV_CODE_LAYER + M: layer_packed<M>(a, mp, (w0.x >> 24) & 0x1Fu, lane); break;     \
+    case DESV_CODE_LAYER_REAL + M: layer_op<M, V_BREAL>(a, mp, (w0.x >> 24) & 0x1Fu, lane); break;
 
 #define DESV_MULTI(M)                                              \
     case DESV_CODE_MULTI + M: multi_reg<M, V_GEN>(a, mp); break;   \
@@ -455,6 +608,7 @@ __device__ __forceinline__ void apply_op_head(T (&a)[16], const OpHead &h, const
         case DESV_CODE_SIGNS:
             signs_group(a, reinterpret_cast<const uint32_t *>(mp), (int)((w0.x >> 16) & 0xFFu), tg);
             break;
+        case DESV_CODE_DIAG_GROUP: diag_group(a, mp, (int)((w0.x >> 16) & 0xFFu), tg); break;
         case DESV_CODE_LANE_CTL:
             m1_lane(a, load_m22(mp), m1_variant((int)((w0.x >> 8) & 0xFFu)), (int)(int8_t)(w0.y & 0xFFu),
                     (int)((w0.x >> 16) & 0xFFu) - 16, (tg & opp->cmask) == opp->cval, lane);

@@ -235,6 +235,81 @@ def fuse_1q(gates: Sequence[IRGate], merge: bool = True) -> List[FOp]:
         out.append(FOp('scalar', src=[s]))
     for op in out:
         _classify(op)
+    if merge:
+        out = _merge_diagonals(out)
+    return out
+
+
+def _constant(op: FOp) -> bool:
+    return all(g.slot < 0 for g in op.src)
+
+
+def zyz(u: np.ndarray):
+    """u = D_post @ R @ D_pre with R = Ry(b) real and D_pre / D_post diagonal
+    (the global phase is folded into D_pre).  Returns (d_pre, r, d_post) or
+    None when the factors do not reproduce u to 1e-12."""
+    det = u[0, 0] * u[1, 1] - u[0, 1] * u[1, 0]
+    if abs(abs(det) - 1.0) > 1e-9:
+        return None
+    g = np.sqrt(det)
+    v = u / g                                   # SU(2): [[e^-ip c, -e^-im s], [e^im s, e^ip c]]
+    c, sn = abs(v[0, 0]), abs(v[1, 0])
+    b = 2.0 * np.arctan2(sn, c)
+    p = np.angle(v[1, 1]) if c > 1e-12 else 0.0          # (a + c') / 2
+    m = np.angle(v[1, 0]) if sn > 1e-12 else 0.0         # (a - c') / 2
+    a, cc = p + m, p - m
+    r = np.array([[np.cos(b / 2), -np.sin(b / 2)], [np.sin(b / 2), np.cos(b / 2)]], dtype=np.complex128)
+    d_pre = g * np.diag([np.exp(-0.5j * cc), np.exp(0.5j * cc)])
+    d_post = np.diag([np.exp(-0.5j * a), np.exp(0.5j * a)])
+    if np.max(np.abs(d_post @ r @ d_pre - u)) > 1e-12:
+        return None
+    return d_pre, r, d_post
+
+
+def _split_zyz(ops: List[FOp]) -> List[FOp]:
+    """Constant uncontrolled 2x2 ops with a general (complex, non-diagonal)
+    matrix become diagonal . real . diagonal.  The real middle factor costs
+    half the arithmetic of a general 2x2 on the device, and the diagonals
+    commute through cz / cp / controls and merge with their neighbours."""
+    out: List[FOp] = []
+    for op in ops:
+        if op.kind != 'm1' or op.cbits or not _constant(op) or not op.nd:
+            out.append(op)
+            continue
+        u = op.matrix(None)
+        if not np.any(u.imag) or (u[0, 0] == 0 and u[1, 1] == 0):
+            out.append(op)          # already real, or anti-diagonal (x / y-like)
+            continue
+        f = zyz(u)
+        if f is None:
+            out.append(op)
+            continue
+        for m in f:
+            kind_name = 'zyz_r' if m[0, 1] != 0 else 'zyz_d'
+            fo = FOp('m1', t=op.t, src=[IRGate('m1', kind_name, t=op.t, const=m)])
+            _classify(fo)
+            out.append(fo)
+    return out
+
+
+def _merge_diagonals(ops: List[FOp]) -> List[FOp]:
+    """Merge every constant uncontrolled 1-bit diagonal into the previous one on
+    the same bit when everything in between acts on that bit diagonally (or not
+    at all): the later diagonal commutes back past those ops."""
+    out: List[FOp] = []
+    open_: dict = {}
+    for op in ops:
+        if op.kind == 'm1' and not op.cbits and not op.nd and _constant(op):
+            j = open_.get(op.t)
+            if j is not None:
+                out[j].src.extend(op.src)
+                continue
+            open_[op.t] = len(out)
+            out.append(op)
+            continue
+        for b in _bits(op.nd):
+            open_.pop(b, None)
+        out.append(op)
     return out
 
 
@@ -722,7 +797,8 @@ class Packed:
         """Forward-pass op stream with runs of ops grouped (desv.h grouped codes).
 
         Inside a stage, a run of uncontrolled general / real 2x2 ops on distinct
-        register slots and lane bits becomes one layer op (the gates commute), and a run
+        register slots and lane bits becomes one layer op (the gates commute; the
+        matrices of an all-real layer are stored as (v, v) pairs), and a run
         of +-1 diagonals becomes one sign group, so the kernel dispatches once
         per run.  Ops are first reordered inside the stage (never across a
         non-commuting pair) to make the runs long.  Call after `materialize`
@@ -735,19 +811,28 @@ class Packed:
         tabs = pool[self.ops['mat'][sg].astype(np.int64)[:, None] + np.arange(4)] if len(sg) else pool[:0]
         key = codes.tobytes() + np.signbit(tabs.real).tobytes()
         cache = getattr(self, '_compact_cache', None)
-        if cache is None or cache[0] != key or cache[5] != len(pool):
-            cache = (key,) + self._compact_structure(pool) + (len(pool),)
+        if cache is None or cache[0] != key or cache[6] != len(pool) or cache[7] != pool.dtype:
+            cache = (key,) + self._compact_structure(pool) + (len(pool), pool.dtype)
             self._compact_cache = cache
-        _, ops, passes, gather, words, _ = cache
-        if words is None and not len(gather):
+        _, ops, passes, (gather, form), words, dv = cache[:6]
+        if words is None and not len(gather) and dv is None:
             return ops, passes, pool
-        ext = [pool, pool[gather]]
+        gathered = pool[gather]
+        # real layer matrices as (v, v); general register-slot matrices as the
+        # packed pairs (re, re), (-im, im): the kernel multiplies them element-wise
+        re_ = (form == 1) | (form == 2)
+        gathered[re_] = gathered[re_].real * (1 + 1j)
+        im_ = form == 3
+        gathered[im_] = gathered[im_].imag * (-1 + 1j)
+        ext = [pool, gathered]
+        wpe = pool.dtype.itemsize // 4
+        w = np.zeros(0 if words is None else (len(words) + wpe - 1) // wpe * wpe, np.uint32)
         if words is not None:
             # sign entries: raw uint32 words stored in whole pool elements
-            wpe = pool.dtype.itemsize // 4
-            w = np.zeros((len(words) + wpe - 1) // wpe * wpe, np.uint32)
             w[:len(words)] = words
-            ext.append(np.frombuffer(w.tobytes(), dtype=pool.dtype))
+        ext.append(np.frombuffer(w.tobytes(), dtype=pool.dtype))
+        if dv is not None:
+            ext.append(_diag_group_values(dv, pool))
         return ops, passes, np.concatenate(ext)
 
     def _compact_structure(self, pool):
@@ -759,6 +844,8 @@ class Packed:
         # sign-entry words go after the gathered matrices: offsets are fixed up
         # once the gather length is known
         sign_recs = []
+        form = []                     # gathered element: 0 plain, 1 (re, re), 2 (re, re) of packed, 3 (-im, im)
+        diag_recs, dvals = [], []     # diagonal groups: pool elements appended after the sign words
         for ps in self.passes:
             begin = len(out)
             k, end = int(ps['op_begin']), int(ps['op_end'])
@@ -792,30 +879,48 @@ class Packed:
                             g['mat'] = base + len(gather)
                             for x in by_t:
                                 m0 = int(body[x]['mat'])
-                                gather.extend(range(m0, m0 + 4))
+                                if real:
+                                    gather.extend(range(m0, m0 + 4))
+                                    form.extend([1] * 4)
+                                elif _layer_target(body[x]) < 4:
+                                    # register slot of a general layer: packed pairs per entry
+                                    for e in range(4):
+                                        gather.extend([m0 + e, m0 + e])
+                                        form.extend([2, 3])
+                                else:
+                                    gather.extend(range(m0, m0 + 4))
+                                    form.extend([0] * 4)
                             new.append(g)
                         else:
                             new.append(r.copy())
                         i = j
-                    elif not c & 0x8000 and 58 <= c <= 82:
+                    elif not c & 0x8000 and 58 <= c <= 107:
                         j = i
-                        ents = []
-                        while j < cnt:
+                        while j < cnt and j - i < 120:
                             cj = int(body[j]['code'])
-                            if cj & 0x8000 or not 58 <= cj <= 82 or len(ents) == 127:
+                            if cj & 0x8000 or not 58 <= cj <= 107:
                                 break
-                            ents.append(self._sign_word(body[j], pool))
                             j += 1
+                        run = body[i:j]
                         g = r.copy()
-                        g['code'] = 152
-                        g['s0'] = len(ents)
-                        sign_recs.append((g, nsign_words))
-                        words.extend(ents)
-                        nsign_words += len(ents)
-                        # keep every group's words whole-element aligned
-                        pad = (-nsign_words) % wpe
-                        words.extend([0] * pad)
-                        nsign_words += pad
+                        if all(58 <= int(x['code']) <= 82 for x in run):
+                            ents = [self._sign_word(x, pool) for x in run]
+                            g['code'] = 152
+                            g['s0'] = len(ents)
+                            sign_recs.append((g, nsign_words))
+                            words.extend(ents)
+                            nsign_words += len(ents)
+                            # keep every group's words whole-element aligned
+                            pad = (-nsign_words) % wpe
+                            words.extend([0] * pad)
+                            nsign_words += pad
+                        else:
+                            ents = _diag_group_plan(run, pool)
+                            g['code'] = 154
+                            g['s0'] = len(ents) // 5
+                            diag_recs.append((g, len(dvals)))
+                            gid = len(diag_recs) - 1
+                            dvals.extend((e, gid) for e in ents)
                         new.append(g)
                         i = j
                     else:
@@ -831,9 +936,26 @@ class Packed:
         wbase = base + len(gather)
         for g, w0 in sign_recs:
             g['mat'] = wbase + w0 // wpe
+        dbase = wbase + (len(words) + wpe - 1) // wpe
+        for g, d0 in diag_recs:
+            g['mat'] = dbase + d0
         ops = np.array(out, dtype=N.OP_DTYPE) if out else np.zeros(0, N.OP_DTYPE)
         passes = np.array(rows, dtype=self.passes.dtype) if rows else np.zeros(0, self.passes.dtype)
-        return ops, passes, np.array(gather, np.int64), (np.array(words, np.uint32) if words else None)
+        dv = None
+        if dvals:
+            # vectorised recipe of the diagonal-group elements (values come from the pool per call)
+            kind = np.array([{'raw': 0, 'fac': 1, 'gph': 2, 'raw1': 3}[e[0]] for e, _ in dvals], np.int8)
+            word = np.array([e[1] if e[0] == 'raw' else 0 for e, _ in dvals], np.uint64)
+            src = np.array([e[1] + e[2] if e[0] == 'fac' else 0 for e, _ in dvals], np.int64)
+            m0 = np.array([e[1] if e[0] == 'fac' else 0 for e, _ in dvals], np.int64)
+            norm = np.array([e[0] == 'fac' and e[3] for e, _ in dvals], bool)
+            grp = np.array([gid for _, gid in dvals], np.int64)
+            raw = np.zeros((len(dvals), pool.dtype.itemsize // 4), np.uint32)
+            raw[:, 0] = word.astype(np.uint32)
+            dv = dict(kind=kind, raw=np.frombuffer(raw.tobytes(), dtype=pool.dtype).copy(), src=src, m0=m0,
+                      norm=norm, grp=grp, ngroups=len(diag_recs))
+        gidx = np.array(gather, np.int64)
+        return ops, passes, (gidx, np.array(form, np.int8)), (np.array(words, np.uint32) if words else None), dv
 
     def _group_order(self, first: int, cnt: int) -> np.ndarray:
         """Record indices of one stage, reordered (respecting every non-commuting
@@ -853,7 +975,7 @@ class Packed:
             if tgt[j] is not None:
                 return 'r'
             c = codes[j]
-            if not c & 0x8000 and 58 <= c <= 82:
+            if not c & 0x8000 and 58 <= c <= 107:
                 return 's'
             return 'o'
         kinds = [cls(j) for j in range(cnt)]
@@ -875,11 +997,17 @@ class Packed:
             elif cur == 's':
                 pick = next((j for j in ready if kinds[j] == 's'), None)
             if pick is None:
+                # open the next group with the class that has the most ready ops
+                # (ties: diagonals, then layer gates, then the rest)
                 slots = set()
-                for want in ('r', 's', 'o'):
-                    pick = next((j for j in ready if kinds[j] == want), None)
-                    if pick is not None:
-                        break
+                best = None
+                for want in ('s', 'r', 'o'):
+                    cand = [j for j in ready if kinds[j] == want]
+                    if want == 'r':
+                        cand = list({tgt[j]: j for j in reversed(cand)}.values())
+                    if cand and (best is None or len(cand) > best[0]):
+                        best = (len(cand), min(cand))
+                pick = best[1]
                 cur = kinds[pick]
             if cur == 'r':
                 slots.add(tgt[pick])
@@ -899,6 +1027,69 @@ class Packed:
         d = pool[m0:m0 + 4]
         pattern = sum(1 << k for k in range(4) if d[k].real < 0)
         return sel('ga', 'sa') | sel('gb', 'sb') << 8 | pattern << 16
+
+
+DG_SIGN, DG_THREAD, DG_SLOT_A, DG_SLOT_B, DG_TWO = 0, 1, 2, 3, 4
+
+
+def _diag_group_values(dv, pool) -> np.ndarray:
+    """Pool elements of every diagonal group for the current pool values."""
+    out = dv['raw'].copy()
+    fac = dv['kind'] == 1
+    vals = pool[dv['src'][fac]].astype(np.complex128)
+    d0 = pool[dv['m0'][fac]].astype(np.complex128)
+    nrm = dv['norm'][fac]
+    vals = np.where(nrm, vals / np.where(nrm, d0, 1.0), vals)
+    out[fac] = vals
+    # global phase per group: the product of d[0] of its normalised entries (once per entry)
+    first = fac.copy()
+    first[np.nonzero(fac)[0]] = (dv['src'][fac] == dv['m0'][fac]) & nrm
+    gph = np.ones(dv['ngroups'], np.complex128)
+    np.multiply.at(gph, dv['grp'][first], pool[dv['m0'][first]].astype(np.complex128))
+    g = dv['kind'] == 2
+    out[g] = gph[dv['grp'][g]]
+    out[dv['kind'] == 3] = 1.0
+    return out
+
+
+def _diag_group_plan(run, pool) -> list:
+    """Element specs of a diagonal group (dispatch code 154): 5 pool elements
+    per entry, a raw header word (a | b << 8 | kind << 16 | sign pattern << 20)
+    then the four factors d[bit(a) + 2 bit(b)].  Entries touching a register
+    slot are normalised so that d[0] == 1 (the factor removed is a global phase,
+    carried by one extra thread-only entry), which lets the kernel apply them to
+    the amplitudes whose slot bits are set only.  Records whose code says +-1
+    become sign entries.  The structure depends on the records' codes only; the
+    factor values are read from the pool on every call (``_diag_group_values``).
+
+    Specs: ('raw', word) | ('fac', m0, k, normalise) | ('gph',)."""
+    def sel(r, gkey, skey):
+        sl = int(r[skey])
+        if sl >= 0:
+            return sl
+        g = int(r[gkey])
+        return 0xFF if g == 0xFF else 0x40 | g
+
+    out, any_norm = [], False
+    for r in run:
+        a, b = sel(r, 'ga', 'sa'), sel(r, 'gb', 'sb')
+        m0 = int(r['mat'])
+        if 58 <= int(r['code']) <= 82:
+            d = pool[m0:m0 + 4]
+            pattern = sum(1 << k for k in range(4) if d[k].real < 0)
+            if pattern:
+                out += [('raw', a | b << 8 | DG_SIGN << 16 | pattern << 20)] + [('raw', 0)] * 4
+            continue
+        ra, rb = a < 4, b < 4
+        kind = DG_THREAD if not (ra or rb) else DG_TWO if (ra and rb) else (DG_SLOT_A if ra else DG_SLOT_B)
+        norm = kind != DG_THREAD
+        any_norm |= norm
+        out += [('raw', a | b << 8 | kind << 16)] + [('fac', m0, k, norm) for k in range(4)]
+    if any_norm:
+        out += [('raw', 0xFF | 0xFF << 8 | DG_THREAD << 16)] + [('gph',)] * 4
+    if not out:
+        out = [('raw', 0xFF | 0xFF << 8 | DG_THREAD << 16)] + [('raw1',)] * 4
+    return out
 
 
 def _layer_target(r):

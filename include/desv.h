@@ -80,8 +80,12 @@ typedef struct desv_op {
                         words at the matrix offset: a | b << 8 | pattern << 16 with a, b = register
                         slot 0..3, 0x40 | global bit, or 0xFF (absent), pattern bit k negating
                         amplitudes with bit(a) + 2*bit(b) == k; 160+M general 2x2 on the register
-                        slots in M and on the lane bits in the 5-bit mask s1, 176+M the same with
-                        real matrices (matrices: slots ascending, then lane bits ascending);
+                        slots in M and on the lane bits in the 5-bit mask s1 (slot matrices ascending
+                        in packed form: per entry m the pair (re m, re m), (-im m, im m); then the
+                        lane matrices ascending, plain), 176+M the same with real matrices stored
+                        as (v, v) pairs, 4 elements per matrix; 154 a group of s0 diagonals, 5
+                        elements per entry (header word a | b << 8 | kind << 16 | signs << 20, then
+                        the 4 factors);
                         192 2x2 on lane bit s0-16 with a register control (cslot) and/or the
                         cmask/cval predicate.  Code 0 is invalid: the kernels skip the op and
                         set the bad-plan device status. */

@@ -226,16 +226,44 @@ def _apply_coded(a, tg, op, g, mats, code):
         real, mask = c >= 176, c - (176 if c >= 176 else 160)
         lmask = int(op['s1']) & 0x1F
         out = a.copy()
-        k = 0
-        tls = [g[S] for S in range(4) if (mask >> S) & 1] + [b for b in range(5) if (lmask >> b) & 1]
-        for tl in tls:
-            m = mats[m0 + 4 * k:m0 + 4 * k + 4].reshape(2, 2)
-            k += 1
+        k = m0
+        tls = [(g[S], True) for S in range(4) if (mask >> S) & 1] + [(b, False) for b in range(5) if (lmask >> b) & 1]
+        for tl, slot in tls:
+            if slot and not real:
+                pk = mats[k:k + 8]          # packed form: (re, re), (-im, im) per entry
+                m = (pk[0::2].real + 1j * pk[1::2].imag).reshape(2, 2)
+                k += 8
+            else:
+                m = mats[k:k + 4].reshape(2, 2)
+                k += 4
             lo = j[((j >> tl) & 1) == 0]
             hi = lo | (1 << tl)
             n0, n1 = _variant_pair(m, 1 if real else 0, out[:, lo], out[:, hi])
             out[:, lo], out[:, hi] = n0, n1
         return np.where(pred, out, a)
+    if c == 154:
+        cnt = int(op['s0'])
+        wpe = mats.dtype.itemsize // 4
+        raw = np.ascontiguousarray(mats).view(np.uint32)
+        f = np.ones(a.shape, dtype=np.complex128)
+
+        def bit(x):
+            if x < 4:
+                return ((j >> g[x]) & 1)[None, :]
+            if x == 0xFF:
+                return np.zeros((1, a.shape[1]), np.int64)
+            return _bit(tg, x & 63)
+        for e in range(cnt):
+            hdr = int(raw[(m0 + 5 * e) * wpe])
+            ba, bb = bit(hdr & 0xFF), bit((hdr >> 8) & 0xFF)
+            kind = (hdr >> 16) & 0xF
+            k = ba + 2 * bb
+            if kind == 0:
+                f = f * np.where(((hdr >> 20) >> k) & 1, -1.0, 1.0)
+            else:
+                d = mats[m0 + 5 * e + 1:m0 + 5 * e + 5]
+                f = f * d[k]
+        return np.where(pred, a * f, a)
     if c == 192:
         return _apply(a, tg, op, g, mats)
     if c == 152:

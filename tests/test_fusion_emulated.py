@@ -96,3 +96,34 @@ def test_adjoint_plan_gradient_matches_fd(n):
                                     for c in circ], n)
     fd = O.fd_gradient(theta, orows, n, terms, h=1e-5)
     assert np.allclose(grad, fd, atol=1e-7)
+
+
+def test_grouped_stream_follows_new_parameters():
+    """One parametric plan, two parameter vectors: the grouped stream (its cached
+    structure and its per-call values) must follow theta."""
+    n, kmax = 11, 10
+    rng = np.random.default_rng(3)
+    circ = []
+    for q in range(n):
+        circ += [('ry', q, 0.0), ('rz', q, 0.0)]
+    circ += [('cx', q, q + 1) for q in range(n - 1)]
+    circ += [('cp', 0, 6, 0.0), ('crz', 9, 2, 0.0), ('rz', 4, 0.0), ('cz', 3, 8), ('p', 7, 0.0)]
+    circ += [('h', q) for q in range(n)] + [('t', q) for q in range(0, n, 2)]
+    target = QuantumTranspiler.transpile(circ)
+    slots, k = [], 0
+    for c in target:
+        if c[0] in ('ry', 'rz', 'cp', 'crz', 'p'):
+            slots.append(k)
+            k += 1
+        else:
+            slots.append(-1)
+    _, _, packed = fusion.build(target, n, kmax, slots)
+    for trial in range(3):
+        theta = rng.uniform(-np.pi, np.pi, k)
+        mats = packed.materialize(theta, np.complex128)
+        ops, passes, pool = packed.compact(mats)
+        got = run_passes(O.zero_state(n), n, passes, ops, pool)
+        it = iter(theta)
+        ref_circ = [(c[0], *c[1:-1], next(it)) if s >= 0 else c for c, s in zip(target, slots)]
+        ref = O.run_circuit(O.zero_state(n), n, ref_circ)
+        assert np.max(np.abs(got - ref)) < 1e-12, trial
