@@ -374,20 +374,20 @@ __device__ __forceinline__ void flip_sign(double2 &v, uint32_t s) {
 }
 
 // A group of +-1 diagonals (cz, and cp / crz at angles that give signs): entry
-// i = a | b << 8 | pattern << 16, where pattern bit k negates the amplitudes
-// with bit(a) + 2 bit(b) == k.  The group's signs are folded into one 16-bit
-// mask per thread and applied once, as sign-bit flips.
+// i is three words -- the thread-fixed bits it reads (ta | tb << 8, 0x40 | global
+// bit or 0xFF) and four 16-bit negation masks over the register amplitudes,
+// one per value (bit ta) + 2 (bit tb), precomputed on the host.  The group's
+// signs fold into one mask per thread, applied once as sign-bit flips.
 template <typename T>
 __device__ __forceinline__ void signs_group(T (&a)[16], const uint32_t *e, int cnt, uint64_t tg) {
     uint32_t neg = 0;
 #pragma unroll 1
     for (int i = 0; i < cnt; ++i) {
-        const uint32_t w = e[i];
-        const uint32_t ma1 = sign_bit_mask(w & 0xFFu, tg), mb1 = sign_bit_mask((w >> 8) & 0xFFu, tg);
-        const uint32_t ma0 = ~ma1 & 0xFFFFu, mb0 = ~mb1 & 0xFFFFu;
-        const uint32_t p = w >> 16;
-        neg ^= (ma0 & mb0 & (0u - (p & 1u))) ^ (ma1 & mb0 & (0u - ((p >> 1) & 1u))) ^
-               (ma0 & mb1 & (0u - ((p >> 2) & 1u))) ^ (ma1 & mb1 & (0u - ((p >> 3) & 1u)));
+        const uint32_t sel = e[3 * i], ta = sel & 0xFFu, tb = (sel >> 8) & 0xFFu;
+        const uint32_t va = ta == 0xFFu ? 0u : (uint32_t)(tg >> (ta & 63u)) & 1u;
+        const uint32_t vb = tb == 0xFFu ? 0u : (uint32_t)(tg >> (tb & 63u)) & 1u;
+        const uint32_t w = e[3 * i + 1 + vb];
+        neg ^= va ? (w >> 16) : (w & 0xFFFFu);
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j) flip_sign(a[j], (neg << (31 - j)) & 0x80000000u);
@@ -397,9 +397,14 @@ __device__ __forceinline__ void signs_group(T (&a)[16], const uint32_t *e, int c
 // pool holds A = (re m, re m) and B = (-im m, im m), so that
 // m x = A * x + B * swap(x) element-wise -- four packed FP32 instructions per
 // output amplitude (fma.rn.f32x2), the swapped inputs shared by both outputs.
+template <typename T> __device__ __forceinline__ void load_packed8(const T *mp, T (&m)[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) m[k] = mp[k];
+}
 template <int S, typename T> __device__ __forceinline__ void m1_reg_packed(T (&a)[16], const T *mp) {
-    const T A00 = mp[0], B00 = mp[1], A01 = mp[2], B01 = mp[3], A10 = mp[4], B10 = mp[5], A11 = mp[6],
-            B11 = mp[7];
+    T m[8];
+    load_packed8(mp, m);
+    const T A00 = m[0], B00 = m[1], A01 = m[2], B01 = m[3], A10 = m[4], B10 = m[5], A11 = m[6], B11 = m[7];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         if (j & (1 << S)) continue;

@@ -904,9 +904,9 @@ class Packed:
                         run = body[i:j]
                         g = r.copy()
                         if all(58 <= int(x['code']) <= 82 for x in run):
-                            ents = [self._sign_word(x, pool) for x in run]
+                            ents = _sign_entries(run, pool)
                             g['code'] = 152
-                            g['s0'] = len(ents)
+                            g['s0'] = len(ents) // 3
                             sign_recs.append((g, nsign_words))
                             words.extend(ents)
                             nsign_words += len(ents)
@@ -1015,21 +1015,56 @@ class Packed:
             order.append(pick)
         return np.array([idx[j] for j in order], np.int64)
 
-    @staticmethod
-    def _sign_word(r, pool) -> int:
-        def sel(gkey, skey):
-            s = int(r[skey])
-            if s >= 0:
-                return s
-            g = int(r[gkey])
-            return 0xFF if g == 0xFF else 0x40 | g
+DG_SIGN, DG_THREAD, DG_SLOT_A, DG_SLOT_B, DG_TWO = 0, 1, 2, 3, 4
+
+
+def _sign_entries(run, pool) -> list:
+    """uint32 words of a sign group (dispatch code 152): 3 words per entry,
+    ``ta | tb << 8`` (the thread-fixed bits the entry reads: 0x40 | global bit,
+    0xFF if none) and the four 16-bit negation masks over the 16 register
+    amplitudes, one per value pair (bit ta) + 2 (bit tb), packed two per word.
+    Entries that read no thread bit fold into one constant mask."""
+    const_mask = 0
+    out = []
+    j = np.arange(16)
+    for r in run:
         m0 = int(r['mat'])
         d = pool[m0:m0 + 4]
-        pattern = sum(1 << k for k in range(4) if d[k].real < 0)
-        return sel('ga', 'sa') | sel('gb', 'sb') << 8 | pattern << 16
-
-
-DG_SIGN, DG_THREAD, DG_SLOT_A, DG_SLOT_B, DG_TWO = 0, 1, 2, 3, 4
+        pattern = [bool(d[k].real < 0) for k in range(4)]
+        sels = []
+        for gkey, skey in (('ga', 'sa'), ('gb', 'sb')):
+            sl, gb = int(r[skey]), int(r[gkey])
+            sels.append(('slot', sl) if sl >= 0 else ('none', 0) if gb == 0xFF else ('thread', gb))
+        tsel = [0x40 | v for k, v in sels if k == 'thread']
+        masks = []
+        for idx in range(4):
+            vals = {}
+            t = 0
+            for k, v in sels:
+                if k == 'thread':
+                    vals[len(vals)] = (idx >> t) & 1
+                    t += 1
+            bits = []
+            t = 0
+            for k, v in sels:
+                if k == 'slot':
+                    bits.append((j >> v) & 1)
+                elif k == 'thread':
+                    bits.append(np.full(16, (idx >> t) & 1))
+                    t += 1
+                else:
+                    bits.append(np.zeros(16, np.int64))
+            neg = np.array([pattern[x] for x in (bits[0] + 2 * bits[1])])
+            masks.append(int(np.sum(neg.astype(np.int64) << j)))
+        if not tsel:
+            const_mask ^= masks[0]
+            continue
+        ta = tsel[0]
+        tb = tsel[1] if len(tsel) > 1 else 0xFF
+        out += [ta | tb << 8, masks[0] | masks[1] << 16, masks[2] | masks[3] << 16]
+    if const_mask:
+        out += [0xFF | 0xFF << 8, const_mask | const_mask << 16, const_mask | const_mask << 16]
+    return out
 
 
 def _diag_group_values(dv, pool) -> np.ndarray:

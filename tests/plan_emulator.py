@@ -269,19 +269,20 @@ def _apply_coded(a, tg, op, g, mats, code):
     if c == 152:
         cnt = int(op['s0'])
         wpe = mats.dtype.itemsize // 4
-        words = np.ascontiguousarray(mats).view(np.uint32)[m0 * wpe:m0 * wpe + cnt]
-        neg = np.zeros(a.shape, dtype=bool)
+        words = np.ascontiguousarray(mats).view(np.uint32)[m0 * wpe:m0 * wpe + 3 * cnt]
+        neg = np.zeros(a.shape, dtype=np.int64)
 
-        def bit(x):
-            if x < 4:
-                return ((j >> g[x]) & 1)[None, :]
-            if x == 0xFF:
-                return np.zeros((1, a.shape[1]), np.int64)
-            return _bit(tg, x & 63)
-        for w in words:
-            w = int(w)
-            ba, bb = bit(w & 0xFF), bit((w >> 8) & 0xFF)
-            pat = (w >> 16) & 0xF
-            neg ^= ((pat >> (ba + 2 * bb)) & 1).astype(bool)
-        return np.where(pred & neg, -a, a)
+        def tbit(x):
+            return np.zeros_like(tg) if x == 0xFF else _bit(tg, x & 63)
+        for e in range(cnt):
+            sel, w1, w2 = (int(x) for x in words[3 * e:3 * e + 3])
+            va, vb = tbit(sel & 0xFF), tbit((sel >> 8) & 0xFF)
+            idx = va + 2 * vb                     # per amplitude row: which mask
+            masks = np.array([w1 & 0xFFFF, w1 >> 16, w2 & 0xFFFF, w2 >> 16], np.int64)
+            m = masks[idx]                        # [T, 2^K]
+            reg = np.zeros(a.shape[1], np.int64)  # register index of every tile position
+            for s_, gp in enumerate(g):
+                reg |= ((j >> gp) & 1) << s_
+            neg ^= (m >> reg[None, :]) & 1
+        return np.where(pred & (neg == 1), -a, a)
     raise AssertionError(f'unknown dispatch code {code}')
