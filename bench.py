@@ -219,16 +219,37 @@ def run_reference(args):
 # our arm
 # ---------------------------------------------------------------------------
 
-def run_ours(args):
+def fidelity_check(n=28, layers=LAYERS):
+    """Config 2's accuracy check: the headline circuit structure at n qubits in
+    complex64 against the same circuit in complex128 (the accuracy mode); both
+    on the GPU, untimed.  Returns fidelity |<a|b>|^2 and max |a - b|."""
     import torch
-    ws, rank, local = _dist()
-    if ws > 1:
-        import torch.distributed as dist
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(0)
+    import dense_evolution as de
+    from dense_evolution.circuits.compiler import CompiledCircuit
+    from dense_evolution.workloads import brick_u3_circuit
+    target = de.QuantumTranspiler.transpile(brick_u3_circuit(n, layers, SEED))
+    out = {}
+    states = []
+    for dt in (torch.complex64, torch.complex128):
+        sv = torch.zeros(1 << n, dtype=dt, device='cuda')
+        sv[0] = 1
+        CompiledCircuit(target, n, dt).run(sv)
+        states.append(sv)
+    a, b = states[0].to(torch.complex128), states[1]
+    out['qubits'] = n
+    out['fidelity_c64_vs_c128'] = float(torch.abs(torch.vdot(b, a)) ** 2)
+    out['max_abs_amp_error_c64'] = float((a - b).abs().max())
+    out['norm_c128'] = float(torch.vdot(b, b).real)
+    del a, b, states
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_headline(args, ws, local):
+    """The headline: fused passes of the brick-wall U3 circuit, timed per pass
+    with CUDA events on the launching stream; then the same metric end to end
+    through DenseSVSimulator."""
+    import torch
     import dense_evolution as de
     from dense_evolution import _native as N
     from dense_evolution.circuits.compiler import CompiledCircuit
@@ -294,7 +315,7 @@ def run_ours(args):
         sim.set_initial_state(None)
         plan_i = sim.compile(c)
         sim.run_circuit(c)
-        z = sim.expectation_z()
+        sim.expectation_z()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         if i >= args.warmup:
@@ -303,47 +324,60 @@ def run_ours(args):
             h2d = int(ops_i.numel() + mats_i.numel() * 4)
         sim._plans.clear()
     e2e_step = _max_over_ranks(float(np.mean(e2e_times)), ws)
-    e2e_passes = npasses
-    e2e_value = ws * e2e_passes * pass_bytes / e2e_step / 1e9
-
+    e2e_value = ws * npasses * pass_bytes / e2e_step / 1e9
     del sv, sim, ops_t, mats_t
     torch.cuda.empty_cache()
-    vqe = run_vqe(args) if not args.skip_vqe else None
+    return {
+        'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'complex64 (fp32 gate math)', 'data': 'synthetic',
+        'config': {'workload': f'{n}-qubit complex64 random circuit, {layers} layers of U3 on every qubit + '
+                               f'brick-wall CZ, fused into tile passes', 'seed': SEED, 'qubits': n,
+                   'layers': layers, 'fused_passes': npasses, 'tile_bits': plan.tile_bits,
+                   'l2': f'state ({(1 << n) * 8 / 2**30:.2f} GiB) larger than L2 (126 MB); no flush needed',
+                   'parallelism': f'replicas x{ws}'},
+        'passes_per_step': npasses, 'layers_per_s': ws * layers / (ms_step / 1e3),
+        'ms_per_layer': ms_step / layers, 'compile_s': compile_s,
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                     'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_src,
+                     'kernel': f'k_fused_pass<float2,{plan.tile_bits},3>',
+                     'algorithmic_bytes_per_launch': pass_bytes,
+                     'avg_launch_ms': avg_pass_ms, 'min_launch_ms': float(per_pass.min()),
+                     'max_launch_ms': float(per_pass.max())},
+        'e2e': {'value': e2e_value, 'unit': 'GB/s', 'h2d_bytes_per_step': h2d,
+                'd2h_bytes_per_step': (n + 1) * 8, 'ms_per_step': e2e_step * 1e3,
+                'path': 'DenseSVSimulator.run_circuit (new angles each step: transpile + fusion + upload) + '
+                        'expectation_z()'},
+        'gpu_launches': args.steps * npasses,
+        'clocks': clk.summary(),
+    }
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    line = run_headline(args, ws, local) if not args.skip_headline else {
+        'metric': METRIC, 'value': None, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,
+        'warmup': args.warmup, 'higher_is_better': True, 'skipped': 'headline (--skip-headline)'}
+    if not args.skip_headline and args.qubits == N_QUBITS:
+        line['fidelity_28q'] = fidelity_check(28, args.layers)
+    line['vqe'] = run_vqe(args) if not args.skip_vqe else None
     torch.cuda.empty_cache()
-    batch = run_batch(args) if not args.skip_batch else None
+    line['batch'] = run_batch(args) if not args.skip_batch else None
     torch.cuda.empty_cache()
-    large = run_large(args) if not args.skip_large else None
+    line['large'] = run_large(args) if not args.skip_large else None
     torch.cuda.empty_cache()
-    cpu = cpu_baseline(n, layers, gates=2, npasses=npasses) if (rank == 0 and ws == 1 and not args.skip_cpu) else None
+    npasses = line.get('passes_per_step')
+    line['cpu_baseline'] = cpu_baseline(args.qubits, args.layers, gates=2, npasses=npasses) \
+        if (rank == 0 and ws == 1 and not args.skip_cpu and not args.skip_headline) else None
     if rank == 0:
-        line = {
-            'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': None, 'dtype': 'complex64 (fp32 gate math)', 'data': 'synthetic',
-            'config': {'workload': f'{n}-qubit complex64 random circuit, {layers} layers of U3 on every qubit + '
-                                   f'brick-wall CZ, fused into tile passes', 'seed': SEED, 'qubits': n,
-                       'layers': layers, 'fused_passes': npasses, 'tile_bits': plan.tile_bits,
-                       'l2': f'state ({(1 << n) * 8 / 2**30:.2f} GiB) larger than L2 (126 MB); no flush needed',
-                       'parallelism': f'replicas x{ws}'},
-            'passes_per_step': npasses, 'layers_per_s': ws * layers / (ms_step / 1e3),
-            'ms_per_layer': ms_step / layers, 'compile_s': compile_s,
-            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                         'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_src,
-                         'kernel': f'k_fused_pass<float2,{plan.tile_bits},3>',
-                         'algorithmic_bytes_per_launch': pass_bytes,
-                         'avg_launch_ms': avg_pass_ms, 'min_launch_ms': float(per_pass.min()),
-                         'max_launch_ms': float(per_pass.max())},
-            'e2e': {'value': e2e_value, 'unit': 'GB/s', 'h2d_bytes_per_step': h2d,
-                    'd2h_bytes_per_step': (n + 1) * 8, 'ms_per_step': e2e_step * 1e3,
-                    'path': 'DenseSVSimulator.run_circuit (new angles each step: transpile + fusion + upload) + '
-                            'expectation_z()'},
-            'gpu_launches': args.steps * npasses,
-            'clocks': clk.summary(),
-            'cpu_baseline': cpu,
-            'vqe': vqe,
-            'batch': batch,
-            'large': large,
-        }
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -355,7 +389,7 @@ def run_vqe(args):
     import torch
     import dense_evolution as de
     from dense_evolution.workloads import hea_circuit, tfim_terms
-    n, layers = VQE_N, VQE_LAYERS
+    n, layers = args.vqe_qubits, VQE_LAYERS
     fn, npar = de.circuit_to_energy_fn(hea_circuit(n, layers), n, use_float32=True)
     prog = fn.program
     op = de.PauliSumOperator(tfim_terms(n), n)
@@ -370,6 +404,8 @@ def run_vqe(args):
     torch.cuda.synchronize()
     adj_s = (time.perf_counter() - t0) / reps
     # parameter shift on the same kernels: 2 * npar forward runs + <H>
+    if args.vqe_no_shift:
+        return {'energy': e, 'adjoint_grads_per_s': 1.0 / adj_s, 'adjoint_ms': adj_s * 1e3, 'qubits': n}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ps = prog.parameter_shift_grad(theta, op)
@@ -383,14 +419,20 @@ def run_vqe(args):
             'backward_passes': int(len(prog.back.passes)), 'adjoint_ms': adj_s * 1e3, 'shift_ms': ps_s * 1e3}
 
 
-def run_batch(args, ncirc=4096, layers=6):
+def run_batch(args, layers=6):
     """Config 4: 4096 circuits, n ~ U{10..20}, HEA of 6 layers, XXZ chain with J_z ~ U[0.5, 1.5];
-    energy + adjoint gradient of every circuit from one persistent launch (CUDA graph replay)."""
+    energy + adjoint gradient of every circuit from one persistent launch (CUDA graph replay).
+    The tile width comes from the autotuner, tuned first on a seeded 256-circuit sample."""
     import torch
+    from dense_evolution import autotune
     from dense_evolution.batch import BatchVQE, hea_xxz_batch
+    ncirc = args.batch_circuits
     rng = np.random.default_rng(SEED)
     ns = rng.integers(10, 21, ncirc)
     jz = rng.uniform(0.5, 1.5, ncirc)
+    srng = np.random.default_rng(SEED + 7)
+    sample = hea_xxz_batch(srng.integers(10, 21, 256), layers, srng.uniform(0.5, 1.5, 256))
+    tune = autotune.tune_batch(sample, use_float32=True)
     t0 = time.perf_counter()
     b = BatchVQE(hea_xxz_batch(ns, layers, jz), use_float32=True)
     build_s = time.perf_counter() - t0
@@ -420,7 +462,8 @@ def run_batch(args, ncirc=4096, layers=6):
             'ms_per_batch': ms, 'circuits_per_s': ncirc / (ms / 1e3), 'grads_per_s': ncirc / (ms / 1e3),
             'e2e_ms_per_batch': e2e_ms, 'plans': len(b.plans), 'launches_per_batch': 1,
             'total_amplitudes': amps, 'resident_circuits': int(np.sum(ns <= 12)),
-            'plan_build_s': build_s, 'energy_mean': float(np.mean(e))}
+            'plan_build_s': build_s, 'energy_mean': float(np.mean(e)), 'tile_bits': b.tile_bits,
+            'autotune_ms_per_launch_256': {str(k): v for k, v in tune.items()}}
 
 
 def run_large(args, n=32, n_ref=30, layers=4):
@@ -475,6 +518,10 @@ def main():
     ap.add_argument('--skip-cpu', action='store_true')
     ap.add_argument('--skip-batch', action='store_true')
     ap.add_argument('--skip-large', action='store_true')
+    ap.add_argument('--skip-headline', action='store_true')
+    ap.add_argument('--vqe-qubits', type=int, default=VQE_N, help='VQE block width (default 24)')
+    ap.add_argument('--vqe-no-shift', action='store_true', help='VQE block without the parameter-shift leg')
+    ap.add_argument('--batch-circuits', type=int, default=4096, help='batch block size (default 4096)')
     ap.add_argument('--qubits', type=int, default=N_QUBITS, help='headline circuit width (default 30)')
     ap.add_argument('--layers', type=int, default=LAYERS, help='headline circuit depth (default 40)')
     args = ap.parse_args()

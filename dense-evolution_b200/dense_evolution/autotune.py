@@ -89,3 +89,62 @@ def tune(n: int, dtype: torch.dtype, layers: int = 4, reps: int = 3, seed: int =
     best = min(res, key=res.get)
     record(n, dtype, best)
     return res
+
+
+# ---------------------------------------------------------------------------
+# batched VQE: tile width of the HBM-resident circuits (n > 12)
+# ---------------------------------------------------------------------------
+
+BATCH_SUPPORTED = (10, 11, 12)
+BATCH_DEFAULT = 12
+
+
+def _batch_key(dtype):
+    name = torch.cuda.get_device_name() if torch.cuda.is_available() else 'cpu'
+    return f'{name}|batch|{"c64" if dtype == torch.complex64 else "c128"}'
+
+
+def batch_tile_bits(dtype: torch.dtype) -> int:
+    """Tile bits of the batched-VQE plans: ``DESV_BATCH_TILE_BITS``, else the
+    tuned value cached for this GPU, else 12."""
+    env = os.environ.get('DESV_BATCH_TILE_BITS')
+    if env:
+        return int(env)
+    with _lock:
+        c = _load()
+        k = c.get(_batch_key(dtype)) if torch.cuda.is_available() else None
+    return int(k) if k else BATCH_DEFAULT
+
+
+def tune_batch(items, use_float32: bool = True, reps: int = 2, seed: int = 0) -> dict:
+    """Time one launch of BatchVQE over `items` at every supported tile width,
+    record the fastest for this GPU and return {K: ms per launch}."""
+    import numpy as np
+    from .batch import BatchVQE
+    dtype = torch.complex64 if use_float32 else torch.complex128
+    rng = np.random.default_rng(seed)
+    res = {}
+    for k in BATCH_SUPPORTED:
+        b = BatchVQE(items, use_float32=use_float32, tile_bits=k)
+        b.set_theta([rng.uniform(-np.pi, np.pi, n) for n in b.nparams_list()])
+        b.launch()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            b.launch()
+        e1.record()
+        torch.cuda.synchronize()
+        res[k] = e0.elapsed_time(e1) / reps
+        del b
+    best = min(res, key=res.get)
+    with _lock:
+        c = _load()
+        c[_batch_key(dtype)] = int(best)
+        try:
+            os.makedirs(os.path.dirname(_path()), exist_ok=True)
+            with open(_path(), 'w') as f:
+                json.dump(c, f, indent=1)
+        except OSError:
+            pass
+    return res

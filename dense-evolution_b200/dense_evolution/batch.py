@@ -87,7 +87,9 @@ class _Plan:
             raise ValueError(f'batched VQE needs at least {fusion.MIN_FUSED_QUBITS} qubits per circuit')
         self.n = n
         self.nparams = 1 + max([s for s in slots if s >= 0], default=-1)
-        K = min(n, tile_bits or RESIDENT_BITS)
+        # a resident state (<= 12 qubits) is one tile; wider states stream tiles of
+        # the tuned width
+        K = n if n <= RESIDENT_BITS else min(n, tile_bits or RESIDENT_BITS)
         self.K = K
         ir = fusion.lower(rows, n, slots)
         fops = fusion.fuse_1q(ir, merge=False)
@@ -165,6 +167,10 @@ class BatchVQE:
         self.dtype = torch.complex64 if use_float32 else torch.complex128
         self.device = N.require_cuda()
         N.lib()
+        if tile_bits is None:
+            from . import autotune
+            tile_bits = autotune.batch_tile_bits(self.dtype)
+        self.tile_bits = int(tile_bits)
         plans: Dict[tuple, int] = {}
         self.plans: List[_Plan] = []
         self.circ = []          # (plan index, coefficients, nparams)
@@ -267,6 +273,10 @@ class BatchVQE:
         self.graph = None
 
     # ------------------------------------------------------------------ run
+    def nparams_list(self) -> List[int]:
+        """Parameter count of every circuit, in item order."""
+        return [c[2] for c in self.circ]
+
     def set_theta(self, thetas: Sequence[np.ndarray]):
         """Copy every circuit's parameters (gate order) into the device buffer."""
         host = np.zeros(self.ntheta)

@@ -52,3 +52,20 @@ def test_batch_cuda_graph_replay():
     assert np.allclose(e0, e1) and all(np.allclose(x, y) for x, y in zip(g0, g1))
     assert np.allclose(e2, e3) and all(np.allclose(x, y) for x, y in zip(g2, g3))
     assert not np.allclose(e0, e2)
+
+
+@pytest.mark.parametrize('k', [10, 11])
+def test_batch_tile_widths_agree(k):
+    """Every tile width the autotuner may pick gives the same energies and
+    gradients (streamed circuits of 13-15 qubits; resident ones keep one tile)."""
+    from dense_evolution import _native as N
+    from dense_evolution.batch import BatchVQE, hea_xxz_batch
+    rng = np.random.default_rng(11)
+    ns = [13, 9, 15, 12, 14]
+    items = hea_xxz_batch(ns, 2, rng.uniform(0.5, 1.5, len(ns)))
+    th = [rng.uniform(-np.pi, np.pi, 4 * n) for n in ns]
+    e_ref, g_ref = BatchVQE(items, use_float32=False, tile_bits=12).run(th)
+    e, g = BatchVQE(items, use_float32=False, tile_bits=k).run(th)
+    assert np.allclose(e, e_ref, atol=1e-10)
+    assert all(np.allclose(x, y, atol=1e-10) for x, y in zip(g, g_ref))
+    assert N.device_status() in (None, 0)
