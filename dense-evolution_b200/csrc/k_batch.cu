@@ -67,8 +67,8 @@ __device__ __forceinline__ void run_recipe(const desv_batch_recipe &r, const dou
 // arrays).  Threads >= 2^(K-4) only take part in the barriers.
 template <typename T, bool ADJ>
 __device__ __forceinline__ void batch_stage(T *s0, T *s1, const desv_op &st, const desv_op *ops, int cnt,
-                                            const T *mats, uint64_t tg_base, const TileGeom &g, int active,
-                                            double *acc) {
+                                            const T *mats, uint64_t tg_base, const uint64_t *ctab, int L,
+                                            int active, double *acc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if ((int)threadIdx.x < active) {
         const uint32_t idx = stage_base(threadIdx.x, st.g);
@@ -80,21 +80,22 @@ __device__ __forceinline__ void batch_stage(T *s0, T *s1, const desv_op &st, con
             a[j] = s0[off];
             if (ADJ) b[j] = s1[off];
         }
-        const uint64_t tg = tg_base | tile_local_to_global(g, idx);
+        const uint64_t tg = tg_base | tl2g(ctab, L, idx);
         if (!ADJ) {
             run_stage_ops(a, ops, cnt, mats, tg, lane);
         } else {
 #pragma unroll 1
             for (int q = 0; q < cnt; ++q) {
-                const desv_op op = ops[q];
+                const desv_op &op = ops[q];
                 if (op.kind == DESV_OP_GRAD) {
                     double v = grad_term(a, b, op, mats + op.mat, tg, lane);
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    if (lane == 0 && op.param >= 0 && op.param < BATCH_MAXP) acc[warp * BATCH_MAXP + op.param] += v;
+                    const int prm = op.param;
+                    if (lane == 0 && prm >= 0 && prm < BATCH_MAXP) acc[warp * BATCH_MAXP + prm] += v;
                 } else {
-                    apply_one_op(a, op, mats, tg, lane);
-                    apply_one_op(b, op, mats, tg, lane);
+                    apply_op_at(a, ops + q, mats, tg, lane);
+                    apply_op_at(b, ops + q, mats, tg, lane);
                 }
             }
         }
@@ -111,13 +112,13 @@ __device__ __forceinline__ void batch_stage(T *s0, T *s1, const desv_op &st, con
 // All stages of one pass on one tile already in shared memory.
 template <typename T, bool ADJ>
 __device__ void batch_tile(T *s0, T *s1, const desv_op *ops, int nops, const T *mats, uint64_t base,
-                           const TileGeom &g, double *acc) {
-    const int active = 1 << (g.K - 4);
+                           const uint64_t *ctab, int K, int L, double *acc) {
+    const int active = 1 << (K - 4);
     int k = 0;
     while (k < nops) {
-        const desv_op st = ops[k];
+        const desv_op &st = ops[k];
         const int cnt = (int)st.mat;
-        batch_stage<T, ADJ>(s0, s1, st, ops + k + 1, cnt, mats, base, g, active, acc);
+        batch_stage<T, ADJ>(s0, s1, st, ops + k + 1, cnt, mats, base, ctab, L, active, acc);
         k += 1 + cnt;
     }
 }
@@ -125,7 +126,7 @@ __device__ void batch_tile(T *s0, T *s1, const desv_op *ops, int nops, const T *
 // one pass over a state (resident: the state is the single tile)
 template <typename T, bool ADJ>
 __device__ void batch_pass(T *gpsi, T *glam, T *spsi, T *slam, bool resident, const desv_pass &ps, int n,
-                           const desv_op *ops, const T *mats, double *acc) {
+                           const desv_op *ops, const T *mats, double *acc, uint64_t *ctab) {
     TileGeom g;
     g.n = n;
     g.K = ps.tile_bits;
@@ -143,41 +144,51 @@ __device__ void batch_pass(T *gpsi, T *glam, T *spsi, T *slam, bool resident, co
     const int nops = ps.op_end - ps.op_begin;
     // tiles must fit the shared-memory buffers and the 4-register-bit stages;
     // a resident state must be exactly one tile (host plans guarantee both)
-    if (g.K < 9 || g.K > BATCH_K || (resident && g.K != n) || g.K > n) {
+    if (g.K < 9 || g.K > BATCH_K || (resident && g.K != n) || g.K > n || g.L < 5) {
         if (threadIdx.x == 0) atomicOr(&g_dev_status, DESV_DEV_BADPLAN);
         return;
     }
+    // the pass's run table (global offset of each 2^L run of a tile); K - L <= 7
+    const uint32_t TILE = 1u << g.K, chunk = 1u << g.L, nch = 1u << (g.K - g.L);
+    for (uint32_t c = threadIdx.x; c < nch; c += blockDim.x) ctab[c] = chunk_offset(g, c);
+    __syncthreads();
     if (resident) {
-        batch_tile<T, ADJ>(spsi, slam, pops, nops, mats, 0, g, acc);
+        batch_tile<T, ADJ>(spsi, slam, pops, nops, mats, 0, ctab, g.K, g.L, acc);
+        __syncthreads();
         return;
     }
-    const uint32_t ntiles = 1u << (n - g.K), TILE = 1u << g.K, chunk = 1u << g.L, nch = 1u << (g.K - g.L);
+    // tile bases by a masked add over the rest bits
+    uint64_t rmask = 0;
+    for (int r = 0; r < g.nrest; ++r) rmask |= 1ull << g.rest[r];
+    const uint64_t one = rmask & (0ull - rmask);  // deposit of tile index 1
+    const uint32_t ntiles = 1u << (n - g.K);
+    uint64_t base = 0;
     for (uint32_t t = 0; t < ntiles; ++t) {
-        const uint64_t base = tile_base(g, t);
         for (uint32_t e = threadIdx.x; e < TILE; e += blockDim.x) {
-            const uint64_t gi = base + chunk_offset(g, e >> g.L) + (e & (chunk - 1));
+            const uint64_t gi = base + ctab[e >> g.L] + (e & (chunk - 1));
             spsi[e] = gpsi[gi];
             if (ADJ) slam[e] = glam[gi];
         }
         __syncthreads();
-        batch_tile<T, ADJ>(spsi, slam, pops, nops, mats, base, g, acc);
+        batch_tile<T, ADJ>(spsi, slam, pops, nops, mats, base, ctab, g.K, g.L, acc);
         for (uint32_t e = threadIdx.x; e < TILE; e += blockDim.x) {
-            const uint64_t gi = base + chunk_offset(g, e >> g.L) + (e & (chunk - 1));
+            const uint64_t gi = base + ctab[e >> g.L] + (e & (chunk - 1));
             gpsi[gi] = spsi[e];
             if (ADJ) glam[gi] = slam[e];
         }
         __syncthreads();
-        (void)nch;
+        base = ((base | ~rmask) + one) & rmask;
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(BATCH_THREADS) k_batch_vqe(desv_batch_args args, int *queue) {
+__global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_vqe(desv_batch_args args, int *queue) {
     extern __shared__ __align__(128) unsigned char smem[];
     T *sA = reinterpret_cast<T *>(smem);
     T *sB = sA + (1u << BATCH_K);
     double *acc = reinterpret_cast<double *>(sB + (1u << BATCH_K));
     double *red = acc + BATCH_NW * BATCH_MAXP;
+    __shared__ uint64_t s_ctab[1u << (BATCH_K - 5)];
     __shared__ int s_c;
     const int tid = threadIdx.x;
     T *wpsi = static_cast<T *>(args.workspace) + (size_t)blockIdx.x * 2 * args.ws_amps;
@@ -207,7 +218,7 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_vqe(desv_batch_args arg
         __threadfence_block();
         __syncthreads();
         for (int p = pl.fwd_begin; p < pl.fwd_end; ++p)
-            batch_pass<T, false>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc);
+            batch_pass<T, false>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc, s_ctab);
         // 3. lambda = H psi, E = <psi|lambda>
         double ere = 0;
         for (uint64_t i = tid; i < dim; i += blockDim.x) {
@@ -237,7 +248,7 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_vqe(desv_batch_args arg
         }
         // 4. adjoint sweep over (psi, lambda)
         for (int p = pl.bwd_begin; p < pl.bwd_end; ++p)
-            batch_pass<T, true>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc);
+            batch_pass<T, true>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc, s_ctab);
         __syncthreads();
         for (int q = tid; q < pl.nparams; q += blockDim.x) {
             double s = 0;
