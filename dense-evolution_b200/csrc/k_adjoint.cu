@@ -18,7 +18,7 @@
 namespace desv {
 
 template <typename T, int K, int NBUF>
-__global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, TileGeom g, const desv_op *ops,
+__global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam, TileGeom g, const desv_op *ops,
                                                                 int nops, const T *mats, int nparams, double *part) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
@@ -29,16 +29,23 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, T
     A.ptr[0] = phi;
     A.ptr[1] = lam;
     A.load[0] = A.load[1] = true;
-    A.store[0] = A.store[1] = true;
+    // the last register stage stores both arrays straight to HBM: the ring only
+    // serves loads, NBUF-1 tiles ahead
+    A.store[0] = A.store[1] = false;
     auto body = [&](T *const *sp, uint64_t base, uint64_t) {
         T *sphi = sp[0], *slam = sp[1];
+        const uint64_t *ctab = pipe_ctab(smem);
         int k = 0;
 #pragma unroll 1
         while (k < nops) {
-            const desv_op st = ops[k];
-            const int cnt = (int)st.mat;
-            const uint32_t idx = stage_base(threadIdx.x, st.g);
-            const uint32_t o0 = 1u << st.g[0], o1 = 1u << st.g[1], o2 = 1u << st.g[2], o3 = 1u << st.g[3];
+            // stage record: register bit positions g[0..3] (bytes 9..12), op count (mat)
+            const OpHead sh = load_head(ops + k);
+            const int cnt = (int)sh.mat;
+            const uint32_t g0 = (sh.w.z >> 8) & 0xFFu, g1 = (sh.w.z >> 16) & 0xFFu, g2 = sh.w.z >> 24,
+                           g3 = sh.w.w & 0xFFu;
+            const uint8_t gs8[4] = {(uint8_t)g0, (uint8_t)g1, (uint8_t)g2, (uint8_t)g3};
+            const uint32_t idx = stage_base(threadIdx.x, gs8);
+            const uint32_t o0 = 1u << g0, o1 = 1u << g1, o2 = 1u << g2, o3 = 1u << g3;
             T a[16], b[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
@@ -47,10 +54,10 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, T
                 a[j] = sphi[off];
                 b[j] = slam[off];
             }
-            const uint64_t tg = base | tl2g(pipe_ctab(smem), g.L, idx);
+            const uint64_t tg = base | tl2g(ctab, g.L, idx);
 #pragma unroll 1
             for (int q = 1; q <= cnt; ++q) {
-                const desv_op op = ops[k + q];
+                const desv_op &op = ops[k + q];
                 if (op.kind == DESV_OP_GRAD) {
                     double v = grad_term(a, b, op, mats + op.mat, tg, lane);
                     v = warp_sum_d(v);
@@ -60,15 +67,30 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_adjoint_pass(T *phi, T *lam, T
                     apply_op_at(b, ops + k + q, mats, tg, lane);
                 }
             }
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const uint32_t off = idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) +
-                                     ((j & 8) ? o3 : 0u);
-                sphi[off] = a[j];
-                slam[off] = b[j];
-            }
-            __syncthreads();
             k += 1 + cnt;
+            if (k >= nops) {
+                const uint64_t q0 = tl_bit(ctab, g.L, g0), q1 = tl_bit(ctab, g.L, g1), q2 = tl_bit(ctab, g.L, g2),
+                               q3 = tl_bit(ctab, g.L, g3);
+                T *outa = phi + tg, *outb = lam + tg;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const uint64_t off = ((j & 1) ? q0 : 0ull) + ((j & 2) ? q1 : 0ull) + ((j & 4) ? q2 : 0ull) +
+                                         ((j & 8) ? q3 : 0ull);
+                    outa[off] = a[j];
+                    outb[off] = b[j];
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const uint32_t off = idx + ((j & 1) ? o0 : 0u) + ((j & 2) ? o1 : 0u) + ((j & 4) ? o2 : 0u) +
+                                         ((j & 8) ? o3 : 0u);
+                    sphi[off] = a[j];
+                    slam[off] = b[j];
+                }
+                __syncthreads();
+                // the next bulk load into this slot (async proxy) must follow these writes
+                fence_proxy_async_smem();
+            }
         }
     };
     __syncthreads();

@@ -41,3 +41,29 @@ def test_32q_adjoint_consistency():
     assert sim_norm == pytest.approx(1.0, abs=1e-5)
     del psi
     torch.cuda.empty_cache()
+
+
+def test_config3_full_size_against_c128_fd():
+    """Config 3 at its full size: 24 qubits, HEA 10 layers (480 parameters),
+    TFIM.  complex64 adjoint gradient against complex128 central differences
+    (h = 1e-3) on a seeded subset of 8 parameters; energies c64 vs c128."""
+    import dense_evolution as de
+    from dense_evolution.workloads import hea_circuit, tfim_terms
+    n, layers = 24, 10
+    circ = hea_circuit(n, layers)
+    f64, npar = de.circuit_to_energy_fn(circ, n)
+    f32, _ = de.circuit_to_energy_fn(circ, n, use_float32=True)
+    assert npar == 480
+    theta = np.random.default_rng(2024).uniform(-np.pi, np.pi, npar)
+    op = de.PauliSumOperator(tfim_terms(n), n)
+    e32, g32, _ = f32.program.value_and_grad(theta, op)
+    e64 = float(f64(theta, op)[0])
+    assert abs(e32 - e64) <= 1e-6
+    h = 1e-3
+    idx = np.random.default_rng(7).choice(npar, 8, replace=False)
+    for i in idx:
+        tp, tm = theta.copy(), theta.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (float(f64(tp, op)[0]) - float(f64(tm, op)[0])) / (2 * h)
+        assert abs(g32[i] - fd) < 2e-5, (i, g32[i], fd)
