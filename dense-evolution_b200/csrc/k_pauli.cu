@@ -36,7 +36,10 @@ template <typename T, int K, int NBUF, int MODE>
 __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, TileGeom g, const desv_pauli_term *terms,
                                                          int nterms, int want_e, double *part) {
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr int NARR = MODE == 0 ? 1 : 2;
+    // only psi travels through the shared-memory ring; H psi is written (MODE 1)
+    // or accumulated (MODE 2) straight in HBM, amplitude j of a tile by thread
+    // j mod 256, so consecutive threads touch consecutive addresses
+    constexpr int NARR = 1;
     TermTab<T> *tab = reinterpret_cast<TermTab<T> *>(smem + PIPE_HDR_BYTES + (size_t)NBUF * NARR * (1u << K) * sizeof(T));
     for (int k = threadIdx.x; k < nterms; k += blockDim.x) {
         const desv_pauli_term tm = terms[k];
@@ -48,13 +51,10 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
     A.ptr[0] = const_cast<T *>(psi);
     A.load[0] = true;
     A.store[0] = false;
-    if (NARR == 2) {
-        A.ptr[NARR - 1] = out;
-        A.load[NARR - 1] = MODE == 2;
-        A.store[NARR - 1] = true;
-    }
+    const bool have_ctab = (1u << (K - g.L)) <= PIPE_CTAB_MAX;
     double ere = 0, eim = 0;
     auto body = [&](T *const *sp, uint64_t base, uint64_t) {
+        const uint64_t *ctab = pipe_ctab(smem);
         // parity of the tile's fixed bits under each term's sign mask
         for (int k = threadIdx.x; k < nterms; k += blockDim.x)
             tab->pb[k] = (uint8_t)(__popcll(base & terms[k].zmask) & 1);
@@ -82,12 +82,16 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
                 ere += (double)a.x * v.x + (double)a.y * v.y;
                 eim += (double)a.x * v.y - (double)a.y * v.x;
             }
-            if (MODE == 1) sp[NARR - 1][j] = mk((decltype(s[0].x))v.x, (decltype(s[0].x))v.y);
-            if (MODE == 2) {
-                T o = sp[NARR - 1][j];
-                o.x = (decltype(o.x))((double)o.x + v.x);
-                o.y = (decltype(o.y))((double)o.y + v.y);
-                sp[NARR - 1][j] = o;
+            if (MODE != 0) {
+                const uint64_t gi = base + (have_ctab ? tl2g(ctab, g.L, j) : tile_local_to_global(g, j));
+                if (MODE == 1) {
+                    out[gi] = mk((decltype(s[0].x))v.x, (decltype(s[0].x))v.y);
+                } else {
+                    T o = out[gi];
+                    o.x = (decltype(o.x))((double)o.x + v.x);
+                    o.y = (decltype(o.y))((double)o.y + v.y);
+                    out[gi] = o;
+                }
             }
         }
     };
@@ -127,7 +131,7 @@ static int launch_pauli(const T *psi, T *out, const TileGeom &g, const desv_paul
     static int bps[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
-    constexpr int NARR = MODE == 0 ? 1 : 2;
+    constexpr int NARR = 1;
     const size_t smem = PIPE_HDR_BYTES + (size_t)NBUF * NARR * (1u << K) * sizeof(T) + sizeof(TermTab<T>);
     if (bps[dev & 63] == 0) {
         cudaFuncSetAttribute(k_pauli<T, K, NBUF, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
