@@ -403,9 +403,11 @@ def run_vqe(args):
         e, g, _ = prog.value_and_grad(theta, op)
     torch.cuda.synchronize()
     adj_s = (time.perf_counter() - t0) / reps
+    pauli = pauli_roofline(prog, theta, n)
     # parameter shift on the same kernels: 2 * npar forward runs + <H>
     if args.vqe_no_shift:
-        return {'energy': e, 'adjoint_grads_per_s': 1.0 / adj_s, 'adjoint_ms': adj_s * 1e3, 'qubits': n}
+        return {'energy': e, 'adjoint_grads_per_s': 1.0 / adj_s, 'adjoint_ms': adj_s * 1e3, 'qubits': n,
+                'pauli': pauli}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ps = prog.parameter_shift_grad(theta, op)
@@ -416,7 +418,40 @@ def run_vqe(args):
             'parameter_shift_grads_per_s': 1.0 / ps_s, 'adjoint_over_parameter_shift': ps_s / adj_s,
             'max_abs_grad_diff_adjoint_vs_shift': float(np.max(np.abs(g - ps))),
             'forward_passes': int(len(prog.forward.packed.passes)),
-            'backward_passes': int(len(prog.back.passes)), 'adjoint_ms': adj_s * 1e3, 'shift_ms': ps_s * 1e3}
+            'backward_passes': int(len(prog.back.passes)), 'adjoint_ms': adj_s * 1e3, 'shift_ms': ps_s * 1e3,
+            'pauli': pauli}
+
+
+def pauli_roofline(prog, theta, n, reps=10):
+    """<H> and H|psi> of the TFIM chain on the VQE state, timed with CUDA events
+    on the launching stream; algorithmic bytes: every Pauli pass reads psi once
+    (<H>), and H|psi> also writes its output once and reads + writes it on every
+    further pass."""
+    import torch
+    from dense_evolution.physics.observables import plan_for
+    from dense_evolution.workloads import tfim_terms
+    psi = prog.forward_state(np.asarray(theta, dtype=np.float64))
+    plan = plan_for(tfim_terms(n), n, dtype=psi.dtype)
+    out = torch.empty_like(psi)
+    amp = (1 << n) * psi.element_size()
+    res = {'terms': int(plan.nterms), 'passes': int(plan.npasses)}
+    for name, fn, nbytes in (('expect', lambda: plan.expect(psi), plan.npasses * amp),
+                             ('matvec', lambda: plan.matvec(psi, out), plan.npasses * amp + amp +
+                              (plan.npasses - 1) * 2 * amp)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res[name] = {'ms': ms, 'algorithmic_bytes': nbytes, 'gbs': nbytes / ms / 1e6,
+                     'frac_of_hbm': nbytes / ms / 1e6 / _peaks()[0]}
+    del psi, out
+    return res
 
 
 def run_batch(args, layers=6):
