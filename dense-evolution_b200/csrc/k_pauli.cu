@@ -60,37 +60,61 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
             tab->pb[k] = (uint8_t)(__popcll(base & terms[k].zmask) & 1);
         __syncthreads();
         const T *s = sp[0];
+        // R amplitudes per thread at a time, each with its own FP64 accumulator:
+        // the term loop then carries R independent FMA chains instead of one
+        constexpr int R = 4;
 #pragma unroll 1
-        for (uint32_t j = threadIdx.x; j < (1u << K); j += PAULI_THREADS) {
-            double2 v = make_double2(0.0, 0.0);
+        for (uint32_t j0 = threadIdx.x; j0 < (1u << K); j0 += PAULI_THREADS * R) {
+            double2 v[R], p[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                v[r] = make_double2(0.0, 0.0);
+                p[r] = make_double2(0.0, 0.0);
+            }
             uint32_t last_x = 0xFFFFFFFFu;
-            double2 p = make_double2(0.0, 0.0);
-#pragma unroll 4
+#pragma unroll 2
             for (int k = 0; k < nterms; ++k) {
-                const uint32_t xl = tab->xl[k];
+                const uint32_t xl = tab->xl[k], zl = tab->zl[k];
+                const uint32_t pb = tab->pb[k];
                 if (xl != last_x) {
-                    const T q = s[j ^ xl];
-                    p = make_double2((double)q.x, (double)q.y);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const uint32_t j = j0 + (uint32_t)r * PAULI_THREADS;
+                        if (j < (1u << K)) {
+                            const T q = s[j ^ xl];
+                            p[r] = make_double2((double)q.x, (double)q.y);
+                        }
+                    }
                     last_x = xl;
                 }
-                const int sg = (__popc((j ^ xl) & tab->zl[k]) ^ tab->pb[k]) & 1;
                 const double2 c = tab->c[k];
-                v = sg ? cfma(cneg(c), p, v) : cfma(c, p, v);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const uint32_t j = j0 + (uint32_t)r * PAULI_THREADS;
+                    const bool sg = ((__popc((j ^ xl) & zl) ^ pb) & 1u) != 0;
+                    const double2 cs = sg ? make_double2(-c.x, -c.y) : c;
+                    v[r] = cfma(cs, p[r], v[r]);
+                }
             }
-            if (MODE != 0 || want_e) {
-                const T a = s[j];
-                ere += (double)a.x * v.x + (double)a.y * v.y;
-                eim += (double)a.x * v.y - (double)a.y * v.x;
-            }
-            if (MODE != 0) {
-                const uint64_t gi = base + (have_ctab ? tl2g(ctab, g.L, j) : tile_local_to_global(g, j));
-                if (MODE == 1) {
-                    out[gi] = mk((decltype(s[0].x))v.x, (decltype(s[0].x))v.y);
-                } else {
-                    T o = out[gi];
-                    o.x = (decltype(o.x))((double)o.x + v.x);
-                    o.y = (decltype(o.y))((double)o.y + v.y);
-                    out[gi] = o;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t j = j0 + (uint32_t)r * PAULI_THREADS;
+                if (j >= (1u << K)) continue;
+                if (MODE != 0 || want_e) {
+                    const T a = s[j];
+                    ere += (double)a.x * v[r].x + (double)a.y * v[r].y;
+                    eim += (double)a.x * v[r].y - (double)a.y * v[r].x;
+                }
+                if (MODE != 0) {
+                    const uint64_t gi = base + (have_ctab ? tl2g(ctab, g.L, j) : tile_local_to_global(g, j));
+                    if (MODE == 1) {
+                        out[gi] = mk((decltype(s[0].x))v[r].x, (decltype(s[0].x))v[r].y);
+                    } else {
+                        T o = out[gi];
+                        o.x = (decltype(o.x))((double)o.x + v[r].x);
+                        o.y = (decltype(o.y))((double)o.y + v[r].y);
+                        out[gi] = o;
+                    }
                 }
             }
         }
