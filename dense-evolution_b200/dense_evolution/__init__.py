@@ -19,6 +19,7 @@ from .physics.observables import (pauli_expectation, pauli_sum_expectation, paul
                                   pauli_sum_expectation_jax, PauliSumOperator)
 from .utils.measurement import sample_counts, statevector_fidelity
 from .solvers.autodiff import circuit_to_energy_fn
+from .noise import NoiseModel, NoiseSpec
 
 
 def set_precision(float64: bool = True) -> None:
@@ -31,4 +32,5 @@ __all__ = ['DenseSVSimulator', 'QASMParser', 'QASMCircuit', 'QuantumTranspiler',
            'PARAMETRIC_GATES', 'GATE_IDS', 'entangling_layer', 'VALID_PATTERNS', 'random_circuit',
            'pauli_expectation', 'pauli_sum_expectation', 'pauli_hamiltonian_to_matrix', 'pauli_sum_matvec',
            'multiply_pauli_terms', 'pauli_sum_matvec_jax', 'pauli_sum_expectation_jax', 'PauliSumOperator',
-           'sample_counts', 'statevector_fidelity', 'circuit_to_energy_fn', 'set_precision', '__version__']
+           'sample_counts', 'statevector_fidelity', 'circuit_to_energy_fn', 'set_precision', 'NoiseModel',
+           'NoiseSpec', '__version__']

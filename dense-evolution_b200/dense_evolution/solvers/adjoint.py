@@ -240,16 +240,45 @@ class AdjointProgram:
             grad += torch.from_numpy(acc).to(grad.device)
 
     # ------------------------------------------------------------ public
-    def energy(self, theta, h, stato_zero=None):
-        """(E as a float64 tensor -- differentiable when theta requires grad, psi)."""
+    def energy(self, theta, h, stato_zero=None, noise=None):
+        """(E as a float64 tensor -- differentiable when theta requires grad, psi).
+
+        ``noise`` (a NoiseSpec-like object: model, p, jax_key, qubits) applies one
+        stochastic Kraus shot to the circuit's output state before the energy,
+        as the reference's energy_fn does (solvers/autodiff.py:159-164).  For the
+        Pauli channels the shot is a fixed Pauli string P, so E = <psi|P H P|psi>
+        and the adjoint gradient runs with lambda = P H P psi; the damping
+        channels are not differentiable here."""
         if isinstance(theta, torch.Tensor) and theta.requires_grad:
             box = {}
-            e = _EnergyFunction.apply(theta, self, h, stato_zero, box)
+            e = _EnergyFunction.apply(theta, self, h, stato_zero, box, noise)
             return e, box['sv']
         th = _as_theta(theta)
         psi = self.forward_state(th, stato_zero)
+        if noise is not None:
+            psi, _ = self.apply_noise(psi, noise)
         _, e = self.apply_h(h, psi, need_lambda=False)
         return torch.tensor(e, dtype=torch.float64), psi
+
+    def apply_noise(self, psi: torch.Tensor, noise):
+        """(noisy normalised copy of psi, Pauli errors or None for damping channels)."""
+        from ..noise import kraus_channels as K
+        model, p = noise.model, float(noise.p)
+        out = psi.clone()
+        if model == 'ideal' or p <= 0.0:
+            return out, []
+        if model not in K.MODELS:
+            raise KeyError(model)
+        rng = K.resolve_rng(getattr(noise, 'rng', None), getattr(noise, 'jax_key', None))
+        qubits = list(noise.qubits) if getattr(noise, 'qubits', None) is not None else None
+        if model in K.PAULI_MODELS:
+            errs = K.draw_pauli_errors(model, p, self.n, rng, qubits)
+            K.apply_pauli_errors(out, self.n, errs)
+            K.normalize_plus_eps(out)
+            return out, errs
+        K.apply_channel(out, self.n, model, p, rng, qubits)
+        K.normalize_plus_eps(out)
+        return out, None
 
     def value_and_grad(self, theta, h, stato_zero=None):
         """(E, dE/dtheta as NumPy float64, psi) without autograd bookkeeping."""
@@ -309,17 +338,33 @@ def _split_params(specs, ops, cap):
 
 class _EnergyFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, theta_t, prog: AdjointProgram, h, stato_zero, box):
+    def forward(ctx, theta_t, prog: AdjointProgram, h, stato_zero, box, noise=None):
+        from ..noise import kraus_channels as K
         th = _as_theta(theta_t)
         psi = prog.forward_state(th, stato_zero)
-        lam, e = prog.apply_h(h, psi, need_lambda=True)
-        box['sv'] = psi
+        ctx.differentiable = True
+        if noise is None:
+            lam, e = prog.apply_h(h, psi, need_lambda=True)
+            box['sv'] = psi
+        else:
+            noisy, errs = prog.apply_noise(psi, noise)
+            lam, e = prog.apply_h(h, noisy, need_lambda=True)
+            box['sv'] = noisy
+            if errs is None:
+                ctx.differentiable = False
+            else:
+                # E = <psi|P H P|psi> (up to the (1 + 1e-15)^-2 of the final
+                # normalisation): lambda = P H (P psi); P is Hermitian
+                K.apply_pauli_errors(lam, prog.n, errs)
         ctx.prog, ctx.th, ctx.psi, ctx.lam = prog, th, psi, lam
         ctx.tdev, ctx.tdtype = theta_t.device, theta_t.dtype
         return torch.tensor(e, dtype=torch.float64, device=theta_t.device)
 
     @staticmethod
     def backward(ctx, g):
+        if not ctx.differentiable:
+            raise NotImplementedError('the gradient through an amplitude-damping channel (amplitude_damping, '
+                                      'combined) is not supported; the Pauli channels are')
         grad = ctx.prog.gradient(ctx.th, ctx.psi, ctx.lam)
         gt = torch.from_numpy(grad).to(device=ctx.tdev, dtype=ctx.tdtype)
-        return g * gt, None, None, None, None
+        return g * gt, None, None, None, None, None

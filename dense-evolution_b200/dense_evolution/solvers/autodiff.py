@@ -77,9 +77,7 @@ def circuit_to_energy_fn(circuit, n_qubits: int, use_float32: bool = False) -> T
     prog = adjoint.AdjointProgram(rows, slots, n_qubits, torch.complex64 if use_float32 else torch.complex128)
 
     def energy_fn(theta, h_matrix, stato_zero=None, noise=None):
-        if noise is not None:
-            raise NotImplementedError('noise= is not supported by the GPU energy function')
-        return prog.energy(theta, h_matrix, stato_zero)
+        return prog.energy(theta, h_matrix, stato_zero, noise)
 
     energy_fn.program = prog
     energy_fn.n_params = n_params

@@ -379,3 +379,75 @@ def fd_gradient(theta, rows, n, terms, h=1e-3, indices=None) -> np.ndarray:
         tm[i] -= h
         g[j] = (energy(tp, rows, n, terms)[0] - energy(tm, rows, n, terms)[0]) / (2 * h)
     return g
+
+
+# ---------------------------------------------------------------------------
+# stochastic single-qubit Kraus channels, NumPy branch
+# (dense_evolution/noise/kraus_channels.py:104-236 and noise/kraus/*.py)
+# ---------------------------------------------------------------------------
+
+NOISE_MODELS = ['ideal', 'depolarizing', 'bitflip', 'phaseflip', 'amplitude_damping', 'combined']
+
+
+def _noise_pairs(dim: int, q: int):
+    """Index pairs of qubit q: bit q of the amplitude index (LSB-first here,
+    unlike the simulator's MSB-first order) -- kraus_channels.py:60-80."""
+    i = np.arange(dim)
+    i0 = i[(i >> q) & 1 == 0]
+    return i0, i0 | (1 << q)
+
+
+def _noise_pauli(v, i0, i1, which):
+    a0, a1 = v[i0].copy(), v[i1].copy()
+    if which == 'x':
+        v[i0], v[i1] = a1, a0
+    elif which == 'y':
+        v[i0], v[i1] = -1j * a1, 1j * a0
+    else:
+        v[i1] = -a1
+
+
+def _noise_depolarizing(v, i0, i1, p, rng):        # kraus/depolarizing.py
+    r, ch = rng.random(), rng.random()
+    if r < p:
+        _noise_pauli(v, i0, i1, 'x' if ch < 1.0 / 3.0 else 'y' if ch < 2.0 / 3.0 else 'z')
+
+
+def _noise_damping(v, i0, i1, p, rng):             # kraus/amplitude_damping.py
+    gamma = float(np.clip(p, 0.0, 1.0))
+    r = rng.random()
+    a0, a1 = v[i0].copy(), v[i1].copy()
+    p1 = float(np.clip(gamma * np.sum(np.abs(a1) ** 2), 0.0, 1.0))
+    if r < p1:
+        v[i0] = a1 * np.sqrt(gamma) / np.sqrt(max(p1, 1e-15))
+        v[i1] = 0.0
+    else:
+        nn = np.sqrt(max(1.0 - p1, 1e-15))
+        v[i0] = a0 / nn
+        v[i1] = a1 * np.sqrt(1.0 - gamma) / nn
+
+
+def noise_apply(sv, n, model, p, rng, qubits=None):
+    """NoiseModel.apply_to_sv, NumPy branch: per target qubit one channel step
+    with the draws in the reference's order, then division by (norm + 1e-15)."""
+    if model == 'ideal' or p <= 0.0:
+        return sv
+    if model not in NOISE_MODELS:
+        raise KeyError(model)
+    v = np.array(sv, dtype=np.complex128).copy()
+    for q in (list(range(n)) if qubits is None else list(qubits)):
+        i0, i1 = _noise_pairs(len(v), q)
+        if model == 'depolarizing':
+            _noise_depolarizing(v, i0, i1, p, rng)
+        elif model == 'bitflip':
+            if rng.random() < p:
+                _noise_pauli(v, i0, i1, 'x')
+        elif model == 'phaseflip':
+            if rng.random() < p:
+                _noise_pauli(v, i0, i1, 'z')
+        elif model == 'amplitude_damping':
+            _noise_damping(v, i0, i1, p, rng)
+        else:                                     # combined (kraus/combined.py)
+            _noise_depolarizing(v, i0, i1, p * 0.5, rng)
+            _noise_damping(v, i0, i1, p * 0.333333, rng)
+    return v / (np.linalg.norm(v) + 1e-15)

@@ -1,0 +1,25 @@
+"""The oracle's restatement of the stochastic Kraus channels against fixtures
+produced by the reference itself (tests/golden/make_noise_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import sv_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), 'golden', 'golden_noise.npz')
+
+
+def _cases():
+    z = np.load(GOLD)
+    for k in range(int(z['ncases'][0])):
+        n, p, seed, mi = z[f'c{k}_meta']
+        q = list(z[f'c{k}_qubits']) if bool(z[f'c{k}_hasq'][0]) else None
+        yield (str(z['models'][int(mi)]), int(n), float(p), int(seed), q, z[f'c{k}_in'], z[f'c{k}_out'])
+
+
+@pytest.mark.parametrize('case', list(_cases()), ids=lambda c: f'{c[0]}-n{c[1]}-p{c[2]}-s{c[3]}')
+def test_oracle_noise_matches_reference(case):
+    model, n, p, seed, q, v, ref = case
+    got = O.noise_apply(v, n, model, p, np.random.default_rng(seed), q)
+    assert np.max(np.abs(np.asarray(got) - ref)) < 1e-12
