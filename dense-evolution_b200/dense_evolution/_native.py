@@ -62,6 +62,9 @@ _SIGS = {
     'desv_batch_workspace_bytes': ([_i, _i, _i], _sz),
     'desv_batch_vqe': ([_i, _i, _i, _vp, _vp, _sz, _vp], _i),
     'desv_adjoint_passes': ([_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp], _i),
+    'desv_sample_scratch_bytes': ([_i], _sz),
+    'desv_sample_prepare': ([_vp, _i, _i, _vp, _sz, _vp, _vp], _i),
+    'desv_sample_pick': ([_vp, _i, _i, _vp, _sz, _vp, ctypes.c_int64, _vp, _vp], _i),
 }
 OPTIONAL = set()
 

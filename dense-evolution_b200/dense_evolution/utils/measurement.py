@@ -40,7 +40,14 @@ def statevector_fidelity(statevector_a, statevector_b) -> float:
 
 
 def sample_counts(statevector, n_shots, rng=None):
-    """Finite-shot counts {'bitstring': count} (qubit 0 = leftmost character)."""
+    """Finite-shot counts {'bitstring': count} (qubit 0 = leftmost character)
+    of n_shots projective measurements in the computational basis
+    (utils/measurement.py:17-68 of the reference).
+
+    The distribution stays on the GPU: FP64 block sums and their prefix form
+    the CDF, and one warp per shot searches it.  The uniforms are drawn on the
+    host as ``rng.random(n_shots)`` -- the draws ``rng.choice`` makes -- so a
+    seeded generator gives the reference's samples."""
     a = _as_state(statevector)
     dim = a.shape[0]
     n = dim.bit_length() - 1
@@ -48,18 +55,24 @@ def sample_counts(statevector, n_shots, rng=None):
         raise ValueError(f"statevector length {dim} is not a power of 2")
     if n_shots < 1:
         raise ValueError(f"n_shots must be >= 1, got {n_shots}")
-    probs = torch.empty(dim, dtype=torch.float64, device=a.device)
     if a.dtype not in (torch.complex64, torch.complex128):
         a = a.to(torch.complex128)
-    N.check(N.lib().desv_probabilities(ctypes.c_void_p(a.data_ptr()), n, N.dtype_code(a),
-                                       ctypes.c_void_p(probs.data_ptr()), ctypes.c_void_p(N.stream_ptr())),
-            'probabilities')
-    p = probs.cpu().numpy()
-    total = p.sum()
-    if not np.isfinite(total) or total <= 0:
+    lib, st = N.lib(), ctypes.c_void_p(N.stream_ptr())
+    nbytes = int(lib.desv_sample_scratch_bytes(n))
+    scratch = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=a.device)
+    total = torch.empty(1, dtype=torch.float64, device=a.device)
+    N.check(lib.desv_sample_prepare(ctypes.c_void_p(a.data_ptr()), n, N.dtype_code(a),
+                                    ctypes.c_void_p(scratch.data_ptr()), scratch.numel() * 8,
+                                    ctypes.c_void_p(total.data_ptr()), st), 'sample prepare')
+    t = float(total.item())
+    if not np.isfinite(t) or t <= 0:
         raise ValueError("statevector has zero or non-finite total probability")
-    p = p / total
     rng = np.random.default_rng() if rng is None else rng
-    outcomes = rng.choice(dim, size=n_shots, p=p)
-    values, freqs = np.unique(outcomes, return_counts=True)
-    return {format(int(v), f'0{n}b'): int(f) for v, f in zip(values, freqs)}
+    u = torch.from_numpy(rng.random(int(n_shots))).to(a.device)
+    idx = torch.empty(int(n_shots), dtype=torch.int64, device=a.device)
+    N.check(lib.desv_sample_pick(ctypes.c_void_p(a.data_ptr()), n, N.dtype_code(a),
+                                 ctypes.c_void_p(scratch.data_ptr()), scratch.numel() * 8,
+                                 ctypes.c_void_p(u.data_ptr()), int(n_shots), ctypes.c_void_p(idx.data_ptr()), st),
+            'sample pick')
+    values, freqs = torch.unique(idx, return_counts=True)
+    return {format(int(v), f'0{n}b'): int(f) for v, f in zip(values.cpu().numpy(), freqs.cpu().numpy())}

@@ -258,6 +258,17 @@ int desv_probabilities(const void *sv, int n, int dtype, double *probs_dev, void
 /* measurement collapse: zero amplitudes whose bit `bit` != outcome, scale the rest by `scale` */
 int desv_collapse(void *sv, int n, int dtype, int bit, int outcome, double scale, void *stream);
 
+/* ---- finite-shot sampling (replaces the host path of sample_counts,
+ *      utils/measurement.py:17-68: rng.choice over |a|^2) ------------------- */
+size_t desv_sample_scratch_bytes(int n);
+/* Block sums and CDF of |a_i|^2 in scratch (FP64); *total_dev = sum |a_i|^2. */
+int desv_sample_prepare(const void *sv, int n, int dtype, void *scratch, size_t scratch_bytes, double *total_dev,
+                        void *stream);
+/* out_dev[s] = first index i with cumsum(|a|^2)[i] > u_dev[s] * total (numpy's
+ * searchsorted(cdf, u, 'right')); needs the scratch of desv_sample_prepare. */
+int desv_sample_pick(const void *sv, int n, int dtype, const void *scratch, size_t scratch_bytes,
+                     const double *u_dev, int64_t nshots, int64_t *out_dev, void *stream);
+
 /* ---- Pauli sums (replaces pauli_sum_expectation / pauli_sum_matvec,
  *      physics/observables.py:63-186,250-308) ------------------------------- */
 /* out_dev[0..1] = sum_k <psi|c_k P_k|psi> (re, im), FP64 accumulation. */

@@ -451,3 +451,24 @@ def noise_apply(sv, n, model, p, rng, qubits=None):
             _noise_depolarizing(v, i0, i1, p * 0.5, rng)
             _noise_damping(v, i0, i1, p * 0.333333, rng)
     return v / (np.linalg.norm(v) + 1e-15)
+
+
+def sample_counts(statevector, n_shots, rng=None):
+    """Finite-shot counts (utils/measurement.py:17-68): probabilities |a|^2,
+    normalised, sampled with ``rng.choice`` (cumsum + searchsorted of
+    ``rng.random(n_shots)``); keys are bitstrings with qubit 0 leftmost."""
+    sv = np.asarray(statevector)
+    dim = sv.shape[0]
+    n = dim.bit_length() - 1
+    if 1 << n != dim:
+        raise ValueError(f"statevector length {dim} is not a power of 2")
+    if n_shots < 1:
+        raise ValueError(f"n_shots must be >= 1, got {n_shots}")
+    probs = np.abs(sv) ** 2
+    total = probs.sum()
+    if not np.isfinite(total) or total <= 0:
+        raise ValueError("statevector has zero or non-finite total probability")
+    rng = np.random.default_rng() if rng is None else rng
+    idx = rng.choice(dim, size=n_shots, p=probs / total)
+    v, f = np.unique(idx, return_counts=True)
+    return {format(int(a), f'0{n}b'): int(b) for a, b in zip(v, f)}
