@@ -32,7 +32,8 @@ __global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam
     // the last register stage stores both arrays straight to HBM: the ring only
     // serves loads, NBUF-1 tiles ahead
     A.store[0] = A.store[1] = false;
-    auto body = [&](T *const *sp, uint64_t base, uint64_t) {
+    const int L = g.L;
+    auto body = [=](T *const *sp, uint64_t base, uint64_t) {
         T *sphi = sp[0], *slam = sp[1];
         const uint64_t *ctab = pipe_ctab(smem);
         int k = 0;
@@ -43,8 +44,7 @@ __global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam
             const int cnt = (int)sh.mat;
             const uint32_t g0 = (sh.w.z >> 8) & 0xFFu, g1 = (sh.w.z >> 16) & 0xFFu, g2 = sh.w.z >> 24,
                            g3 = sh.w.w & 0xFFu;
-            const uint8_t gs8[4] = {(uint8_t)g0, (uint8_t)g1, (uint8_t)g2, (uint8_t)g3};
-            const uint32_t idx = stage_base(threadIdx.x, gs8);
+            const uint32_t idx = stage_base4(threadIdx.x, g0, g1, g2, g3);
             const uint32_t o0 = 1u << g0, o1 = 1u << g1, o2 = 1u << g2, o3 = 1u << g3;
             T a[16], b[16];
 #pragma unroll
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam
                 a[j] = sphi[off];
                 b[j] = slam[off];
             }
-            const uint64_t tg = base | tl2g(ctab, g.L, idx);
+            const uint64_t tg = base | tl2g(ctab, L, idx);
 #pragma unroll 1
             for (int q = 1; q <= cnt; ++q) {
                 const desv_op &op = ops[k + q];
@@ -69,8 +69,8 @@ __global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam
             }
             k += 1 + cnt;
             if (k >= nops) {
-                const uint64_t q0 = tl_bit(ctab, g.L, g0), q1 = tl_bit(ctab, g.L, g1), q2 = tl_bit(ctab, g.L, g2),
-                               q3 = tl_bit(ctab, g.L, g3);
+                const uint64_t q0 = tl_bit(ctab, L, g0), q1 = tl_bit(ctab, L, g1), q2 = tl_bit(ctab, L, g2),
+                               q3 = tl_bit(ctab, L, g3);
                 T *outa = phi + tg, *outb = lam + tg;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {

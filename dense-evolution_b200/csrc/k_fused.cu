@@ -21,8 +21,7 @@ __device__ __forceinline__ void fused_tile_body(T *s, T *sv, uint64_t base, cons
         const int cnt = (int)sh.mat;
         const uint32_t g0 = (sh.w.z >> 8) & 0xFFu, g1 = (sh.w.z >> 16) & 0xFFu, g2 = sh.w.z >> 24,
                        g3 = sh.w.w & 0xFFu;
-        const uint8_t gs8[4] = {(uint8_t)g0, (uint8_t)g1, (uint8_t)g2, (uint8_t)g3};
-        const uint32_t idx = stage_base(threadIdx.x, gs8);
+        const uint32_t idx = stage_base4(threadIdx.x, g0, g1, g2, g3);
         const uint32_t o0 = 1u << g0, o1 = 1u << g1, o2 = 1u << g2, o3 = 1u << g3;
         T a[16];
 #pragma unroll
@@ -64,8 +63,9 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_fused_pass(T *sv, TileGeom g, 
     A.ptr[0] = sv;
     A.load[0] = true;
     A.store[0] = false;
-    auto body = [&](T *const *sp, uint64_t base, uint64_t) {
-        fused_tile_body<T, K>(sp[0], sv, base, pipe_ctab(smem), g.L, ops, nops, mats);
+    const int L = g.L;
+    auto body = [=](T *const *sp, uint64_t base, uint64_t) {
+        fused_tile_body<T, K>(sp[0], sv, base, pipe_ctab(smem), L, ops, nops, mats);
     };
     run_tiles<T, K, NBUF, 1>(g, A, body, smem);
 }

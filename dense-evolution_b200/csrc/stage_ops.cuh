@@ -649,6 +649,15 @@ __device__ __forceinline__ void run_stage_ops(T (&a)[16], const desv_op *ops, in
 #undef DESV_DGROW
 
 // Thread's tile-local index with zeros at the 4 register bits g[0..3] (ascending).
+// thread t's register-amplitude-0 index: zero bits inserted at the four register
+// positions g0 < g1 < g2 < g3 (scalar arguments keep everything in registers)
+__device__ __forceinline__ uint32_t stage_base4(uint32_t t, uint32_t g0, uint32_t g1, uint32_t g2, uint32_t g3) {
+    uint32_t x = (uint32_t)insert0(t, (int)g0);
+    x = (uint32_t)insert0(x, (int)g1);
+    x = (uint32_t)insert0(x, (int)g2);
+    return (uint32_t)insert0(x, (int)g3);
+}
+
 __device__ __forceinline__ uint32_t stage_base(uint32_t t, const uint8_t *g) {
     uint32_t x = t;
 #pragma unroll

@@ -125,5 +125,7 @@ def test_torch_autograd_and_unsupported_gates():
     circ = de.QASMParser().parse('OPENQASM 2.0; qreg q[1]; u3(0.1,0.2,0.3) q[0];')
     with pytest.raises(ValueError):
         de.circuit_to_energy_fn(circ, 1)
-    with pytest.raises(NotImplementedError):
+    # noise= reads .model / .p / .jax_key / .qubits like the reference's energy_fn
+    # (solvers/autodiff.py:159-164), so an object without them fails the same way
+    with pytest.raises(AttributeError):
         fn(np.zeros(npar), [(1.0, 'Z' * n)], noise=object())
