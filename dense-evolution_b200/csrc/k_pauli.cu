@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
     A.store[0] = false;
     const bool have_ctab = (1u << (K - g.L)) <= PIPE_CTAB_MAX;
     double ere = 0, eim = 0;
-    auto body = [&](T *const *sp, uint64_t base, uint64_t) {
+    auto body = [=, &ere, &eim](T *const *sp, uint64_t base, uint64_t) {
         const uint64_t *ctab = pipe_ctab(smem);
         // parity of the tile's fixed bits under each term's sign mask
         for (int k = threadIdx.x; k < nterms; k += blockDim.x)
