@@ -3,6 +3,27 @@
 // bounded waits, and the host-side error plumbing.
 #pragma once
 
+#ifdef __CUDACC_RTC__
+// Compiled at run time by NVRTC (plan-specialised pass kernels): no host
+// headers; the fixed-width types come from here and the status word is the
+// module's own, found by name through the driver.
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef unsigned short uint16_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+extern "C" {
+__device__ int desv_rtc_status = 0;
+}
+#define g_dev_status desv_rtc_status
+#define DESV_DEV_TIMEOUT 1
+#define DESV_DEV_BADPLAN 2
+#include "desv.h"
+
+namespace desv {
+#else
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -35,6 +56,7 @@ static int tu_status_read_clear() {
     return h;
 }
 static const int tu_status_registered = (register_status_reader(&tu_status_read_clear), 0);
+#endif  // __CUDACC_RTC__
 
 // ---------------------------------------------------------------- complex
 template <typename R> struct CT;

@@ -1,0 +1,242 @@
+// Plan-specialised pass kernels: compile a pass's CUDA source with NVRTC for
+// sm_100a, load it with the driver API and launch it on the caller's stream.
+// NVRTC and the driver are opened with dlopen on first use, so the library
+// still loads (and every other entry point works) where they are absent.
+// The kernels themselves are written against csrc/jit_pass.cuh, which reuses
+// the tile pipeline and the op bodies of the fused interpreter.
+#include <dlfcn.h>
+
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "desv_common.cuh"
+#include "tile_pipeline.cuh"
+
+namespace desv {
+
+// ---- the few NVRTC / driver entry points used (public API signatures)
+typedef int nvrtcResult_t;
+typedef void *nvrtcProgram_t;
+typedef int CUresult_t;
+typedef void *CUmodule_t;
+typedef void *CUfunction_t;
+typedef unsigned long long CUdeviceptr_t;
+
+struct JitApi {
+    bool tried = false, ok = false;
+    std::string why;
+    nvrtcResult_t (*CreateProgram)(nvrtcProgram_t *, const char *, const char *, int, const char *const *,
+                                   const char *const *);
+    nvrtcResult_t (*CompileProgram)(nvrtcProgram_t, int, const char *const *);
+    nvrtcResult_t (*GetProgramLogSize)(nvrtcProgram_t, size_t *);
+    nvrtcResult_t (*GetProgramLog)(nvrtcProgram_t, char *);
+    nvrtcResult_t (*GetCUBINSize)(nvrtcProgram_t, size_t *);
+    nvrtcResult_t (*GetCUBIN)(nvrtcProgram_t, char *);
+    nvrtcResult_t (*DestroyProgram)(nvrtcProgram_t *);
+    CUresult_t (*ModuleLoadData)(CUmodule_t *, const void *);
+    CUresult_t (*ModuleUnload)(CUmodule_t);
+    CUresult_t (*ModuleGetFunction)(CUfunction_t *, CUmodule_t, const char *);
+    CUresult_t (*ModuleGetGlobal)(CUdeviceptr_t *, size_t *, CUmodule_t, const char *);
+    CUresult_t (*FuncSetAttribute)(CUfunction_t, int, int);
+    CUresult_t (*OccupancyMaxActiveBlocksPerMultiprocessor)(int *, CUfunction_t, int, size_t);
+    CUresult_t (*LaunchKernel)(CUfunction_t, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
+                               void *, void **, void **);
+};
+
+static std::mutex g_jit_mu;
+static JitApi g_api;
+
+template <class F> static bool sym(void *lib, const char *name, F &f, std::string &why) {
+    f = reinterpret_cast<F>(dlsym(lib, name));
+    if (!f) why = std::string("missing symbol ") + name;
+    return f != nullptr;
+}
+
+static const JitApi &api() {
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    if (g_api.tried) return g_api;
+    g_api.tried = true;
+    void *rtc = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
+    if (!rtc) rtc = dlopen("libnvrtc.so", RTLD_NOW | RTLD_LOCAL);
+    void *drv = dlopen("libcuda.so.1", RTLD_NOW | RTLD_LOCAL);
+    if (!rtc || !drv) {
+        g_api.why = !rtc ? "libnvrtc not found" : "libcuda.so.1 not found";
+        return g_api;
+    }
+    std::string &w = g_api.why;
+    g_api.ok = sym(rtc, "nvrtcCreateProgram", g_api.CreateProgram, w) &&
+               sym(rtc, "nvrtcCompileProgram", g_api.CompileProgram, w) &&
+               sym(rtc, "nvrtcGetProgramLogSize", g_api.GetProgramLogSize, w) &&
+               sym(rtc, "nvrtcGetProgramLog", g_api.GetProgramLog, w) &&
+               sym(rtc, "nvrtcGetCUBINSize", g_api.GetCUBINSize, w) && sym(rtc, "nvrtcGetCUBIN", g_api.GetCUBIN, w) &&
+               sym(rtc, "nvrtcDestroyProgram", g_api.DestroyProgram, w) &&
+               sym(drv, "cuModuleLoadData", g_api.ModuleLoadData, w) &&
+               sym(drv, "cuModuleUnload", g_api.ModuleUnload, w) &&
+               sym(drv, "cuModuleGetFunction", g_api.ModuleGetFunction, w) &&
+               sym(drv, "cuModuleGetGlobal_v2", g_api.ModuleGetGlobal, w) &&
+               sym(drv, "cuFuncSetAttribute", g_api.FuncSetAttribute, w) &&
+               sym(drv, "cuOccupancyMaxActiveBlocksPerMultiprocessor",
+                   g_api.OccupancyMaxActiveBlocksPerMultiprocessor, w) &&
+               sym(drv, "cuLaunchKernel", g_api.LaunchKernel, w);
+    return g_api;
+}
+
+// One loaded pass kernel.
+struct JitKernel {
+    CUmodule_t mod = nullptr;
+    CUfunction_t fn = nullptr;
+    CUdeviceptr_t status = 0;  // the module's desv_rtc_status word
+    int K = 0, dtype = 0, blocks_per_sm = 1;
+    size_t smem = 0;
+};
+
+static std::vector<JitKernel *> g_kernels;  // status words of live modules (under g_jit_mu)
+
+static int jit_status_read_clear() {
+    std::vector<CUdeviceptr_t> words;
+    {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        for (auto *k : g_kernels) words.push_back(k->status);
+    }
+    int h = 0;
+    for (CUdeviceptr_t w : words) {
+        int v = 0;
+        if (!w || cudaMemcpy(&v, reinterpret_cast<void *>(w), sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+            continue;
+        if (v) {
+            const int zero = 0;
+            cudaMemcpy(reinterpret_cast<void *>(w), &zero, sizeof(int), cudaMemcpyHostToDevice);
+        }
+        h |= v;
+    }
+    return h;
+}
+static const int jit_status_registered = (register_status_reader(&jit_status_read_clear), 0);
+
+}  // namespace desv
+
+using namespace desv;
+
+extern "C" int desv_jit_available(char *why, size_t len) {
+    const JitApi &a = api();
+    if (why && len) {
+        std::strncpy(why, a.ok ? "" : a.why.c_str(), len - 1);
+        why[len - 1] = 0;
+    }
+    return a.ok ? 1 : 0;
+}
+
+extern "C" int desv_jit_load(const char *src, const char *include_dir, int tile_bits, int nbuf, int dtype,
+                             int device, void **handle, char *log, size_t loglen) {
+    if (!src || !include_dir || !handle) return fail(DESV_EINVAL, "jit load: null argument");
+    *handle = nullptr;
+    if (dtype != DESV_C64 && dtype != DESV_C128) return fail(DESV_EINVAL, "jit load: bad dtype");
+    if (tile_bits < 9 || tile_bits > (dtype == DESV_C64 ? 13 : 12) || nbuf < 2 || nbuf > 4)
+        return fail(DESV_EINVAL, "jit load: bad tile shape");
+    const JitApi &a = api();
+    if (!a.ok) return fail(DESV_EUNSUPPORTED, "jit: " + a.why);
+    nvrtcProgram_t prog = nullptr;
+    if (a.CreateProgram(&prog, src, "desv_pass.cu", 0, nullptr, nullptr) != 0)
+        return fail(DESV_ECUDA, "nvrtcCreateProgram failed");
+    // include_dir: one or more directories separated by ':'
+    std::vector<std::string> incs;
+    for (const char *p = include_dir; *p;) {
+        const char *e = std::strchr(p, ':');
+        const size_t len = e ? (size_t)(e - p) : std::strlen(p);
+        if (len) incs.push_back(std::string("-I") + std::string(p, len));
+        p += len + (e ? 1 : 0);
+    }
+    // -default-device: the C-ABI prototypes of desv.h parse as (unused) device declarations
+    std::vector<const char *> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-default-device"};
+    for (auto &i : incs) opts.push_back(i.c_str());
+    const int cr = a.CompileProgram(prog, (int)opts.size(), opts.data());
+    size_t ls = 0;
+    a.GetProgramLogSize(prog, &ls);
+    std::string plog(ls, '\0');
+    if (ls) a.GetProgramLog(prog, &plog[0]);
+    if (log && loglen) {
+        std::strncpy(log, plog.c_str(), loglen - 1);
+        log[loglen - 1] = 0;
+    }
+    if (cr != 0) {
+        a.DestroyProgram(&prog);
+        return fail(DESV_EINVAL, "jit: NVRTC compile failed: " + plog.substr(0, 2000));
+    }
+    size_t cs = 0;
+    a.GetCUBINSize(prog, &cs);
+    std::vector<char> cubin(cs);
+    a.GetCUBIN(prog, cubin.data());
+    a.DestroyProgram(&prog);
+
+    auto *k = new JitKernel();
+    k->K = tile_bits;
+    k->dtype = dtype;
+    const size_t esz = dtype == DESV_C64 ? 8 : 16;
+    k->smem = PIPE_HDR_BYTES + (size_t)nbuf * ((size_t)1 << tile_bits) * esz;
+    size_t ssz = 0;
+    // bind the device's primary context to this thread (compiles may run on worker threads)
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete k;
+        return check_launch("jit load: cudaSetDevice");
+    }
+    if (a.ModuleLoadData(&k->mod, cubin.data()) != 0 || a.ModuleGetFunction(&k->fn, k->mod, "desv_jit_kernel") != 0 ||
+        a.ModuleGetGlobal(&k->status, &ssz, k->mod, "desv_rtc_status") != 0) {
+        if (k->mod) a.ModuleUnload(k->mod);
+        delete k;
+        return fail(DESV_ECUDA, "jit: loading the compiled pass failed (no current CUDA context?)");
+    }
+    // CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES = 8
+    if (a.FuncSetAttribute(k->fn, 8, (int)k->smem) != 0) {
+        a.ModuleUnload(k->mod);
+        delete k;
+        return fail(DESV_ECUDA, "jit: shared-memory attribute refused");
+    }
+    int b = 0;
+    a.OccupancyMaxActiveBlocksPerMultiprocessor(&b, k->fn, 1 << (tile_bits - 4), k->smem);
+    k->blocks_per_sm = b > 0 ? b : 1;
+    {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        g_kernels.push_back(k);
+    }
+    *handle = k;
+    return DESV_OK;
+}
+
+extern "C" int desv_jit_free(void *handle) {
+    if (!handle) return DESV_OK;
+    auto *k = static_cast<JitKernel *>(handle);
+    {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        for (size_t i = 0; i < g_kernels.size(); ++i)
+            if (g_kernels[i] == k) {
+                g_kernels.erase(g_kernels.begin() + i);
+                break;
+            }
+    }
+    if (api().ok && k->mod) api().ModuleUnload(k->mod);
+    delete k;
+    return DESV_OK;
+}
+
+extern "C" int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *ps, const void *mats_dev,
+                             void *stream) {
+    if (!handle || !sv || !ps || !mats_dev) return fail(DESV_EINVAL, "jit pass: null argument");
+    auto *k = static_cast<JitKernel *>(handle);
+    if (dtype != k->dtype) return fail(DESV_EINVAL, "jit pass: dtype differs from the compiled kernel");
+    if (n < 1 || n > 34) return fail(DESV_EINVAL, "jit pass: n out of range");
+    if (reinterpret_cast<uintptr_t>(sv) % 16) return fail(DESV_EINVAL, "jit pass: state not 16-byte aligned");
+    TileGeom g;
+    if (ps->tile_bits != k->K || ps->tile_bits > n || ps->low_bits < 5 || ps->tile_bits - ps->low_bits > 8 ||
+        !make_geom(g, n, ps->tile_bits, ps->low_bits, ps->high))
+        return fail(DESV_EINVAL, "jit pass: tile geometry does not match the compiled kernel");
+    if (ps->op_end == ps->op_begin) return DESV_OK;
+    const uint64_t ntiles = 1ull << (n - k->K);
+    const uint64_t cap = (uint64_t)sm_count() * k->blocks_per_sm;
+    const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
+    void *args[] = {&sv, &g, const_cast<void **>(&mats_dev)};
+    if (api().LaunchKernel(k->fn, grid, 1, 1, 1u << (k->K - 4), 1, 1, (unsigned)k->smem, stream, args, nullptr) != 0)
+        return fail(DESV_ECUDA, "jit pass: launch failed");
+    return DESV_OK;
+}

@@ -305,7 +305,7 @@ __device__ __forceinline__ void apply_one_op(T (&a)[16], const desv_op &op, cons
 #define DESV_CODE_PRED 0x8000u
 #define DESV_CODE_MULTI 120u      // + slot mask 1..15: general 2x2 on each slot in the mask
 #define DESV_CODE_MULTI_REAL 136u // + slot mask: real 2x2 on each slot in the mask
-#define DESV_CODE_SIGNS 152u      // group of +-1 diagonals, s0 entries at the op's matrix offset
+#define DESV_CODE_SIGNS 152u      // group of +-1 diagonals: normal-form record, s0 product pairs
 #define DESV_CODE_DIAG_GROUP 154u // group of diagonals, s0 entries of 5 elements at the op's matrix offset
 #define DESV_CODE_LAYER 160u      // + slot mask 0..15: general 2x2 on those slots (packed form, 8 elements
                                   // per matrix) and on the lane bits in s1 (plain form)
@@ -373,24 +373,40 @@ __device__ __forceinline__ void flip_sign(double2 &v, uint32_t s) {
     v.y = __longlong_as_double(__double_as_longlong(v.y) ^ (long long)t);
 }
 
-// A group of +-1 diagonals (cz, and cp / crz at angles that give signs): entry
-// i is three words -- the thread-fixed bits it reads (ta | tb << 8, 0x40 | global
-// bit or 0xFF) and four 16-bit negation masks over the register amplitudes,
-// one per value (bit ta) + 2 (bit tb), precomputed on the host.  The group's
-// signs fold into one mask per thread, applied once as sign-bit flips.
-template <typename T>
-__device__ __forceinline__ void signs_group(T (&a)[16], const uint32_t *e, int cnt, uint64_t tg) {
-    uint32_t neg = 0;
-#pragma unroll 1
-    for (int i = 0; i < cnt; ++i) {
-        const uint32_t sel = e[3 * i], ta = sel & 0xFFu, tb = (sel >> 8) & 0xFFu;
-        const uint32_t va = ta == 0xFFu ? 0u : (uint32_t)(tg >> (ta & 63u)) & 1u;
-        const uint32_t vb = tb == 0xFFu ? 0u : (uint32_t)(tg >> (tb & 63u)) & 1u;
-        const uint32_t w = e[3 * i + 1 + vb];
-        neg ^= va ? (w >> 16) : (w & 0xFFFFu);
-    }
+// A group of +-1 diagonals (cz, and cp / crz at angles that give signs) in
+// algebraic normal form over the thread-fixed index bits, precomputed on the
+// host.  Record (64-bit words at the op's matrix offset): q[0] the 16-bit
+// negation mask shared by every thread; q[1] the global bits whose parity
+// negates all 16 register amplitudes; q[2 + S] the global bits whose parity
+// negates the amplitudes with register bit S set; then npairs pairs (d, M):
+// the parity of bit(i) & bit(i + d) over i in M negates all 16.  tg has zeros
+// at the register bits, so only thread-fixed bits enter.  The negations fold
+// into one 16-bit mask per thread, applied once as sign-bit flips; every load
+// of the record is independent of the others.
+__device__ __forceinline__ uint32_t parity_mask(uint64_t x, uint32_t m) {
+    return (0u - ((uint32_t)__popcll(x) & 1u)) & m;
+}
+
+// negate the register amplitudes j whose bit j of `neg` is set
+template <typename T> __device__ __forceinline__ void sign_flips(T (&a)[16], uint32_t neg) {
 #pragma unroll
     for (int j = 0; j < 16; ++j) flip_sign(a[j], (neg << (31 - j)) & 0x80000000u);
+}
+
+template <typename T>
+__device__ __forceinline__ void signs_group(T (&a)[16], const uint64_t *q, int npairs, uint64_t tg) {
+    const uint64_t c = q[0], lall = q[1], l0 = q[2], l1 = q[3], l2 = q[4], l3 = q[5];
+    uint64_t x = tg & lall;
+    if (npairs > 0) {
+        const uint64_t d0 = q[6], m0 = q[7];
+        x ^= tg & (tg >> (uint32_t)d0) & m0;
+#pragma unroll 1
+        for (int i = 1; i < npairs; ++i) x ^= tg & (tg >> (uint32_t)q[6 + 2 * i]) & q[7 + 2 * i];
+    }
+    const uint32_t neg = ((uint32_t)c & 0xFFFFu) ^ parity_mask(x, 0xFFFFu) ^ parity_mask(tg & l0, 0xAAAAu) ^
+                         parity_mask(tg & l1, 0xCCCCu) ^ parity_mask(tg & l2, 0xF0F0u) ^
+                         parity_mask(tg & l3, 0xFF00u);
+    sign_flips(a, neg);
 }
 
 // 2x2 on register slot S with the matrix in packed form: for every entry m the
@@ -611,7 +627,7 @@ __device__ __forceinline__ void apply_op_head(T (&a)[16], const OpHead &h, const
         DESV_LAYER(7) DESV_LAYER(8) DESV_LAYER(9) DESV_LAYER(10) DESV_LAYER(11) DESV_LAYER(12) DESV_LAYER(13)
         DESV_LAYER(14) DESV_LAYER(15)
         case DESV_CODE_SIGNS:
-            signs_group(a, reinterpret_cast<const uint32_t *>(mp), (int)((w0.x >> 16) & 0xFFu), tg);
+            signs_group(a, reinterpret_cast<const uint64_t *>(mp), (int)((w0.x >> 16) & 0xFFu), tg);
             break;
         case DESV_CODE_DIAG_GROUP: diag_group(a, mp, (int)((w0.x >> 16) & 0xFFu), tg); break;
         case DESV_CODE_LANE_CTL:

@@ -187,6 +187,7 @@ __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body 
     return ok;
 }
 
+#ifndef __CUDACC_RTC__
 // host-side geometry builder
 inline bool make_geom(TileGeom &g, int n, int K, int L, const uint8_t *high) {
     if (K > n || L < 1 || L > K || n > 34) return false;
@@ -204,5 +205,6 @@ inline bool make_geom(TileGeom &g, int n, int K, int L, const uint8_t *high) {
     g.nrest = r;
     return r == n - K;
 }
+#endif
 
 }  // namespace desv

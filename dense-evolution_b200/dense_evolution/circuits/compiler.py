@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from .. import _native as N
-from . import fusion
+from . import fusion, jit
 
 
 class QuantumTranspiler:
@@ -94,6 +94,8 @@ class CompiledCircuit:
         self.ir, self.fops, self.packed = fusion.build(target, self.n, self.tile_bits, slots, merge_1q)
         self._dev_cache = None
         self._dev_theta_key = None
+        self._host_arrays = None
+        self._jit_kernels = None
 
     # ------------------------------------------------------------ stats
     @property
@@ -120,6 +122,8 @@ class CompiledCircuit:
             return self._dev_cache[1], self._dev_cache[2]
         mats = self.packed.materialize(theta, self._np_dtype())
         ops, self._passes, mats = self.packed.compact(mats)
+        self._host_arrays = (ops, mats)
+        self._jit_kernels = None
         ops_t = torch.from_numpy(ops.view(np.uint8).copy()).to(device)
         rdt = np.float32 if self.dtype == torch.complex64 else np.float64
         mats_t = torch.from_numpy(mats.view(rdt).copy()).to(device)
@@ -142,11 +146,25 @@ class CompiledCircuit:
             return sv
         ops_t, mats_t = self.device_arrays(sv.device, theta)
         passes = self._passes
+        if jit.enabled(self.n):
+            jit.run_passes(self.specialised_kernels(sv.device), sv.data_ptr(), self.n, code, passes,
+                           mats_t.data_ptr(), st.value)
+            return sv
         N.check(lib.desv_apply_passes(ctypes.c_void_p(sv.data_ptr()), self.n, code,
                                       ctypes.c_void_p(passes.ctypes.data), len(passes),
                                       ctypes.c_void_p(ops_t.data_ptr()), ctypes.c_void_p(mats_t.data_ptr()), st),
                 'apply fused passes')
         return sv
+
+
+    def specialised_kernels(self, device):
+        """Plan-specialised kernels (one per pass) of the op stream that
+        device_arrays() uploaded last; compiled once per structure."""
+        if self._jit_kernels is None:
+            ops, mats = self._host_arrays
+            dev = device.index if device.index is not None else torch.cuda.current_device()
+            self._jit_kernels = jit.compile_passes(ops, self._passes, mats, self.dtype == torch.complex64, dev)
+        return self._jit_kernels
 
 
 def apply_fop(sv: torch.Tensor, n: int, op: 'fusion.FOp', theta, st):

@@ -903,10 +903,12 @@ class Packed:
                             j += 1
                         run = body[i:j]
                         g = r.copy()
-                        if all(58 <= int(x['code']) <= 82 for x in run):
-                            ents = _sign_entries(run, pool)
+                        sign = (_sign_entries(run, pool)
+                                if all(58 <= int(x['code']) <= 82 for x in run) else None)
+                        if sign is not None:
+                            ents, npairs = sign
                             g['code'] = 152
-                            g['s0'] = len(ents) // 3
+                            g['s0'] = npairs
                             sign_recs.append((g, nsign_words))
                             words.extend(ents)
                             nsign_words += len(ents)
@@ -1018,14 +1020,25 @@ class Packed:
 DG_SIGN, DG_THREAD, DG_SLOT_A, DG_SLOT_B, DG_TWO = 0, 1, 2, 3, 4
 
 
+_SLOT_MASKS = (0xAAAA, 0xCCCC, 0xF0F0, 0xFF00)
+
+
 def _sign_entries(run, pool) -> list:
-    """uint32 words of a sign group (dispatch code 152): 3 words per entry,
-    ``ta | tb << 8`` (the thread-fixed bits the entry reads: 0x40 | global bit,
-    0xFF if none) and the four 16-bit negation masks over the 16 register
-    amplitudes, one per value pair (bit ta) + 2 (bit tb), packed two per word.
-    Entries that read no thread bit fold into one constant mask."""
+    """uint32 words of a sign group (dispatch code 152), or None when a mask is
+    not affine in the register bits (the caller then emits a diagonal group).
+
+    The group's negation of register amplitude j of a thread is a parity
+    (XOR) of terms, each sign diagonal contributing its algebraic normal form
+    over the thread-fixed bits it reads.  The record is 64-bit words:
+    q[0] the 16-bit mask common to every thread; q[1] the global bits whose
+    parity negates all 16 amplitudes; q[2 + S] the global bits whose parity
+    negates the amplitudes with register bit S set; then, per distance d of a
+    product term, q = d and the mask M of the lower bits i: the parity of
+    bit(i) * bit(i + d) over i in M negates all 16.  Returns the words and the
+    number of (d, M) pairs."""
     const_mask = 0
-    out = []
+    lin = [0] * 5                 # all, slot 0..3
+    prod = {}
     j = np.arange(16)
     for r in run:
         m0 = int(r['mat'])
@@ -1035,15 +1048,9 @@ def _sign_entries(run, pool) -> list:
         for gkey, skey in (('ga', 'sa'), ('gb', 'sb')):
             sl, gb = int(r[skey]), int(r[gkey])
             sels.append(('slot', sl) if sl >= 0 else ('none', 0) if gb == 0xFF else ('thread', gb))
-        tsel = [0x40 | v for k, v in sels if k == 'thread']
+        tbits = [v for k, v in sels if k == 'thread']
         masks = []
-        for idx in range(4):
-            vals = {}
-            t = 0
-            for k, v in sels:
-                if k == 'thread':
-                    vals[len(vals)] = (idx >> t) & 1
-                    t += 1
+        for idx in range(1 << len(tbits)):
             bits = []
             t = 0
             for k, v in sels:
@@ -1056,15 +1063,49 @@ def _sign_entries(run, pool) -> list:
                     bits.append(np.zeros(16, np.int64))
             neg = np.array([pattern[x] for x in (bits[0] + 2 * bits[1])])
             masks.append(int(np.sum(neg.astype(np.int64) << j)))
-        if not tsel:
-            const_mask ^= masks[0]
-            continue
-        ta = tsel[0]
-        tb = tsel[1] if len(tsel) > 1 else 0xFF
-        out += [ta | tb << 8, masks[0] | masks[1] << 16, masks[2] | masks[3] << 16]
-    if const_mask:
-        out += [0xFF | 0xFF << 8, const_mask | const_mask << 16, const_mask | const_mask << 16]
-    return out
+        const_mask ^= masks[0]
+        if len(tbits) >= 1:
+            # linear term of the first thread bit (at the second one == 0)
+            w = masks[1] ^ masks[0]
+            if not _add_linear(lin, tbits[0], w):
+                return None
+        if len(tbits) == 2:
+            w = masks[2] ^ masks[0]
+            if not _add_linear(lin, tbits[1], w):
+                return None
+            w = masks[0] ^ masks[1] ^ masks[2] ^ masks[3]
+            if w not in (0, 0xFFFF):
+                return None
+            if w:
+                lo, hi = sorted(tbits)
+                if lo == hi:      # bit(i)^2 == bit(i): a linear term
+                    lin[0] ^= 1 << lo
+                else:
+                    prod[hi - lo] = prod.get(hi - lo, 0) ^ (1 << lo)
+    q = [const_mask, *lin]
+    pairs = [(dd, m) for dd, m in sorted(prod.items()) if m]
+    for dd, m in pairs:
+        q += [dd, m]
+    out = []
+    for v in q:
+        out += [v & 0xFFFFFFFF, v >> 32]
+    return out, len(pairs)
+
+
+def _add_linear(lin, bit, w) -> bool:
+    """Add the linear term bit * w (w a 16-bit mask over the register
+    amplitudes) to `lin`; False if w is not affine in the register bits."""
+    if w == 0:
+        return True
+    c = w & 1                     # value at j == 0: the all-amplitudes part
+    rest = w ^ (0xFFFF if c else 0)
+    if c:
+        lin[0] ^= 1 << bit
+    for s, sm in enumerate(_SLOT_MASKS):
+        if (rest >> (1 << s)) & 1:
+            rest ^= sm
+            lin[1 + s] ^= 1 << bit
+    return rest == 0
 
 
 def _diag_group_values(dv, pool) -> np.ndarray:

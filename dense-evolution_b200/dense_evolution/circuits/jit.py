@@ -1,0 +1,235 @@
+"""Plan-specialised fused-pass kernels.
+
+A compacted pass (the op records that ``PackedPlan.compact`` uploads for the
+fused interpreter ``k_fused_pass``) is written out as CUDA source in which
+every structural field is a constant: the register bit positions of each
+stage, the op bodies picked by their dispatch codes, the matrix offsets, the
+thread predicates and the +-1 sign masks.  libdesv compiles the source with
+NVRTC for sm_100a (``desv_jit_load``) against ``csrc/jit_pass.cuh``, which
+reuses the interpreter's tile pipeline and op bodies, and launches it with
+``desv_jit_pass``.  The matrix values stay in the same device pool, so new
+angles need no recompile; a kernel is cached per source text.
+
+The op bodies and their order are the interpreter's, so a specialised pass
+computes what the interpreter computes (tests compare the two).
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import os
+import threading
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+from .. import _native as N
+
+_PKG = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+CSRC = os.path.join(_PKG, 'csrc')
+INCLUDE = os.path.join(os.path.dirname(_PKG), 'include')
+INCLUDE_PATH = CSRC + ':' + INCLUDE
+V_BREAL = 5
+PRED = 0x8000
+
+
+def _hex(v: int) -> str:
+    return f'0x{int(v):x}ull'
+
+
+def _signs_code(words: np.ndarray, w0: int, npairs: int) -> str:
+    """Code of a +-1 group (dispatch code 152) with its normal-form record as
+    immediates: neg = c ^ par(x) * 0xFFFF ^ sum_S par(tg & L_S) * slot mask S."""
+    q = [int(words[w0 + 2 * i]) | int(words[w0 + 2 * i + 1]) << 32 for i in range(6 + 2 * npairs)]
+    c, lall, ls = q[0] & 0xFFFF, q[1], q[2:6]
+    xs = [f'(tg & {_hex(lall)})'] if lall else []
+    for i in range(npairs):
+        d, m = q[6 + 2 * i], q[7 + 2 * i]
+        if m:
+            xs.append(f'(tg & (tg >> {d}) & {_hex(m)})')
+    terms = [f'0x{c:x}u'] if c else []
+    if xs:
+        terms.append(f'parity_mask({" ^ ".join(xs)}, 0xFFFFu)')
+    for s, (l, sm) in enumerate(zip(ls, (0xAAAA, 0xCCCC, 0xF0F0, 0xFF00))):
+        if l:
+            terms.append(f'parity_mask(tg & {_hex(l)}, 0x{sm:X}u)')
+    if not terms:
+        return ''
+    return f'sign_flips(a, {" ^ ".join(terms)});'
+
+
+def _op_code(o, words: np.ndarray, wpe: int) -> str:
+    c = int(o['code'])
+    pred, c = c & PRED, c & 0x7FFF
+    off = int(o['mat'])
+    mp = f'mats + {off}'
+    s0 = int(o['s0'])
+    s1 = int(o['s1']) & 0xFF
+    if 1 <= c <= 20:
+        S, V = divmod(c - 1, 5)
+        call = f'm1_reg<{S}, {V}, -1>(a, load_m22({mp}));'
+    elif 21 <= c <= 52:
+        x = c - 21
+        S, CS = divmod(x // 2, 4)
+        call = f'm1_ctl_case<{S}, {CS}>(a, load_m22({mp}), {"false" if x & 1 else "true"});'
+    elif 53 <= c <= 57:
+        call = f'm1_lane_free<{c - 53}>(a, load_m22({mp}), {s0 - 16}, lane);'
+    elif 58 <= c <= 107:
+        sg = c < 83
+        x = c - (58 if sg else 83)
+        SA, SB = x // 5 - 1, x % 5 - 1
+        w0y = (int(o['ga']) << 8) | (int(o['gb']) << 16)
+        call = f'diag_case<{SA}, {SB}>(a, {mp}, 0x{w0y:x}u, tg, {"true" if sg else "false"});'
+    elif 120 <= c <= 151:
+        M, V = (c - 120, 0) if c < 136 else (c - 136, 1)
+        call = f'multi_reg<{M}, {V}>(a, {mp});'
+    elif c == 152:
+        call = _signs_code(words, off * wpe, s0)
+    elif c == 154:
+        call = f'diag_group(a, {mp}, {s0}, tg);'
+    elif 160 <= c <= 191:
+        real = c >= 176
+        M = c - (176 if real else 160)
+        nreg = bin(M).count('1')
+        parts = []
+        if M:
+            parts.append(f'multi_reg<{M}, {V_BREAL}>(a, {mp});' if real else f'multi_reg_packed<{M}>(a, {mp});')
+        k = off + (4 if real else 8) * nreg
+        for b in range(5):
+            if (s1 >> b) & 1:
+                parts.append(f'm1_lane_free<{V_BREAL if real else 0}>(a, load_m22(mats + {k}), {b}, lane);')
+                k += 4
+        call = ' '.join(parts)
+    elif c == 192:
+        cs = int(o['cslot'])
+        call = (f'm1_lane(a, load_m22({mp}), m1_variant({int(o["flags"])}), {cs}, {s0 - 16}, '
+                f'(tg & {_hex(o["cmask"])}) == {_hex(o["cval"])}, lane);')
+    else:
+        raise ValueError(f'dispatch code {c} has no specialised form')
+    if pred and call:
+        call = f'if ((tg & {_hex(o["cmask"])}) == {_hex(o["cval"])}) {{ {call} }}'
+    return call
+
+
+def pass_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: int, complex64: bool,
+                words: np.ndarray, wpe: int) -> str:
+    """CUDA source of one specialised pass over ops[begin:end]."""
+    T = 'float2' if complex64 else 'double2'
+    lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
+             f'extern "C" __global__ void __launch_bounds__({1 << (tile_bits - 4)}, {2 if complex64 else 1})',
+             f'desv_jit_kernel({T} *sv, TileGeom g, const {T} *__restrict__ mats) {{',
+             '    extern __shared__ __align__(128) unsigned char smem[];',
+             '    const int lane = threadIdx.x & 31;',
+             f'    auto stages = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L) {{',
+             f'        {T} a[16];']
+    k = begin
+    while k < end:
+        st = ops[k]
+        if int(st['kind']) != N.OP_STAGE:
+            raise ValueError('pass does not start with a stage record')
+        cnt = int(st['mat'])
+        g = [int(x) for x in st['g']]
+        last = k + 1 + cnt >= end
+        lines.append('        {')
+        lines.append(f'            using S = JitStage<{T}, {g[0]}u, {g[1]}u, {g[2]}u, {g[3]}u>;')
+        lines.append('            const uint32_t idx = S::index();')
+        lines.append('            S::load(a, s, idx);')
+        lines.append('            const uint64_t tg = base | tl2g(ctab, L, idx);')
+        for o in ops[k + 1:k + 1 + cnt]:
+            code = _op_code(o, words, wpe)
+            if code:
+                lines.append('            ' + code)
+        lines.append('            S::store_global(a, sv, tg, ctab, L);' if last else '            S::store_smem(a, s, idx);')
+        lines.append('        }')
+        k += 1 + cnt
+    lines += ['    };', f'    jit_pass_kernel<{T}, {tile_bits}, {nbuf}>(sv, g, smem, stages);', '}', '']
+    return '\n'.join(lines)
+
+
+def nbuf_for(tile_bits: int) -> int:
+    """Ring depth of the interpreter for this tile width (k_fused.cu)."""
+    return 3 if tile_bits >= 12 else 4
+
+
+# below this size a pass is too short for its compile to pay off
+MIN_QUBITS = 20
+_available = None
+
+
+def available() -> bool:
+    """NVRTC and the CUDA driver can be opened (libdesv loads them with dlopen)."""
+    global _available
+    if _available is None:
+        buf = ctypes.create_string_buffer(256)
+        _available = bool(N.lib().desv_jit_available(buf, 256))
+    return _available
+
+
+def enabled(n: int) -> bool:
+    """Use specialised kernels for an n-qubit plan: DESV_JIT=1 / 0 forces the
+    choice; by default from MIN_QUBITS qubits on."""
+    v = os.environ.get('DESV_JIT', '')
+    if v in ('0', '1'):
+        return v == '1'
+    return n >= MIN_QUBITS and available()
+
+
+class _Kernel:
+    __slots__ = ('handle',)
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __del__(self):
+        try:
+            N.lib().desv_jit_free(self.handle)
+        except Exception:
+            pass
+
+
+_cache: dict = {}
+_cache_lock = threading.Lock()
+
+
+def _load(src: str, tile_bits: int, nbuf: int, dtype_code: int, device: int) -> _Kernel:
+    key = (hashlib.sha1(src.encode()).hexdigest(), device)
+    with _cache_lock:
+        k = _cache.get(key)
+    if k is not None:
+        return k
+    h = ctypes.c_void_p()
+    log = ctypes.create_string_buffer(8192)
+    rc = N.lib().desv_jit_load(src.encode(), INCLUDE_PATH.encode(), tile_bits, nbuf, dtype_code, device,
+                               ctypes.byref(h), log, 8192)
+    N.check(rc, 'desv_jit_load')
+    k = _Kernel(h)
+    with _cache_lock:
+        _cache.setdefault(key, k)
+        return _cache[key]
+
+
+def compile_passes(ops: np.ndarray, passes: np.ndarray, mats_host: np.ndarray, complex64: bool, device: int,
+                   workers: int = 0) -> list:
+    """One specialised kernel per pass (NVRTC compiles run in parallel threads;
+    the ctypes call releases the GIL)."""
+    words = np.ascontiguousarray(mats_host).view(np.uint32)
+    wpe = mats_host.dtype.itemsize // 4
+    code = N.DESV_C64 if complex64 else N.DESV_C128
+    jobs = []
+    for p in passes:
+        K = int(p['tile_bits'])
+        nb = nbuf_for(K)
+        jobs.append((pass_source(ops, int(p['op_begin']), int(p['op_end']), K, nb, complex64, words, wpe), K, nb))
+    workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(lambda j: _load(j[0], j[1], j[2], code, device), jobs))
+
+
+def run_passes(kernels: list, sv_ptr: int, n: int, dtype_code: int, passes: np.ndarray, mats_ptr: int, stream):
+    lib = N.lib()
+    st = ctypes.c_void_p(stream)
+    base = passes.ctypes.data
+    for i, k in enumerate(kernels):
+        N.check(lib.desv_jit_pass(k.handle, ctypes.c_void_p(sv_ptr), n, dtype_code,
+                                  ctypes.c_void_p(base + i * passes.itemsize), ctypes.c_void_p(mats_ptr), st),
+                'desv_jit_pass')

@@ -19,8 +19,10 @@
 #ifndef DESV_H
 #define DESV_H
 
+#ifndef __CUDACC_RTC__
 #include <stddef.h>
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -268,6 +270,24 @@ int desv_sample_prepare(const void *sv, int n, int dtype, void *scratch, size_t 
  * searchsorted(cdf, u, 'right')); needs the scratch of desv_sample_prepare. */
 int desv_sample_pick(const void *sv, int n, int dtype, const void *scratch, size_t scratch_bytes,
                      const double *u_dev, int64_t nshots, int64_t *out_dev, void *stream);
+
+/* ---- plan-specialised fused passes (the same work as desv_apply_passes for
+ *      one pass, with the pass's op list compiled in).  The source is CUDA
+ *      written against csrc/jit_pass.cuh; it is compiled with NVRTC for
+ *      sm_100a and loaded into `device`'s primary context.  NVRTC and the
+ *      driver are opened with dlopen on first use. ---------------------------- */
+/* 1 if NVRTC and the CUDA driver could be opened; else 0 and the reason in why */
+int desv_jit_available(char *why, size_t len);
+/* Compile + load one pass kernel (entry point "desv_jit_kernel", tile shape
+ * tile_bits / nbuf ring slots).  include_dirs: directories separated by ':'.
+ * The NVRTC log goes to log (may be NULL). */
+int desv_jit_load(const char *src, const char *include_dirs, int tile_bits, int nbuf, int dtype, int device,
+                  void **handle, char *log, size_t loglen);
+int desv_jit_free(void *handle);
+/* Run the loaded kernel over one pass (its tile geometry must match the
+ * compiled tile_bits); mats_dev is the same matrix pool desv_apply_passes reads. */
+int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pass, const void *mats_dev,
+                  void *stream);
 
 /* ---- Pauli sums (replaces pauli_sum_expectation / pauli_sum_matvec,
  *      physics/observables.py:63-186,250-308) ------------------------------- */

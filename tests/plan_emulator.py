@@ -267,22 +267,26 @@ def _apply_coded(a, tg, op, g, mats, code):
     if c == 192:
         return _apply(a, tg, op, g, mats)
     if c == 152:
-        cnt = int(op['s0'])
+        npairs = int(op['s0'])
         wpe = mats.dtype.itemsize // 4
-        words = np.ascontiguousarray(mats).view(np.uint32)[m0 * wpe:m0 * wpe + 3 * cnt]
-        neg = np.zeros(a.shape, dtype=np.int64)
+        w = np.ascontiguousarray(mats).view(np.uint32)[m0 * wpe:m0 * wpe + 2 * (6 + 2 * npairs)].astype(np.uint64)
+        q = [int(w[2 * i]) | int(w[2 * i + 1]) << 32 for i in range(6 + 2 * npairs)]
+        t = tg.astype(np.uint64)
 
-        def tbit(x):
-            return np.zeros_like(tg) if x == 0xFF else _bit(tg, x & 63)
-        for e in range(cnt):
-            sel, w1, w2 = (int(x) for x in words[3 * e:3 * e + 3])
-            va, vb = tbit(sel & 0xFF), tbit((sel >> 8) & 0xFF)
-            idx = va + 2 * vb                     # per amplitude row: which mask
-            masks = np.array([w1 & 0xFFFF, w1 >> 16, w2 & 0xFFFF, w2 >> 16], np.int64)
-            m = masks[idx]                        # [T, 2^K]
-            reg = np.zeros(a.shape[1], np.int64)  # register index of every tile position
-            for s_, gp in enumerate(g):
-                reg |= ((j >> gp) & 1) << s_
-            neg ^= (m >> reg[None, :]) & 1
+        def par(x):
+            x = x.astype(np.uint64)
+            for sh in (32, 16, 8, 4, 2, 1):
+                x = x ^ (x >> np.uint64(sh))
+            return (x & np.uint64(1)).astype(np.int64)
+        x = t & np.uint64(q[1])
+        for i in range(npairs):
+            x = x ^ (t & (t >> np.uint64(q[6 + 2 * i])) & np.uint64(q[7 + 2 * i]))
+        reg = np.zeros(a.shape[1], np.int64)  # register index of every tile position
+        for s_, gp in enumerate(g):
+            reg |= ((j >> gp) & 1) << s_
+        neg = ((q[0] & 0xFFFF) >> reg[None, :]) & 1
+        neg = neg ^ par(x)
+        for s_ in range(4):
+            neg = neg ^ (par(t & np.uint64(q[2 + s_])) * ((reg[None, :] >> s_) & 1))
         return np.where(pred & (neg == 1), -a, a)
     raise AssertionError(f'unknown dispatch code {code}')

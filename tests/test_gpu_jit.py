@@ -1,0 +1,119 @@
+"""Plan-specialised pass kernels (NVRTC-compiled for sm_100a) against the fused
+interpreter and the oracle on the same seeded circuits.
+
+The specialised kernel runs the interpreter's op bodies in the same order, so
+the two agree to rounding (FMA contraction may differ); both are held to the
+oracle at the north-star tolerances (complex128 1e-12, complex64 1e-5)."""
+import numpy as np
+import pytest
+
+from oracle import sv_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+# every lowering family: controlled on slots / lanes / thread bits, diagonals,
+# sign groups, predicated and anti-diagonal ops
+MIXED = ['h', 'x', 'y', 'z', 's', 'sdg', 't', 'rx', 'ry', 'rz', 'p', 'u3', 'sx',
+         'cx', 'cz', 'cy', 'swap', 'iswap', 'ecr', 'cp', 'crz', 'ccx']
+
+
+def _run(plan, n, dt, theta=None):
+    import torch
+    sv = torch.zeros(1 << n, dtype=dt, device='cuda')
+    sv[0] = 1
+    plan.run(sv, theta)
+    torch.cuda.synchronize()
+    return sv.cpu().numpy()
+
+
+def _circuit(n, seed):
+    import dense_evolution as de
+    rng = np.random.default_rng(seed)
+    circ = de.random_circuit(n, 25 * n, seed=seed)
+    for _ in range(3 * n):
+        a, b, c = (int(x) for x in rng.choice(n, 3, replace=False))
+        g = MIXED[rng.integers(len(MIXED))]
+        if g == 'ccx':
+            circ.append(('ccx', a, b, c))
+        elif g in ('cp', 'crz'):
+            circ.append((g, a, b, float(rng.choice([np.pi, rng.uniform(-3, 3)]))))
+        elif g in ('cx', 'cz', 'cy', 'swap', 'iswap', 'ecr'):
+            circ.append((g, a, b))
+        elif g == 'u3':
+            circ.append(('u3', a, *rng.uniform(0, 2 * np.pi, 3)))
+        elif g in ('rx', 'ry', 'rz', 'p'):
+            circ.append((g, a, float(rng.uniform(-3, 3))))
+        else:
+            circ.append((g, a))
+    return circ
+
+
+@pytest.mark.parametrize('n,seed', [(10, 0), (13, 1), (16, 2)])
+def test_specialised_passes_match_interpreter_and_oracle(n, seed, monkeypatch):
+    import torch
+    import dense_evolution as de
+    from dense_evolution.circuits.compiler import CompiledCircuit
+    circ = _circuit(n, seed)
+    ref = O.run_circuit(O.zero_state(n), n, circ)
+    for dt, tol in ((torch.complex128, 1e-12), (torch.complex64, 1e-5)):
+        plan = CompiledCircuit(de.QuantumTranspiler.transpile(circ), n, dt)
+        monkeypatch.setenv('DESV_JIT', '0')
+        interp = _run(plan, n, dt)
+        monkeypatch.setenv('DESV_JIT', '1')
+        spec = _run(plan, n, dt)
+        assert np.max(np.abs(spec - interp)) <= (1e-14 if dt == torch.complex128 else 1e-6)
+        assert np.max(np.abs(spec - ref)) <= tol
+
+
+@pytest.mark.parametrize('tile_bits', [10, 11, 12])
+def test_specialised_brick_every_tile_and_new_angles(tile_bits, monkeypatch):
+    """Kernels compile once per structure; new angles reuse them."""
+    import torch
+    import dense_evolution as de
+    from dense_evolution.circuits.compiler import CompiledCircuit
+    from dense_evolution.circuits import jit
+    from dense_evolution.workloads import brick_u3_circuit
+    n = 17
+    monkeypatch.setenv('DESV_JIT', '1')
+    for seed in (5, 6):
+        circ = brick_u3_circuit(n, 6, seed=seed)
+        ref = O.run_circuit(O.zero_state(n), n, circ)
+        plan = CompiledCircuit(de.QuantumTranspiler.transpile(circ), n, torch.complex64, tile_bits=tile_bits)
+        before = len(jit._cache)
+        got = _run(plan, n, torch.complex64)
+        assert np.max(np.abs(got - ref)) <= 1e-5
+        if seed == 6:
+            assert len(jit._cache) == before   # same structure: no new compile
+
+
+def test_parametric_plan_follows_theta(monkeypatch):
+    import torch
+    import dense_evolution as de
+    from dense_evolution.workloads import hea_circuit, tfim_terms
+    n = 14
+    monkeypatch.setenv('DESV_JIT', '1')
+    fn, npar = de.circuit_to_energy_fn(hea_circuit(n, 3), n)
+    op = de.PauliSumOperator(tfim_terms(n), n)
+    rows, _ = O.energy_template([{'name': c[0], 'qubits': [q for q in c[1:] if isinstance(q, int)]}
+                                 for c in hea_circuit(n, 3)], n)
+    for s in (0, 1):
+        theta = np.random.default_rng(s).uniform(-np.pi, np.pi, npar)
+        e, _ = fn(theta, op)
+        assert float(e) == pytest.approx(O.energy(theta, rows, n, tfim_terms(n))[0], abs=1e-10)
+
+
+def test_default_path_at_22_qubits_matches_interpreter(monkeypatch):
+    import torch
+    import dense_evolution as de
+    from dense_evolution.circuits.compiler import CompiledCircuit
+    from dense_evolution.circuits import jit
+    from dense_evolution.workloads import brick_u3_circuit
+    n = 22
+    monkeypatch.delenv('DESV_JIT', raising=False)
+    assert jit.enabled(n)
+    plan = CompiledCircuit(de.QuantumTranspiler.transpile(brick_u3_circuit(n, 12, 3)), n, torch.complex64)
+    spec = _run(plan, n, torch.complex64)
+    monkeypatch.setenv('DESV_JIT', '0')
+    interp = _run(plan, n, torch.complex64)
+    assert np.max(np.abs(spec - interp)) <= 1e-6
+    de._native.device_status()
