@@ -253,6 +253,7 @@ def run_headline(args, ws, local):
     import dense_evolution as de
     from dense_evolution import _native as N
     from dense_evolution.circuits.compiler import CompiledCircuit
+    from dense_evolution.circuits import jit
     from dense_evolution.workloads import brick_u3_circuit
 
     dev = torch.device('cuda', torch.cuda.current_device())
@@ -270,8 +271,16 @@ def run_headline(args, ws, local):
     ops_t, mats_t = plan.device_arrays(dev)
     passes = plan.device_passes
     pass_bytes = 2 * (1 << n) * 8
+    specialised = jit.enabled(n)
+    t_c = time.perf_counter()
+    kernels = plan.specialised_kernels(dev) if specialised else None
+    jit_compile_s = time.perf_counter() - t_c
 
     def one_pass(i):
+        if specialised:
+            jit.run_passes(kernels[i:i + 1], sv.data_ptr(), n, N.DESV_C64, passes[i:i + 1], mats_t.data_ptr(),
+                           st.cuda_stream)
+            return
         N.check(lib.desv_apply_passes(ctypes.c_void_p(sv.data_ptr()), n, N.DESV_C64,
                                       ctypes.c_void_p(passes[i:i + 1].ctypes.data), 1,
                                       ctypes.c_void_p(ops_t.data_ptr()), ctypes.c_void_p(mats_t.data_ptr()),
@@ -337,10 +346,11 @@ def run_headline(args, ws, local):
                    'l2': f'state ({(1 << n) * 8 / 2**30:.2f} GiB) larger than L2 (126 MB); no flush needed',
                    'parallelism': f'replicas x{ws}'},
         'passes_per_step': npasses, 'layers_per_s': ws * layers / (ms_step / 1e3),
-        'ms_per_layer': ms_step / layers, 'compile_s': compile_s,
+        'ms_per_layer': ms_step / layers, 'compile_s': compile_s, 'jit_compile_s': jit_compile_s,
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_src,
-                     'kernel': f'k_fused_pass<float2,{plan.tile_bits},3>',
+                     'kernel': ('desv_jit_kernel (plan-specialised fused pass, NVRTC sm_100a)' if specialised
+                                else f'k_fused_pass<float2,{plan.tile_bits},3>'),
                      'algorithmic_bytes_per_launch': pass_bytes,
                      'avg_launch_ms': avg_pass_ms, 'min_launch_ms': float(per_pass.min()),
                      'max_launch_ms': float(per_pass.max())},

@@ -5,9 +5,9 @@
  * (passed as void*; NULL = legacy default stream), takes device pointers the
  * caller owns, returns an int status (DESV_OK == 0, negative on error) and
  * never aborts.  desv_last_error() returns the message of the last failure on
- * the calling thread.  No entry point allocates device memory: reductions
- * take a caller-provided scratch buffer whose size desv_scratch_bytes()
- * reports.
+ * the calling thread.  No entry point allocates device memory (except the
+ * code of a module that desv_jit_load loads): reductions take a
+ * caller-provided scratch buffer whose size desv_scratch_bytes() reports.
  *
  * Statevector layout: 2^n amplitudes, complex64 (float2) or complex128
  * (double2), interleaved re/im, MSB-first qubit order -- qubit q is bit
