@@ -27,6 +27,7 @@ The output is packed into the ``desv_pass`` / ``desv_op`` structs of
 """
 from __future__ import annotations
 
+import hashlib
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence, Tuple
 
@@ -50,6 +51,10 @@ def _unknown(name):
     return ValueError(
         f"unknown gate '{name}' -- not in GATES or PARAMETRIC_GATES. A typo in a gate name used to be "
         f"silently dropped from the circuit instead of raising (issue #4).")
+
+
+# grouped op streams by structure (see PackedPlan.compact), oldest dropped first
+_STRUCT_CACHE: dict = {}
 
 
 @dataclass
@@ -812,7 +817,18 @@ class Packed:
         key = codes.tobytes() + np.signbit(tabs.real).tobytes()
         cache = getattr(self, '_compact_cache', None)
         if cache is None or cache[0] != key or cache[6] != len(pool) or cache[7] != pool.dtype:
-            cache = (key,) + self._compact_structure(pool) + (len(pool), pool.dtype)
+            # plans of the same structure (a circuit re-run with new angles) share the
+            # grouping: the records (slots, masks, offsets, codes), the passes and the
+            # sign pattern determine it completely
+            skey = hashlib.sha1(self.ops.tobytes() + self.passes.tobytes() + key +
+                                str((len(pool), pool.dtype.str)).encode()).digest()
+            struct = _STRUCT_CACHE.get(skey)
+            if struct is None:
+                struct = self._compact_structure(pool)
+                if len(_STRUCT_CACHE) >= 32:
+                    _STRUCT_CACHE.pop(next(iter(_STRUCT_CACHE)))
+                _STRUCT_CACHE[skey] = struct
+            cache = (key,) + struct + (len(pool), pool.dtype)
             self._compact_cache = cache
         _, ops, passes, (gather, form), words, dv = cache[:6]
         if words is None and not len(gather) and dv is None:
