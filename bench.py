@@ -278,8 +278,8 @@ def run_headline(args, ws, local):
 
     def one_pass(i):
         if specialised:
-            jit.run_passes(kernels[i:i + 1], sv.data_ptr(), n, N.DESV_C64, passes[i:i + 1], mats_t.data_ptr(),
-                           st.cuda_stream)
+            jit.run_passes(kernels[i:i + 1], sv.data_ptr(), n, N.DESV_C64, passes[i:i + 1], ops_t.data_ptr(),
+                           mats_t.data_ptr(), st.cuda_stream)
             return
         N.check(lib.desv_apply_passes(ctypes.c_void_p(sv.data_ptr()), n, N.DESV_C64,
                                       ctypes.c_void_p(passes[i:i + 1].ctypes.data), 1,

@@ -88,9 +88,16 @@ struct JitKernel {
     CUmodule_t mod = nullptr;
     CUfunction_t fn = nullptr;
     CUdeviceptr_t status = 0;  // the module's desv_rtc_status word
-    int K = 0, dtype = 0, blocks_per_sm = 1;
-    size_t smem = 0;
+    int kind = 0, K = 0, nbuf = 0, dtype = 0, blocks_per_sm = 1;
+    size_t smem = 0;  // forward: the launch's dynamic shared memory; adjoint: without the accumulators
 };
+
+// Adjoint passes: at most this many gradient slots per pass and partial-sum
+// rows (the bounds of the interpreter k_adjoint_pass).
+constexpr int JIT_ADJ_MAX_PARAMS = 1024;
+constexpr int JIT_ADJ_MAX_ROWS = 1184;
+int grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad, cudaStream_t st);
+size_t adjoint_scratch_bytes(int max_params);
 
 static std::vector<JitKernel *> g_kernels;  // status words of live modules (under g_jit_mu)
 
@@ -128,11 +135,12 @@ extern "C" int desv_jit_available(char *why, size_t len) {
     return a.ok ? 1 : 0;
 }
 
-extern "C" int desv_jit_load(const char *src, const char *include_dir, int tile_bits, int nbuf, int dtype,
-                             int device, void **handle, char *log, size_t loglen) {
+extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind, int tile_bits, int nbuf,
+                             int dtype, int device, void **handle, char *log, size_t loglen) {
     if (!src || !include_dir || !handle) return fail(DESV_EINVAL, "jit load: null argument");
     *handle = nullptr;
     if (dtype != DESV_C64 && dtype != DESV_C128) return fail(DESV_EINVAL, "jit load: bad dtype");
+    if (kind != 0 && kind != 1) return fail(DESV_EINVAL, "jit load: kind must be 0 (pass) or 1 (adjoint)");
     if (tile_bits < 9 || tile_bits > (dtype == DESV_C64 ? 13 : 12) || nbuf < 2 || nbuf > 4)
         return fail(DESV_EINVAL, "jit load: bad tile shape");
     const JitApi &a = api();
@@ -171,10 +179,15 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int tile_
     a.DestroyProgram(&prog);
 
     auto *k = new JitKernel();
+    k->kind = kind;
     k->K = tile_bits;
+    k->nbuf = nbuf;
     k->dtype = dtype;
     const size_t esz = dtype == DESV_C64 ? 8 : 16;
-    k->smem = PIPE_HDR_BYTES + (size_t)nbuf * ((size_t)1 << tile_bits) * esz;
+    const int nw = (1 << (tile_bits - 4)) / 32 > 0 ? (1 << (tile_bits - 4)) / 32 : 1;
+    k->smem = PIPE_HDR_BYTES + (size_t)nbuf * (kind ? 2 : 1) * ((size_t)1 << tile_bits) * esz;
+    // adjoint kernels: room for the per-warp gradient accumulators of the largest pass
+    const size_t smem_max = k->smem + (kind ? (size_t)nw * JIT_ADJ_MAX_PARAMS * sizeof(double) : 0);
     size_t ssz = 0;
     // bind the device's primary context to this thread (compiles may run on worker threads)
     if (cudaSetDevice(device) != cudaSuccess) {
@@ -188,7 +201,7 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int tile_
         return fail(DESV_ECUDA, "jit: loading the compiled pass failed (no current CUDA context?)");
     }
     // CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES = 8
-    if (a.FuncSetAttribute(k->fn, 8, (int)k->smem) != 0) {
+    if (a.FuncSetAttribute(k->fn, 8, (int)smem_max) != 0) {
         a.ModuleUnload(k->mod);
         delete k;
         return fail(DESV_ECUDA, "jit: shared-memory attribute refused");
@@ -224,6 +237,7 @@ extern "C" int desv_jit_pass(void *handle, void *sv, int n, int dtype, const des
                              void *stream) {
     if (!handle || !sv || !ps || !mats_dev) return fail(DESV_EINVAL, "jit pass: null argument");
     auto *k = static_cast<JitKernel *>(handle);
+    if (k->kind != 0) return fail(DESV_EINVAL, "jit pass: the kernel is an adjoint pass");
     if (dtype != k->dtype) return fail(DESV_EINVAL, "jit pass: dtype differs from the compiled kernel");
     if (n < 1 || n > 34) return fail(DESV_EINVAL, "jit pass: n out of range");
     if (reinterpret_cast<uintptr_t>(sv) % 16) return fail(DESV_EINVAL, "jit pass: state not 16-byte aligned");
@@ -238,5 +252,43 @@ extern "C" int desv_jit_pass(void *handle, void *sv, int n, int dtype, const des
     void *args[] = {&sv, &g, const_cast<void **>(&mats_dev)};
     if (api().LaunchKernel(k->fn, grid, 1, 1, 1u << (k->K - 4), 1, 1, (unsigned)k->smem, stream, args, nullptr) != 0)
         return fail(DESV_ECUDA, "jit pass: launch failed");
+    return DESV_OK;
+}
+
+extern "C" int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int dtype, const desv_adj_pass *ps,
+                                const desv_op *ops_dev, const void *mats_dev, const int32_t *map_dev,
+                                double *grad_dev, void *scratch, size_t scratch_bytes, void *stream) {
+    if (!handle || !phi || !lam || !ps || !ops_dev || !mats_dev || !map_dev || !grad_dev || !scratch)
+        return fail(DESV_EINVAL, "jit adjoint: null argument");
+    if (phi == lam) return fail(DESV_EINVAL, "jit adjoint: phi and lambda must be distinct buffers");
+    auto *k = static_cast<JitKernel *>(handle);
+    if (k->kind != 1) return fail(DESV_EINVAL, "jit adjoint: the kernel is not an adjoint pass");
+    if (dtype != k->dtype) return fail(DESV_EINVAL, "jit adjoint: dtype differs from the compiled kernel");
+    if (n < 1 || n > 34) return fail(DESV_EINVAL, "jit adjoint: n out of range");
+    if (reinterpret_cast<uintptr_t>(phi) % 16 || reinterpret_cast<uintptr_t>(lam) % 16)
+        return fail(DESV_EINVAL, "jit adjoint: states not 16-byte aligned");
+    if (ps->nparams < 0 || ps->nparams > JIT_ADJ_MAX_PARAMS || ps->map_begin < 0)
+        return fail(DESV_EINVAL, "jit adjoint: parameter range invalid");
+    if (scratch_bytes < adjoint_scratch_bytes(ps->nparams)) return fail(DESV_EINVAL, "jit adjoint: scratch too small");
+    TileGeom g;
+    if (ps->tile_bits != k->K || ps->tile_bits > n || ps->low_bits < 5 || ps->tile_bits - ps->low_bits > 8 ||
+        !make_geom(g, n, ps->tile_bits, ps->low_bits, ps->high))
+        return fail(DESV_EINVAL, "jit adjoint: tile geometry does not match the compiled kernel");
+    if (ps->op_end == ps->op_begin) return DESV_OK;
+    const int nw = (1 << (k->K - 4)) / 32 > 0 ? (1 << (k->K - 4)) / 32 : 1;
+    const size_t smem = k->smem + (size_t)nw * ps->nparams * sizeof(double);
+    int bps = 0;
+    api().OccupancyMaxActiveBlocksPerMultiprocessor(&bps, k->fn, 1 << (k->K - 4), smem);
+    if (bps < 1) bps = 1;
+    const uint64_t ntiles = 1ull << (n - k->K);
+    uint64_t cap = (uint64_t)sm_count() * bps;
+    if (cap > JIT_ADJ_MAX_ROWS) cap = JIT_ADJ_MAX_ROWS;
+    const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
+    int np = ps->nparams;
+    double *part = static_cast<double *>(scratch);
+    void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&mats_dev), &np, &part};
+    if (api().LaunchKernel(k->fn, grid, 1, 1, 1u << (k->K - 4), 1, 1, (unsigned)smem, stream, args, nullptr) != 0)
+        return fail(DESV_ECUDA, "jit adjoint: launch failed");
+    if (np > 0) return grad_reduce(part, (int)grid, np, map_dev + ps->map_begin, grad_dev, static_cast<cudaStream_t>(stream));
     return DESV_OK;
 }

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "desv_common.cuh"
+#include "grad_ops.cuh"
 #include "stage_ops.cuh"
 #include "tile_pipeline.cuh"
 
@@ -47,6 +48,20 @@ template <typename T, uint32_t G0, uint32_t G1, uint32_t G2, uint32_t G3> struct
     }
 };
 
+// Two arrays in lockstep (the adjoint pass's phi and lambda).
+template <typename T, class S> struct JitStage2 {
+    static __device__ __forceinline__ void store_smem(const T (&a)[16], const T (&b)[16], T *sa, T *sb,
+                                                      uint32_t idx) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            sa[idx + S::off(j)] = a[j];
+            sb[idx + S::off(j)] = b[j];
+        }
+        __syncthreads();
+        fence_proxy_async_smem();
+    }
+};
+
 // The pass: `stages(slot, tile_base, ctab, L)` applies every stage of one tile.
 template <typename T, int K, int NBUF, class Stages>
 __device__ __forceinline__ void jit_pass_kernel(T *sv, const TileGeom &g, unsigned char *smem, Stages &stages) {
@@ -57,6 +72,74 @@ __device__ __forceinline__ void jit_pass_kernel(T *sv, const TileGeom &g, unsign
     const int L = g.L;
     auto body = [=, &stages](T *const *sp, uint64_t base, uint64_t) { stages(sp[0], base, pipe_ctab(smem), L); };
     run_tiles<T, K, NBUF, 1>(g, A, body, smem);
+}
+
+// Gradient probes Re sum conj(b) (G a) with the generator's placement as
+// compile-time constants (the forms of grad_term in grad_ops.cuh).  The thread
+// predicate is applied by the caller after the call, since lane-bit
+// generators shuffle with every lane.
+template <int S, int CS, typename T>
+__device__ __forceinline__ double jit_grad_reg(const T (&a)[16], const T (&b)[16], const T *mp) {
+    return (double)grad_reg<S>(a, b, mp[0], mp[1], mp[2], mp[3], CS);
+}
+template <int CS, typename T>
+__device__ __forceinline__ double jit_grad_lane(const T (&a)[16], const T (&b)[16], const T *mp, int lb, int lane) {
+    const T g00 = mp[0], g01 = mp[1], g10 = mp[2], g11 = mp[3];
+    const int mine = (lane >> lb) & 1;
+    const T cself = mine ? g11 : g00, coth = mine ? g10 : g01;
+    decltype(a[0].x) acc = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if (CS >= 0 && !((j >> CS) & 1)) continue;
+        const T p = shfl_xor(a[j], 1 << lb);
+        const T v = cfma(coth, p, cmul(cself, a[j]));
+        acc += b[j].x * v.x + b[j].y * v.y;
+    }
+    return (double)acc;
+}
+template <int SA, int SB, typename T>
+__device__ __forceinline__ double jit_grad_diag(const T (&a)[16], const T (&b)[16], const T *mp, int fa, int fb) {
+    const T d0 = mp[0], d1 = mp[1], d2 = mp[2], d3 = mp[3];
+    decltype(a[0].x) acc = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int ba = SA >= 0 ? ((j >> SA) & 1) : fa;
+        const int bb = SB >= 0 ? ((j >> SB) & 1) : fb;
+        const int k = ba | (bb << 1);
+        const T f = k == 0 ? d0 : k == 1 ? d1 : k == 2 ? d2 : d3;
+        const T ga = cmul(f, a[j]);
+        acc += b[j].x * ga.x + b[j].y * ga.y;
+    }
+    return (double)acc;
+}
+
+// Adjoint backward pass over (phi, lambda): `stages(sphi, slam, base, ctab, L,
+// acc)` walks one tile; GRAD probes add into the per-warp FP64 accumulators
+// acc[warp * nparams + p] in shared memory, reduced per CTA into part[] at the
+// end (the layout k_grad_reduce reads).
+template <typename T, int K, int NBUF, class Stages>
+__device__ __forceinline__ void jit_adjoint_kernel(T *phi, T *lam, const TileGeom &g, unsigned char *smem, int nparams,
+                                                   double *part, Stages &stages) {
+    constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
+    double *acc = reinterpret_cast<double *>(smem + PIPE_HDR_BYTES + (size_t)NBUF * 2 * (1u << K) * sizeof(T));
+    for (int i = threadIdx.x; i < NW * nparams; i += blockDim.x) acc[i] = 0.0;
+    PipeArrays<T, 2> A;
+    A.ptr[0] = phi;
+    A.ptr[1] = lam;
+    A.load[0] = A.load[1] = true;
+    A.store[0] = A.store[1] = false;
+    const int L = g.L;
+    auto body = [=, &stages](T *const *sp, uint64_t base, uint64_t) {
+        stages(sp[0], sp[1], base, pipe_ctab(smem), L, acc);
+    };
+    __syncthreads();
+    run_tiles<T, K, NBUF, 2>(g, A, body, smem);
+    __syncthreads();
+    for (int p = threadIdx.x; p < nparams; p += blockDim.x) {
+        double s = 0;
+        for (int w = 0; w < NW; ++w) s += acc[w * nparams + p];
+        part[(size_t)blockIdx.x * nparams + p] = s;
+    }
 }
 
 }  // namespace desv

@@ -148,7 +148,7 @@ class CompiledCircuit:
         passes = self._passes
         if jit.enabled(self.n):
             jit.run_passes(self.specialised_kernels(sv.device), sv.data_ptr(), self.n, code, passes,
-                           mats_t.data_ptr(), st.value)
+                           ops_t.data_ptr(), mats_t.data_ptr(), st.value)
             return sv
         N.check(lib.desv_apply_passes(ctypes.c_void_p(sv.data_ptr()), self.n, code,
                                       ctypes.c_void_p(passes.ctypes.data), len(passes),

@@ -111,6 +111,82 @@ def _op_code(o, words: np.ndarray, wpe: int) -> str:
     return call
 
 
+def _grad_code(o) -> str:
+    """A GRAD probe with its generator's placement compiled in (grad_term's forms)."""
+    mp = f'mats + {int(o["mat"])}'
+    cs = int(o['cslot'])
+    if int(o['s1']) == 1:                          # diagonal generator over ga / gb
+        sa, sb = int(o['sa']), int(o['sb'])
+        ga, gb = int(o['ga']), int(o['gb'])
+        fa = '0' if ga == 0xFF else f'(int)((tg >> {ga}) & 1ull)'
+        fb = '0' if gb == 0xFF else f'(int)((tg >> {gb}) & 1ull)'
+        call = f'jit_grad_diag<{sa}, {sb}>(a, b, {mp}, {fa}, {fb})'
+    elif int(o['s0']) >= 16:                       # lane-bit generator
+        call = f'jit_grad_lane<{cs}>(a, b, {mp}, {int(o["s0"]) - 16}, lane)'
+    else:
+        call = f'jit_grad_reg<{int(o["s0"])}, {cs}>(a, b, {mp})'
+    pred = f'(tg & {_hex(o["cmask"])}) == {_hex(o["cval"])}'
+    return (f'{{ double v = {call}; v = warp_sum_d({pred} ? v : 0.0); '
+            f'if (lane == 0) acc[warp * nparams + {int(o["param"])}] += v; }}')
+
+
+def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: int, complex64: bool,
+                   words: np.ndarray, wpe: int) -> str:
+    """CUDA source of one specialised adjoint backward pass over ops[begin:end]
+    (absolute indices into the op array the kernel receives): every inverse
+    gate is applied to phi (a) and lambda (b); a GRAD op adds its probe
+    2 Re<lambda|G|phi> (the factor 2 comes in the reduction) to its slot."""
+    T = 'float2' if complex64 else 'double2'
+    lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
+             f'extern "C" __global__ void __launch_bounds__({1 << (tile_bits - 4)}, 1)',
+             f'desv_jit_kernel({T} *phi, {T} *lam, TileGeom g, const desv_op *__restrict__ ops, '
+             f'const {T} *__restrict__ mats, int nparams, double *part) {{',
+             '    extern __shared__ __align__(128) unsigned char smem[];',
+             '    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;',
+             f'    auto stages = [=]({T} *sphi, {T} *slam, uint64_t base, const uint64_t *ctab, int L, double *acc) {{',
+             f'        {T} a[16], b[16];']
+    k = begin
+    while k < end:
+        st = ops[k]
+        if int(st['kind']) != N.OP_STAGE:
+            raise ValueError('pass does not start with a stage record')
+        cnt = int(st['mat'])
+        g = [int(x) for x in st['g']]
+        last = k + 1 + cnt >= end
+        lines.append('        {')
+        lines.append(f'            using S = JitStage<{T}, {g[0]}u, {g[1]}u, {g[2]}u, {g[3]}u>;')
+        lines.append('            const uint32_t idx = S::index();')
+        lines.append('            S::load(a, sphi, idx);')
+        lines.append('            S::load(b, slam, idx);')
+        lines.append('            const uint64_t tg = base | tl2g(ctab, L, idx);')
+        for q in range(k + 1, k + 1 + cnt):
+            o = ops[q]
+            if int(o['kind']) == N.OP_GRAD:
+                lines.append('            ' + _grad_code(o))
+                continue
+            code = _op_code(o, words, wpe)
+            if code:
+                lines.append('            ' + code)
+                lines.append('            ' + code.replace('(a, ', '(b, '))
+        if last:
+            lines.append('            S::store_global(a, phi, tg, ctab, L);')
+            lines.append('            S::store_global(b, lam, tg, ctab, L);')
+        else:
+            lines.append(f'            JitStage2<{T}, S>::store_smem(a, b, sphi, slam, idx);')
+        lines.append('        }')
+        k += 1 + cnt
+    lines += ['    };', f'    jit_adjoint_kernel<{T}, {tile_bits}, {nbuf}>(phi, lam, g, smem, nparams, part, stages);',
+              '}', '']
+    return '\n'.join(lines)
+
+
+def adjoint_nbuf_for(tile_bits: int, complex64: bool) -> int:
+    """Ring depth of the adjoint interpreter for this tile width (k_adjoint.cu)."""
+    if complex64:
+        return 3 if tile_bits >= 11 else 4
+    return 3 if tile_bits >= 10 else 4
+
+
 def pass_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: int, complex64: bool,
                 words: np.ndarray, wpe: int) -> str:
     """CUDA source of one specialised pass over ops[begin:end]."""
@@ -153,6 +229,9 @@ def nbuf_for(tile_bits: int) -> int:
 
 # below this size a pass is too short for its compile to pay off
 MIN_QUBITS = 20
+# passes with more op records than this stay on the interpreter: every op is
+# unrolled over 16 amplitudes, and compile time grows with the pass
+MAX_OPS = 96
 _available = None
 
 
@@ -191,21 +270,31 @@ _cache: dict = {}
 _cache_lock = threading.Lock()
 
 
-def _load(src: str, tile_bits: int, nbuf: int, dtype_code: int, device: int) -> _Kernel:
-    key = (hashlib.sha1(src.encode()).hexdigest(), device)
+KIND_PASS, KIND_ADJOINT = 0, 1
+
+
+def _load(src: str, tile_bits: int, nbuf: int, dtype_code: int, device: int, kind: int = KIND_PASS) -> _Kernel:
+    key = (hashlib.sha1(src.encode()).hexdigest(), device, kind)
     with _cache_lock:
         k = _cache.get(key)
     if k is not None:
         return k
     h = ctypes.c_void_p()
     log = ctypes.create_string_buffer(8192)
-    rc = N.lib().desv_jit_load(src.encode(), INCLUDE_PATH.encode(), tile_bits, nbuf, dtype_code, device,
+    rc = N.lib().desv_jit_load(src.encode(), INCLUDE_PATH.encode(), kind, tile_bits, nbuf, dtype_code, device,
                                ctypes.byref(h), log, 8192)
     N.check(rc, 'desv_jit_load')
     k = _Kernel(h)
     with _cache_lock:
         _cache.setdefault(key, k)
         return _cache[key]
+
+
+def _compile(jobs, code, device, kind, workers):
+    """Kernels for the jobs (None stays None: that pass runs on the interpreter)."""
+    workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(lambda j: None if j is None else _load(j[0], j[1], j[2], code, device, kind), jobs))
 
 
 def compile_passes(ops: np.ndarray, passes: np.ndarray, mats_host: np.ndarray, complex64: bool, device: int,
@@ -219,17 +308,59 @@ def compile_passes(ops: np.ndarray, passes: np.ndarray, mats_host: np.ndarray, c
     for p in passes:
         K = int(p['tile_bits'])
         nb = nbuf_for(K)
-        jobs.append((pass_source(ops, int(p['op_begin']), int(p['op_end']), K, nb, complex64, words, wpe), K, nb))
-    workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
-    with ThreadPoolExecutor(max_workers=workers) as ex:
-        return list(ex.map(lambda j: _load(j[0], j[1], j[2], code, device), jobs))
+        b, e = int(p['op_begin']), int(p['op_end'])
+        jobs.append((pass_source(ops, b, e, K, nb, complex64, words, wpe), K, nb) if 0 < e - b <= MAX_OPS else None)
+    return _compile(jobs, code, device, KIND_PASS, workers)
 
 
-def run_passes(kernels: list, sv_ptr: int, n: int, dtype_code: int, passes: np.ndarray, mats_ptr: int, stream):
+def compile_adjoint(ops: np.ndarray, passes: np.ndarray, mats_host: np.ndarray, complex64: bool, device: int,
+                    workers: int = 0) -> list:
+    """One specialised adjoint backward kernel per pass (None for an empty pass)."""
+    words = np.ascontiguousarray(mats_host).view(np.uint32)
+    wpe = mats_host.dtype.itemsize // 4
+    code = N.DESV_C64 if complex64 else N.DESV_C128
+    jobs = []
+    for p in passes:
+        K = int(p['tile_bits'])
+        nb = adjoint_nbuf_for(K, complex64)
+        b, e = int(p['op_begin']), int(p['op_end'])
+        jobs.append((adjoint_source(ops, b, e, K, nb, complex64, words, wpe), K, nb) if 0 < e - b <= MAX_OPS else None)
+    return _compile(jobs, code, device, KIND_ADJOINT, workers)
+
+
+def run_adjoint(kernels: list, phi_ptr: int, lam_ptr: int, n: int, dtype_code: int, passes: np.ndarray,
+                ops_ptr: int, mats_ptr: int, map_ptr: int, grad_ptr: int, scratch_ptr: int, scratch_bytes: int,
+                stream):
+    """The backward sweep, pass by pass: each launch is followed by the
+    gradient reduction of its partial sums (desv_jit_adjoint)."""
     lib = N.lib()
     st = ctypes.c_void_p(stream)
     base = passes.ctypes.data
     for i, k in enumerate(kernels):
-        N.check(lib.desv_jit_pass(k.handle, ctypes.c_void_p(sv_ptr), n, dtype_code,
-                                  ctypes.c_void_p(base + i * passes.itemsize), ctypes.c_void_p(mats_ptr), st),
-                'desv_jit_pass')
+        pp = ctypes.c_void_p(base + i * passes.itemsize)
+        if k is None:
+            N.check(lib.desv_adjoint_passes(ctypes.c_void_p(phi_ptr), ctypes.c_void_p(lam_ptr), n, dtype_code, pp, 1,
+                                            ctypes.c_void_p(ops_ptr), ctypes.c_void_p(mats_ptr),
+                                            ctypes.c_void_p(map_ptr), ctypes.c_void_p(grad_ptr),
+                                            ctypes.c_void_p(scratch_ptr), scratch_bytes, st), 'adjoint pass')
+        else:
+            N.check(lib.desv_jit_adjoint(k.handle, ctypes.c_void_p(phi_ptr), ctypes.c_void_p(lam_ptr), n, dtype_code,
+                                         pp, ctypes.c_void_p(ops_ptr), ctypes.c_void_p(mats_ptr),
+                                         ctypes.c_void_p(map_ptr), ctypes.c_void_p(grad_ptr),
+                                         ctypes.c_void_p(scratch_ptr), scratch_bytes, st), 'desv_jit_adjoint')
+
+
+def run_passes(kernels: list, sv_ptr: int, n: int, dtype_code: int, passes: np.ndarray, ops_ptr: int,
+               mats_ptr: int, stream):
+    """passes[i] through kernels[i], or through the interpreter where that is None."""
+    lib = N.lib()
+    st = ctypes.c_void_p(stream)
+    base = passes.ctypes.data
+    for i, k in enumerate(kernels):
+        pp = ctypes.c_void_p(base + i * passes.itemsize)
+        if k is None:
+            N.check(lib.desv_apply_passes(ctypes.c_void_p(sv_ptr), n, dtype_code, pp, 1, ctypes.c_void_p(ops_ptr),
+                                          ctypes.c_void_p(mats_ptr), st), 'apply fused pass')
+        else:
+            N.check(lib.desv_jit_pass(k.handle, ctypes.c_void_p(sv_ptr), n, dtype_code, pp,
+                                      ctypes.c_void_p(mats_ptr), st), 'desv_jit_pass')

@@ -27,7 +27,7 @@ import numpy as np
 import torch
 
 from .. import _native as N
-from ..circuits import fusion
+from ..circuits import fusion, jit
 from ..circuits.compiler import CompiledCircuit, apply_fop
 from ..physics.observables import PauliPlan, PauliSumOperator, plan_for
 
@@ -192,12 +192,22 @@ class AdjointProgram:
             ops_t = torch.from_numpy(self.back.ops.view(np.uint8).copy()).to(dev)
             mats_t = torch.from_numpy(mats.view(rdt).copy()).to(dev)
             map_t = torch.tensor(self.back.param_map or [0], dtype=torch.int32, device=dev)
-            self._back_dev = (key, ops_t, mats_t, map_t)
-        _, ops_t, mats_t, map_t = self._back_dev
+            self._back_dev = (key, ops_t, mats_t, map_t, mats)
+        _, ops_t, mats_t, map_t, mats = self._back_dev
         need = int(N.lib().desv_adjoint_scratch_bytes(max(self.back.max_params, 1)))
         if self._scratch is None or self._scratch.numel() * 8 < need:
             self._scratch = torch.empty((need + 7) // 8, dtype=torch.float64, device=dev)
         p = self.back.passes
+        if jit.enabled(self.n) and self.dtype == torch.complex64:
+            # plan-specialised backward passes (complex64: the complex128 pair of
+            # register tiles does not fit the register file); sources, and so
+            # kernels, change only with the records' dispatch codes
+            kernels = jit.compile_adjoint(self.back.ops, p, mats, self.dtype == torch.complex64,
+                                          dev.index if dev.index is not None else torch.cuda.current_device())
+            jit.run_adjoint(kernels, mu.data_ptr(), lam.data_ptr(), self.n, N.dtype_code(mu), p, ops_t.data_ptr(),
+                            mats_t.data_ptr(), map_t.data_ptr(), grad.data_ptr(), self._scratch.data_ptr(),
+                            self._scratch.numel() * 8, N.stream_ptr())
+            return
         N.check(N.lib().desv_adjoint_passes(
             ctypes.c_void_p(mu.data_ptr()), ctypes.c_void_p(lam.data_ptr()), self.n, N.dtype_code(mu),
             ctypes.c_void_p(p.ctypes.data), len(p), ctypes.c_void_p(ops_t.data_ptr()),

@@ -279,15 +279,22 @@ int desv_sample_pick(const void *sv, int n, int dtype, const void *scratch, size
 /* 1 if NVRTC and the CUDA driver could be opened; else 0 and the reason in why */
 int desv_jit_available(char *why, size_t len);
 /* Compile + load one pass kernel (entry point "desv_jit_kernel", tile shape
- * tile_bits / nbuf ring slots).  include_dirs: directories separated by ':'.
- * The NVRTC log goes to log (may be NULL). */
-int desv_jit_load(const char *src, const char *include_dirs, int tile_bits, int nbuf, int dtype, int device,
-                  void **handle, char *log, size_t loglen);
+ * tile_bits / nbuf ring slots); kind 0: a fused pass (desv_jit_pass), kind 1:
+ * an adjoint backward pass (desv_jit_adjoint).  include_dirs: directories
+ * separated by ':'.  The NVRTC log goes to log (may be NULL). */
+int desv_jit_load(const char *src, const char *include_dirs, int kind, int tile_bits, int nbuf, int dtype,
+                  int device, void **handle, char *log, size_t loglen);
 int desv_jit_free(void *handle);
 /* Run the loaded kernel over one pass (its tile geometry must match the
  * compiled tile_bits); mats_dev is the same matrix pool desv_apply_passes reads. */
 int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pass, const void *mats_dev,
                   void *stream);
+/* One adjoint backward pass (the work of desv_adjoint_passes for that pass,
+ * including the gradient reduction into grad_dev[map_dev[map_begin + p]]);
+ * ops_dev is the whole op array (the compiled source indexes it absolutely). */
+int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int dtype, const desv_adj_pass *pass,
+                     const desv_op *ops_dev, const void *mats_dev, const int32_t *map_dev, double *grad_dev,
+                     void *scratch, size_t scratch_bytes, void *stream);
 
 /* ---- Pauli sums (replaces pauli_sum_expectation / pauli_sum_matvec,
  *      physics/observables.py:63-186,250-308) ------------------------------- */

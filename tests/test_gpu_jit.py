@@ -117,3 +117,32 @@ def test_default_path_at_22_qubits_matches_interpreter(monkeypatch):
     interp = _run(plan, n, torch.complex64)
     assert np.max(np.abs(spec - interp)) <= 1e-6
     de._native.device_status()
+
+
+@pytest.mark.parametrize('n', [12, 15])
+def test_specialised_adjoint_matches_interpreter_and_fd(n, monkeypatch):
+    """Backward passes compiled per pass (complex64) against the interpreted
+    backward sweep and complex128 central differences."""
+    import dense_evolution as de
+    from dense_evolution.workloads import hea_circuit, tfim_terms
+    layers = 3
+    circ = hea_circuit(n, layers) + [('crz', 0, n - 1, 0.0), ('cp', 2, 1, 0.0), ('p', 3, 0.0)]
+    terms = tfim_terms(n) + [(0.3, {0: 'Y', n - 1: 'Y'})]
+    theta = np.random.default_rng(n).uniform(-np.pi, np.pi, de.circuit_to_energy_fn(circ, n)[1])
+    res = {}
+    for flag in ('0', '1'):
+        monkeypatch.setenv('DESV_JIT', flag)
+        fn, _ = de.circuit_to_energy_fn(circ, n, use_float32=True)
+        e, g, _ = fn.program.value_and_grad(theta, terms)
+        res[flag] = (e, g)
+    assert res['1'][0] == pytest.approx(res['0'][0], abs=1e-7)
+    assert np.max(np.abs(res['1'][1] - res['0'][1])) <= 1e-6
+    monkeypatch.setenv('DESV_JIT', '0')
+    f64, _ = de.circuit_to_energy_fn(circ, n)
+    h = 1e-4
+    for i in np.random.default_rng(1).choice(theta.size, 6, replace=False):
+        tp, tm = theta.copy(), theta.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (float(f64(tp, terms)[0]) - float(f64(tm, terms)[0])) / (2 * h)
+        assert res['1'][1][i] == pytest.approx(fd, abs=2e-5)
