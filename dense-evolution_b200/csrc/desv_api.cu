@@ -62,6 +62,8 @@ int adjoint_pass(void *, void *, int, const TileGeom &, const desv_op *, int, co
 int grad_reduce(const double *, int, int, const int32_t *, double *, cudaStream_t);
 size_t adjoint_scratch_bytes(int);
 __global__ void k_sum_rows(const double *, int, int, int, double *);
+int jit_pauli_launch(void *handle, const void *psi, void *out, int dtype, int mode, const TileGeom &g, int want_e,
+                     double *part, int *grid_out, cudaStream_t st);
 
 static inline cudaStream_t S(void *s) { return static_cast<cudaStream_t>(s); }
 
@@ -233,9 +235,10 @@ int desv_collapse(void *sv, int n, int dtype, int bit, int outcome, double s, vo
     return collapse(sv, n, dtype, bit, outcome, s, S(stream));
 }
 
+// handles: NULL, or one specialised kernel (or NULL) per pass (desv_jit_pauli)
 static int pauli_common(const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes, int npasses,
                         const desv_pauli_term *terms, double *expect, void *scratch, size_t sb, bool matvec,
-                        void *stream) {
+                        void *stream, void *const *handles = nullptr) {
     int r = check_state(psi, n, dtype);
     if (r) return r;
     if (matvec && (r = check_state(out, n, dtype))) return r;
@@ -262,8 +265,12 @@ static int pauli_common(const void *psi, void *out, int n, int dtype, const desv
             if (ps.tile_bits > n || ps.low_bits < (n < 5 ? n : 5) ||
                 !make_geom(g, n, ps.tile_bits, ps.low_bits, ps.high))
                 return fail(DESV_EINVAL, "Pauli pass " + std::to_string(p) + ": invalid tile geometry");
-            r = pauli_pass(psi, out, dtype, mode, g, terms + ps.term_begin, nt, want_e ? 1 : 0, part + 2 * rows,
-                           &grid, S(stream));
+            if (handles && handles[p])
+                r = jit_pauli_launch(handles[p], psi, out, dtype, mode, g, want_e ? 1 : 0, part + 2 * rows, &grid,
+                                     S(stream));
+            else
+                r = pauli_pass(psi, out, dtype, mode, g, terms + ps.term_begin, nt, want_e ? 1 : 0,
+                               part + 2 * rows, &grid, S(stream));
         }
         if (r) return r;
         if (want_e) rows += grid;
@@ -294,6 +301,19 @@ int desv_pauli_matvec(const void *psi, void *out, int n, int dtype, const desv_p
                       const desv_pauli_term *terms, double *expect, void *scratch, size_t sb, void *stream) {
     if (psi == out) return fail(DESV_EINVAL, "matvec output must not alias the input");
     return pauli_common(psi, out, n, dtype, passes, npasses, terms, expect, scratch, sb, true, stream);
+}
+
+int desv_jit_pauli(void *const *handles, const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes,
+                   int npasses, const desv_pauli_term *terms, double *expect, void *scratch, size_t sb, int matvec,
+                   void *stream) {
+    if (!handles) return fail(DESV_EINVAL, "jit Pauli: null handle array");
+    if (matvec) {
+        if (psi == out) return fail(DESV_EINVAL, "matvec output must not alias the input");
+    } else if (!expect) {
+        return fail(DESV_EINVAL, "null output");
+    }
+    return pauli_common(psi, matvec ? out : nullptr, n, dtype, passes, npasses, terms, expect, scratch, sb,
+                        matvec != 0, stream, handles);
 }
 
 }  // extern "C"

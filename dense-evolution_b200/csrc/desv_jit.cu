@@ -122,6 +122,26 @@ static int jit_status_read_clear() {
 }
 static const int jit_status_registered = (register_status_reader(&jit_status_read_clear), 0);
 
+// One tiled Pauli pass through a specialised kernel (called by the Pauli-sum
+// driver in desv_api.cu for the passes that have one): same grid rule and
+// partial-sum layout as the interpreter pass.
+int jit_pauli_launch(void *handle, const void *psi, void *out, int dtype, int mode, const TileGeom &g, int want_e,
+                     double *part, int *grid_out, cudaStream_t st) {
+    auto *k = static_cast<JitKernel *>(handle);
+    if (k->kind != 2 + mode) return fail(DESV_EINVAL, "jit Pauli pass: the kernel was compiled for another mode");
+    if (dtype != k->dtype || g.K != k->K || g.K - g.L > 8)
+        return fail(DESV_EINVAL, "jit Pauli pass: dtype or tile geometry differs from the compiled kernel");
+    const uint64_t ntiles = 1ull << (g.n - k->K);
+    const uint64_t cap = (uint64_t)sm_count() * k->blocks_per_sm;
+    const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
+    *grid_out = (int)grid;
+    TileGeom gg = g;
+    void *args[] = {const_cast<void **>(&psi), &out, &gg, &want_e, &part};
+    if (api().LaunchKernel(k->fn, grid, 1, 1, 256, 1, 1, (unsigned)k->smem, st, args, nullptr) != 0)
+        return fail(DESV_ECUDA, "jit Pauli pass: launch failed");
+    return DESV_OK;
+}
+
 }  // namespace desv
 
 using namespace desv;
@@ -140,7 +160,8 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind,
     if (!src || !include_dir || !handle) return fail(DESV_EINVAL, "jit load: null argument");
     *handle = nullptr;
     if (dtype != DESV_C64 && dtype != DESV_C128) return fail(DESV_EINVAL, "jit load: bad dtype");
-    if (kind != 0 && kind != 1) return fail(DESV_EINVAL, "jit load: kind must be 0 (pass) or 1 (adjoint)");
+    if (kind < 0 || kind > 4)
+        return fail(DESV_EINVAL, "jit load: kind must be 0 (pass), 1 (adjoint) or 2..4 (Pauli pass, mode 0..2)");
     if (tile_bits < 9 || tile_bits > (dtype == DESV_C64 ? 13 : 12) || nbuf < 2 || nbuf > 4)
         return fail(DESV_EINVAL, "jit load: bad tile shape");
     const JitApi &a = api();
@@ -185,9 +206,9 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind,
     k->dtype = dtype;
     const size_t esz = dtype == DESV_C64 ? 8 : 16;
     const int nw = (1 << (tile_bits - 4)) / 32 > 0 ? (1 << (tile_bits - 4)) / 32 : 1;
-    k->smem = PIPE_HDR_BYTES + (size_t)nbuf * (kind ? 2 : 1) * ((size_t)1 << tile_bits) * esz;
+    k->smem = PIPE_HDR_BYTES + (size_t)nbuf * (kind == 1 ? 2 : 1) * ((size_t)1 << tile_bits) * esz;
     // adjoint kernels: room for the per-warp gradient accumulators of the largest pass
-    const size_t smem_max = k->smem + (kind ? (size_t)nw * JIT_ADJ_MAX_PARAMS * sizeof(double) : 0);
+    const size_t smem_max = k->smem + (kind == 1 ? (size_t)nw * JIT_ADJ_MAX_PARAMS * sizeof(double) : 0);
     size_t ssz = 0;
     // bind the device's primary context to this thread (compiles may run on worker threads)
     if (cudaSetDevice(device) != cudaSuccess) {
@@ -207,7 +228,7 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind,
         return fail(DESV_ECUDA, "jit: shared-memory attribute refused");
     }
     int b = 0;
-    a.OccupancyMaxActiveBlocksPerMultiprocessor(&b, k->fn, 1 << (tile_bits - 4), k->smem);
+    a.OccupancyMaxActiveBlocksPerMultiprocessor(&b, k->fn, kind >= 2 ? 256 : 1 << (tile_bits - 4), k->smem);
     k->blocks_per_sm = b > 0 ? b : 1;
     {
         std::lock_guard<std::mutex> lk(g_jit_mu);

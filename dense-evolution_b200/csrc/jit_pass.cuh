@@ -142,4 +142,46 @@ __device__ __forceinline__ void jit_adjoint_kernel(T *phi, T *lam, const TileGeo
     }
 }
 
+// Pauli-sum pass over psi tiles (MODE 0: <H> only, 1: write H psi, 2: add
+// into H psi): `body(tile, base, ctab, L, ere, eim)` evaluates the pass's terms
+// (compiled in) for the tile's amplitudes.  The FP64 energy partials are
+// reduced per CTA into part[2 * blockIdx.x + {0, 1}], the layout the
+// interpreter k_pauli writes.
+template <typename T, int K, int NBUF, class Body>
+__device__ __forceinline__ void jit_pauli_kernel(const T *psi, const TileGeom &g, int want_e, double *part,
+                                                 unsigned char *smem, Body &body) {
+    PipeArrays<T, 1> A;
+    A.ptr[0] = const_cast<T *>(psi);
+    A.load[0] = true;
+    A.store[0] = false;
+    const int L = g.L;
+    double ere = 0, eim = 0;
+    auto tb = [=, &ere, &eim, &body](T *const *sp, uint64_t base, uint64_t) {
+        body(sp[0], base, pipe_ctab(smem), L, ere, eim);
+    };
+    __syncthreads();
+    run_tiles<T, K, NBUF, 1>(g, A, tb, smem);
+    if (want_e) {
+        __shared__ double sh[32];
+        const double r = warp_sum_d(ere), i2 = warp_sum_d(eim);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        __syncthreads();
+        if (l == 0) sh[w] = r;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+            part[2 * blockIdx.x] = t;
+        }
+        __syncthreads();
+        if (l == 0) sh[w] = i2;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+            part[2 * blockIdx.x + 1] = t;
+        }
+    }
+}
+
 }  // namespace desv

@@ -222,6 +222,134 @@ def pass_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: int
     return '\n'.join(lines)
 
 
+# Pauli passes: more terms than this stay on the interpreter
+MAX_PAULI_TERMS = 64
+
+
+def _tile_local(m: int, L: int, high) -> int:
+    """Tile-local form of the global bit mask m (bits 0..L-1, then high[i] -> L + i)."""
+    x = m & ((1 << L) - 1)
+    for i, h in enumerate(high):
+        if (m >> h) & 1:
+            x |= 1 << (L + i)
+    return x
+
+
+def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: int, complex64: bool) -> str:
+    """CUDA source of one specialised Pauli pass (the interpreter k_pauli with
+    the pass's terms compiled in): mode 0 <H> only, 1 write H psi, 2 add into
+    H psi.  Terms with one flip mask share the partner amplitude; real
+    coefficients take the two-FMA form.  (P psi)[i] = psi[i ^ x] c
+    (-1)^popcount((i ^ x) & z); the z bits outside the tile give a per-tile
+    parity."""
+    T = 'float2' if complex64 else 'double2'
+    R = 'float' if complex64 else 'double'
+    K, L = tile_bits, low_bits
+    high = [int(h) for h in high[:K - L]]
+    tile_mask = ((1 << L) - 1) | sum(1 << h for h in high)
+    lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
+             'extern "C" __global__ void __launch_bounds__(256)',
+             f'desv_jit_kernel(const {T} *psi, {T} *out, TileGeom g, int want_e, double *part) {{',
+             '    extern __shared__ __align__(128) unsigned char smem[];',
+             f'    auto body = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L, double &ere, double &eim) {{']
+    groups = {}
+    for k, t in enumerate(terms):
+        groups.setdefault(int(t['xmask']), []).append(k)
+    for k, t in enumerate(terms):
+        zo = int(t['zmask']) & ~tile_mask
+        if zo:
+            lines.append(f'        const uint32_t pb{k} = (uint32_t)__popcll(base & {_hex(zo)}) & 1u;')
+    lines += ['#pragma unroll 1',
+              f'        for (uint32_t j0 = threadIdx.x; j0 < {1 << K}u; j0 += 1024u) {{',
+              '            double2 v[4];',
+              '#pragma unroll',
+              '            for (int r = 0; r < 4; ++r) v[r] = make_double2(0.0, 0.0);']
+    for x, ks in groups.items():
+        xl = _tile_local(x, L, high)
+        lines.append('            {')
+        lines.append('                double2 p[4];')
+        lines.append('#pragma unroll')
+        lines.append(f'                for (int r = 0; r < 4; ++r) {{ const {T} q = s[(j0 + r * 256u) ^ {xl}u]; '
+                     'p[r] = make_double2((double)q.x, (double)q.y); }')
+        lines.append('#pragma unroll')
+        lines.append('                for (int r = 0; r < 4; ++r) {')
+        lines.append('                    const uint32_t j = j0 + r * 256u;')
+        for k in ks:
+            t = terms[k]
+            zl = _tile_local(int(t['zmask']) & tile_mask, L, high)
+            zo = int(t['zmask']) & ~tile_mask
+            cre, cim = float(t['cre']), float(t['cim'])
+            parts = []
+            if zl:
+                parts.append(f'__popc((j ^ {xl}u) & {zl}u)')
+            if zo:
+                parts.append(f'pb{k}')
+            sg = f'(({" ^ ".join(parts)}) & 1u)' if parts else None
+            if cim == 0.0:
+                c = f'{cre!r}' if sg is None else f'({sg} ? {-cre!r} : {cre!r})'
+                lines.append(f'                    {{ const double c = {c}; v[r].x = fma(c, p[r].x, v[r].x); '
+                             'v[r].y = fma(c, p[r].y, v[r].y); }')
+            else:
+                c = (f'make_double2({cre!r}, {cim!r})' if sg is None else
+                     f'({sg} ? make_double2({-cre!r}, {-cim!r}) : make_double2({cre!r}, {cim!r}))')
+                lines.append(f'                    v[r] = cfma({c}, p[r], v[r]);')
+        lines.append('                }')
+        lines.append('            }')
+    lines += ['#pragma unroll',
+              '            for (int r = 0; r < 4; ++r) {',
+              '                const uint32_t j = j0 + r * 256u;']
+    if mode != 0:
+        lines.append('                { const ' + T + ' a = s[j]; ere += (double)a.x * v[r].x + (double)a.y * v[r].y; '
+                     'eim += (double)a.x * v[r].y - (double)a.y * v[r].x; }')
+        lines.append('                const uint64_t gi = base + tl2g(ctab, L, j);')
+        if mode == 1:
+            lines.append(f'                out[gi] = mk(({R})v[r].x, ({R})v[r].y);')
+        else:
+            lines.append(f'                {{ {T} o = out[gi]; o.x = ({R})((double)o.x + v[r].x); '
+                         f'o.y = ({R})((double)o.y + v[r].y); out[gi] = o; }}')
+    else:
+        lines.append('                if (want_e) { const ' + T + ' a = s[j]; ere += (double)a.x * v[r].x + '
+                     '(double)a.y * v[r].y; eim += (double)a.x * v[r].y - (double)a.y * v[r].x; }')
+    lines += ['            }', '        }', '    };',
+              f'    jit_pauli_kernel<{T}, {K}, 4>(psi, g, want_e, part, smem, body);', '}', '']
+    return '\n'.join(lines)
+
+
+def pauli_modes(passes: np.ndarray, matvec: bool) -> list:
+    """The kernel mode each pass runs in, as desv_jit_pauli walks them (None:
+    skipped): <H> passes 0; H psi: 1 for the first pass run, 2 after it."""
+    out, wrote = [], False
+    for p in passes:
+        nt = int(p['term_end']) - int(p['term_begin'])
+        if nt == 0 and (not matvec or wrote):
+            out.append(None)
+            continue
+        out.append((2 if wrote else 1) if matvec else 0)
+        wrote = True
+    return out
+
+
+def compile_pauli(terms: np.ndarray, passes: np.ndarray, matvec: bool, complex64: bool, device: int,
+                  workers: int = 0) -> list:
+    """One specialised kernel per tiled Pauli pass in the mode that call runs it
+    (None: the interpreter runs that pass)."""
+    code = N.DESV_C64 if complex64 else N.DESV_C128
+    jobs, kinds = [], []
+    for p, mode in zip(passes, pauli_modes(passes, matvec)):
+        K, L = int(p['tile_bits']), int(p['low_bits'])
+        b, e = int(p['term_begin']), int(p['term_end'])
+        if mode is None or K < 10 or K - L > 8 or not 0 < e - b <= MAX_PAULI_TERMS:
+            jobs.append(None)
+            kinds.append(None)
+            continue
+        jobs.append((pauli_source(terms[b:e], K, L, p['high'], mode, complex64), K, 4))
+        kinds.append(KIND_PAULI + mode)
+    workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(lambda a: None if a[0] is None else _load(a[0][0], a[0][1], a[0][2], code, device, a[1]),
+                           zip(jobs, kinds)))
+
+
 def nbuf_for(tile_bits: int) -> int:
     """Ring depth of the interpreter for this tile width (k_fused.cu)."""
     return 3 if tile_bits >= 12 else 4
@@ -270,7 +398,7 @@ _cache: dict = {}
 _cache_lock = threading.Lock()
 
 
-KIND_PASS, KIND_ADJOINT = 0, 1
+KIND_PASS, KIND_ADJOINT, KIND_PAULI = 0, 1, 2   # Pauli: + mode (0, 1, 2)
 
 
 def _load(src: str, tile_bits: int, nbuf: int, dtype_code: int, device: int, kind: int = KIND_PASS) -> _Kernel:

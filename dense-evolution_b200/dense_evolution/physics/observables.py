@@ -144,10 +144,27 @@ class PauliPlan:
         self.terms =np.array(term_rows, dtype=N.TERM_DTYPE) if term_rows else np.zeros(0, N.TERM_DTYPE)
         self.passes = np.array(pass_rows, dtype=N.PPASS_DTYPE) if pass_rows else np.zeros(0, N.PPASS_DTYPE)
         self._dev = {}
+        self._jit = {}
 
     @property
     def npasses(self) -> int:
         return len(self.passes)
+
+    def specialised(self, device, dtype, matvec: bool):
+        """ctypes array of one specialised kernel handle (or NULL) per pass for
+        desv_jit_pauli, or None when the interpreter runs every pass."""
+        from ..circuits import jit
+        if not jit.enabled(self.n):
+            return None
+        dev = device.index if device.index is not None else torch.cuda.current_device()
+        key = (dev, dtype, matvec)
+        h = self._jit.get(key)
+        if h is None:
+            ks = jit.compile_pauli(self.terms, self.passes, matvec, dtype == torch.complex64, dev)
+            arr = (ctypes.c_void_p * max(1, len(ks)))(*[k.handle.value if k is not None else None for k in ks])
+            h = (arr, ks)                       # the kernels stay referenced with their handles
+            self._jit[key] = h
+        return h[0]
 
     def terms_dev(self, device) -> torch.Tensor:
         key = (device.type, device.index)
@@ -164,6 +181,14 @@ class PauliPlan:
             return out
         sc = N.scratch(self.n, psi.device)
         tdev = self.terms_dev(psi.device)
+        hs = self.specialised(psi.device, psi.dtype, False)
+        if hs is not None:
+            N.check(N.lib().desv_jit_pauli(hs, ctypes.c_void_p(psi.data_ptr()), None, self.n, N.dtype_code(psi),
+                                           ctypes.c_void_p(self.passes.ctypes.data), len(self.passes),
+                                           ctypes.c_void_p(tdev.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                           ctypes.c_void_p(sc.data_ptr()), sc.numel() * 8, 0,
+                                           ctypes.c_void_p(N.stream_ptr(stream))), 'pauli expectation')
+            return out
         N.check(N.lib().desv_pauli_expect(ctypes.c_void_p(psi.data_ptr()), self.n, N.dtype_code(psi),
                                           ctypes.c_void_p(self.passes.ctypes.data), len(self.passes),
                                           ctypes.c_void_p(tdev.data_ptr()), ctypes.c_void_p(out.data_ptr()),
@@ -181,6 +206,15 @@ class PauliPlan:
             return (out, e) if want_expect else out
         sc = N.scratch(self.n, psi.device)
         tdev = self.terms_dev(psi.device)
+        hs = self.specialised(psi.device, psi.dtype, True)
+        if hs is not None:
+            N.check(N.lib().desv_jit_pauli(hs, ctypes.c_void_p(psi.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                           self.n, N.dtype_code(psi), ctypes.c_void_p(self.passes.ctypes.data),
+                                           len(self.passes), ctypes.c_void_p(tdev.data_ptr()),
+                                           ctypes.c_void_p(e.data_ptr()) if e is not None else None,
+                                           ctypes.c_void_p(sc.data_ptr()), sc.numel() * 8, 1,
+                                           ctypes.c_void_p(N.stream_ptr(stream))), 'pauli matvec')
+            return (out, e) if want_expect else out
         N.check(N.lib().desv_pauli_matvec(ctypes.c_void_p(psi.data_ptr()), ctypes.c_void_p(out.data_ptr()), self.n,
                                           N.dtype_code(psi), ctypes.c_void_p(self.passes.ctypes.data),
                                           len(self.passes), ctypes.c_void_p(tdev.data_ptr()),

@@ -280,7 +280,8 @@ int desv_sample_pick(const void *sv, int n, int dtype, const void *scratch, size
 int desv_jit_available(char *why, size_t len);
 /* Compile + load one pass kernel (entry point "desv_jit_kernel", tile shape
  * tile_bits / nbuf ring slots); kind 0: a fused pass (desv_jit_pass), kind 1:
- * an adjoint backward pass (desv_jit_adjoint).  include_dirs: directories
+ * an adjoint backward pass (desv_jit_adjoint), kind 2 + mode: a Pauli pass
+ * (desv_jit_pauli).  include_dirs: directories
  * separated by ':'.  The NVRTC log goes to log (may be NULL). */
 int desv_jit_load(const char *src, const char *include_dirs, int kind, int tile_bits, int nbuf, int dtype,
                   int device, void **handle, char *log, size_t loglen);
@@ -292,6 +293,13 @@ int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pas
 /* One adjoint backward pass (the work of desv_adjoint_passes for that pass,
  * including the gradient reduction into grad_dev[map_dev[map_begin + p]]);
  * ops_dev is the whole op array (the compiled source indexes it absolutely). */
+/* desv_pauli_expect (matvec == 0) or desv_pauli_matvec (matvec != 0) with the
+ * tiled passes that have a specialised kernel (handles[p] != NULL, loaded with
+ * kind 2 + the mode the pass runs in: 0 <H>; 1 the first H psi pass, 2 the
+ * later ones) run through it; the other passes through the interpreter. */
+int desv_jit_pauli(void *const *handles, const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes,
+                   int npasses, const desv_pauli_term *terms, double *expect, void *scratch, size_t scratch_bytes,
+                   int matvec, void *stream);
 int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int dtype, const desv_adj_pass *pass,
                      const desv_op *ops_dev, const void *mats_dev, const int32_t *map_dev, double *grad_dev,
                      void *scratch, size_t scratch_bytes, void *stream);
