@@ -3,7 +3,7 @@ interpreter and the oracle on the same seeded circuits.
 
 The specialised kernel runs the interpreter's op bodies in the same order, so
 the two agree to rounding (FMA contraction may differ); both are held to the
-oracle at the north-star tolerances (complex128 1e-12, complex64 1e-5)."""
+oracle at the engine's tolerances (complex128 1e-12, complex64 1e-5)."""
 import numpy as np
 import pytest
 

@@ -1,7 +1,7 @@
 """GPU parity: DenseSVSimulator (fused CUDA passes / single-gate kernels) vs the
 reference's own outputs (golden fixtures) and the oracle.
 
-Tolerances (north star): complex128 fidelity >= 1 - 1e-12; complex64
+Tolerances: complex128 fidelity >= 1 - 1e-12; complex64
 max |d amplitude| <= 1e-5."""
 import json
 import os
