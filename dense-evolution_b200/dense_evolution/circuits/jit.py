@@ -259,13 +259,48 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
         zo = int(t['zmask']) & ~tile_mask
         if zo:
             lines.append(f'        const uint32_t pb{k} = (uint32_t)__popcll(base & {_hex(zo)}) & 1u;')
+    # Per flip mask: real-coefficient terms fold into one real factor per
+    # amplitude -- sign masks of one bit, or of two bits at a fixed tile-local
+    # distance, become one popcount per class (sum of c (-1)^bit... over the
+    # class = c (count - 2 popcount)); sign masks wholly outside the tile give a
+    # per-tile constant; the rest add their signed coefficient.  Complex
+    # coefficients keep the per-term complex FMA.
+    plan = []
+    for gi, (x, ks) in enumerate(groups.items()):
+        xl = _tile_local(x, L, high)
+        classes, outside, single, cplx = [], [], [], []
+        for k in ks:
+            t = terms[k]
+            zl = _tile_local(int(t['zmask']) & tile_mask, L, high)
+            zo = int(t['zmask']) & ~tile_mask
+            cre, cim = float(t['cre']), float(t['cim'])
+            if cim != 0.0:
+                cplx.append((k, zl, zo, cre, cim))
+            elif zl == 0:
+                outside.append((k, zo, cre))
+            elif zo == 0 and bin(zl).count('1') <= 2:
+                lo = (zl & -zl).bit_length() - 1
+                d = zl.bit_length() - 1 - lo
+                for cl in classes:
+                    if cl[0] == cre and cl[1] == d and not (cl[2] >> lo) & 1:
+                        cl[2] |= 1 << lo
+                        cl[3] += 1
+                        break
+                else:
+                    classes.append([cre, d, 1 << lo, 1])
+            else:
+                single.append((k, zl, zo, cre))
+        plan.append((xl, classes, outside, single, cplx))
+        const = sum(c for (_, zo, c) in outside if not zo)
+        ts = [f'(pb{k} ? {-c!r} : {c!r})' for (k, zo, c) in outside if zo]
+        if const or ts:
+            lines.append(f'        const double dg{gi} = {" + ".join(([repr(const)] if const else []) + ts)};')
     lines += ['#pragma unroll 1',
               f'        for (uint32_t j0 = threadIdx.x; j0 < {1 << K}u; j0 += 1024u) {{',
               '            double2 v[4];',
               '#pragma unroll',
               '            for (int r = 0; r < 4; ++r) v[r] = make_double2(0.0, 0.0);']
-    for x, ks in groups.items():
-        xl = _tile_local(x, L, high)
+    for gi, (xl, classes, outside, single, cplx) in enumerate(plan):
         lines.append('            {')
         lines.append('                double2 p[4];')
         lines.append('#pragma unroll')
@@ -273,26 +308,23 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
                      'p[r] = make_double2((double)q.x, (double)q.y); }')
         lines.append('#pragma unroll')
         lines.append('                for (int r = 0; r < 4; ++r) {')
-        lines.append('                    const uint32_t j = j0 + r * 256u;')
-        for k in ks:
-            t = terms[k]
-            zl = _tile_local(int(t['zmask']) & tile_mask, L, high)
-            zo = int(t['zmask']) & ~tile_mask
-            cre, cim = float(t['cre']), float(t['cim'])
-            parts = []
-            if zl:
-                parts.append(f'__popc((j ^ {xl}u) & {zl}u)')
-            if zo:
-                parts.append(f'pb{k}')
+        lines.append(f'                    const uint32_t jx = (j0 + r * 256u) ^ {xl}u;')
+        real = bool(classes or outside or single)
+        if real:
+            lines.append(f'                    double cr = {"dg%d" % gi if outside else "0.0"};')
+            for c, d, m, cnt in classes:
+                pc = f'__popc(jx & {m}u)' if d == 0 else f'__popc((jx ^ (jx >> {d})) & {m}u)'
+                lines.append(f'                    cr = fma({c!r}, (double)({cnt} - 2 * (int){pc}), cr);')
+            for k, zl, zo, c in single:
+                parts = [f'__popc(jx & {zl}u)'] + ([f'pb{k}'] if zo else [])
+                lines.append(f'                    cr += (({" ^ ".join(parts)}) & 1u) ? {-c!r} : {c!r};')
+            lines.append('                    v[r].x = fma(cr, p[r].x, v[r].x); v[r].y = fma(cr, p[r].y, v[r].y);')
+        for k, zl, zo, cre, cim in cplx:
+            parts = ([f'__popc(jx & {zl}u)'] if zl else []) + ([f'pb{k}'] if zo else [])
             sg = f'(({" ^ ".join(parts)}) & 1u)' if parts else None
-            if cim == 0.0:
-                c = f'{cre!r}' if sg is None else f'({sg} ? {-cre!r} : {cre!r})'
-                lines.append(f'                    {{ const double c = {c}; v[r].x = fma(c, p[r].x, v[r].x); '
-                             'v[r].y = fma(c, p[r].y, v[r].y); }')
-            else:
-                c = (f'make_double2({cre!r}, {cim!r})' if sg is None else
-                     f'({sg} ? make_double2({-cre!r}, {-cim!r}) : make_double2({cre!r}, {cim!r}))')
-                lines.append(f'                    v[r] = cfma({c}, p[r], v[r]);')
+            c = (f'make_double2({cre!r}, {cim!r})' if sg is None else
+                 f'({sg} ? make_double2({-cre!r}, {-cim!r}) : make_double2({cre!r}, {cim!r}))')
+            lines.append(f'                    v[r] = cfma({c}, p[r], v[r]);')
         lines.append('                }')
         lines.append('            }')
     lines += ['#pragma unroll',
