@@ -56,6 +56,12 @@ static int tu_status_read_clear() {
     return h;
 }
 static const int tu_status_registered = (register_status_reader(&tu_status_read_clear), 0);
+
+// Pauli passes (k_pauli.cu): at most this many terms per tiled pass, and at
+// most this many CTAs per SM in the grid of any Pauli pass (tiled or direct),
+// so one pass writes at most PAULI_MAX_BLOCKS_PER_SM x SMs partial-sum rows.
+constexpr int PAULI_MAX_TERMS = 512;
+constexpr int PAULI_MAX_BLOCKS_PER_SM = 8;
 #endif  // __CUDACC_RTC__
 
 // ---------------------------------------------------------------- complex

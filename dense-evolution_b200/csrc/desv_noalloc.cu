@@ -11,10 +11,12 @@
 //
 // Limits and rules:
 //  * The array holds DESV_NOALLOC_PARTIAL_ROWS partial rows (2 doubles each,
-//    256 KiB).  One Pauli pass uses at most 8 x (number of SMs) rows (1184 on
-//    a 148-SM B200), so a call may run at most 16384 / (8 x SMs) passes with
-//    terms (13 on a B200); larger calls are rejected with DESV_EINVAL before
-//    any kernel is launched.
+//    256 KiB).  One Pauli pass uses at most PAULI_MAX_BLOCKS_PER_SM (8) x
+//    (number of SMs) rows (1184 on a 148-SM B200; k_pauli.cu clamps every
+//    Pauli grid to that bound), so a call may run at most 16384 / (8 x SMs)
+//    passes with terms (13 on a B200); larger calls, and passes the kernels
+//    would refuse (more than PAULI_MAX_TERMS terms, tiles too wide for the
+//    precision), are rejected with DESV_EINVAL before any kernel is launched.
 //  * Every GPU that loads the library keeps this array until the process exits.
 //  * The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, with that device current).  Make
@@ -77,7 +79,8 @@ extern "C" int desv_pauli_expect_noalloc(const void *psi, int n, int dtype, cons
     if (reinterpret_cast<uintptr_t>(psi) % 16) return fail(DESV_EINVAL, "noalloc Pauli expectation: psi not 16-byte aligned");
     if (npasses < 0 || (npasses && (!passes || !terms))) return fail(DESV_EINVAL, "noalloc Pauli expectation: null pass arrays");
     // validate every pass and the scratch budget before launching anything
-    const size_t rows_per_pass = (size_t)8 * (size_t)sm_count();
+    const size_t rows_per_pass = (size_t)PAULI_MAX_BLOCKS_PER_SM * (size_t)sm_count();
+    const int kmax = dtype == DESV_C64 ? 11 : 10;
     size_t budget = 0;
     for (int p = 0; p < npasses; ++p) {
         const desv_pauli_pass &ps = passes[p];
@@ -86,8 +89,12 @@ extern "C" int desv_pauli_expect_noalloc(const void *psi, int n, int dtype, cons
         if (ps.term_end == ps.term_begin) continue;
         if (ps.tile_bits != 0) {
             TileGeom g;
-            if (ps.tile_bits > n || ps.low_bits < (n < 5 ? n : 5) || !make_geom(g, n, ps.tile_bits, ps.low_bits, ps.high))
+            if (ps.tile_bits > n || ps.tile_bits > kmax || ps.low_bits < (n < 5 ? n : 5) ||
+                !make_geom(g, n, ps.tile_bits, ps.low_bits, ps.high))
                 return fail(DESV_EINVAL, "noalloc Pauli expectation: invalid tile geometry in pass " + std::to_string(p));
+            if (ps.term_end - ps.term_begin > PAULI_MAX_TERMS)
+                return fail(DESV_EINVAL, "noalloc Pauli expectation: more than " + std::to_string(PAULI_MAX_TERMS) +
+                                             " terms in tiled pass " + std::to_string(p));
         }
         budget += rows_per_pass;
     }

@@ -219,8 +219,11 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_vqe(desv_batch_args 
         __syncthreads();
         for (int p = pl.fwd_begin; p < pl.fwd_end; ++p)
             batch_pass<T, false>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc, s_ctab);
-        // 3. lambda = H psi, E = <psi|lambda>
-        double ere = 0;
+        // 3. lambda = H psi, E = <psi|lambda>; complex64 circuits divide E (and
+        // later the gradient) by the FP64 norm <psi|psi>, which is 1 in exact
+        // arithmetic: that removes the first-order effect of the complex64
+        // rounding drift of the norm from both
+        double ere = 0, nrm = 0;
         for (uint64_t i = tid; i < dim; i += blockDim.x) {
             double2 v = make_double2(0.0, 0.0);
             for (int k = pl.term_begin; k < pl.term_end; ++k) {
@@ -235,16 +238,29 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_vqe(desv_batch_args 
             glam[i] = cpx<T>(v.x, v.y);
             const T a = gpsi[i];
             ere += (double)a.x * v.x + (double)a.y * v.y;
+            nrm += (double)a.x * a.x + (double)a.y * a.y;
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) ere += __shfl_xor_sync(0xffffffffu, ere, o);
-        if ((tid & 31) == 0) red[tid >> 5] = ere;
+        for (int o = 16; o > 0; o >>= 1) {
+            ere += __shfl_xor_sync(0xffffffffu, ere, o);
+            nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+        }
+        if ((tid & 31) == 0) {
+            red[tid >> 5] = ere;
+            red[BATCH_NW + (tid >> 5)] = nrm;
+        }
         __threadfence_block();
         __syncthreads();
+        double inv_norm = 1.0;
+        if (sizeof(T) == sizeof(float2)) {
+            double nn = 0;
+            for (int w = 0; w < BATCH_NW; ++w) nn += red[BATCH_NW + w];
+            inv_norm = nn > 0 ? 1.0 / nn : 1.0;
+        }
         if (tid == 0) {
             double e = 0;
             for (int w = 0; w < BATCH_NW; ++w) e += red[w];
-            args.energy[cd.out_index] = e;
+            args.energy[cd.out_index] = e * inv_norm;
         }
         // 4. adjoint sweep over (psi, lambda)
         for (int p = pl.bwd_begin; p < pl.bwd_end; ++p)
@@ -253,7 +269,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_vqe(desv_batch_args 
         for (int q = tid; q < pl.nparams; q += blockDim.x) {
             double s = 0;
             for (int w = 0; w < BATCH_NW; ++w) s += acc[w * BATCH_MAXP + q];
-            args.grad[cd.grad_off + q] = 2.0 * s;
+            args.grad[cd.grad_off + q] = 2.0 * s * inv_norm;
         }
         __syncthreads();
     }

@@ -15,7 +15,9 @@
 namespace desv {
 
 constexpr int PAULI_THREADS = 256;
-constexpr int PAULI_MAX_TERMS = 512;
+// an SM holds at most 2048 threads, so the occupancy of a tiled pass can never
+// exceed the per-SM grid bound the partial-sum buffers are sized for
+static_assert(2048 / PAULI_THREADS <= PAULI_MAX_BLOCKS_PER_SM, "Pauli grid bound");
 
 template <typename T> struct TermTab {
     uint32_t xl[PAULI_MAX_TERMS];
@@ -161,7 +163,7 @@ static int launch_pauli(const T *psi, T *out, const TileGeom &g, const desv_paul
         cudaFuncSetAttribute(k_pauli<T, K, NBUF, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int b = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_pauli<T, K, NBUF, MODE>, PAULI_THREADS, smem);
-        bps[dev & 63] = b > 0 ? b : 1;
+        bps[dev & 63] = b < 1 ? 1 : b > PAULI_MAX_BLOCKS_PER_SM ? PAULI_MAX_BLOCKS_PER_SM : b;
     }
     const uint64_t ntiles = 1ull << (g.n - K);
     const uint64_t cap = (uint64_t)sm_count() * bps[dev & 63];
@@ -232,7 +234,7 @@ int pauli_direct(const void *psi, void *out, int dtype, int mode, int n, const d
                  int want_e, double *part, int *grid_out, cudaStream_t st) {
     const uint64_t dim = 1ull << n;
     uint64_t b = (dim + 255) / 256;
-    const uint64_t cap = (uint64_t)sm_count() * 8;
+    const uint64_t cap = (uint64_t)sm_count() * PAULI_MAX_BLOCKS_PER_SM;
     const int grid = (int)(b < cap ? b : cap);
     *grid_out = grid;
 #define DESV_PD(T, M)                                                                                          \

@@ -20,12 +20,8 @@ from .physics.observables import (pauli_expectation, pauli_sum_expectation, paul
 from .utils.measurement import sample_counts, statevector_fidelity
 from .solvers.autodiff import circuit_to_energy_fn
 from .noise import NoiseModel, NoiseSpec
-
-
-def set_precision(float64: bool = True) -> None:
-    """Kept for API compatibility: precision is chosen per simulator / energy
-    function (``use_float32``), not process-wide."""
-    return None
+from . import config
+from .config import set_precision
 
 
 __all__ = ['DenseSVSimulator', 'QASMParser', 'QASMCircuit', 'QuantumTranspiler', 'CompiledCircuit', 'GATES',
@@ -33,4 +29,4 @@ __all__ = ['DenseSVSimulator', 'QASMParser', 'QASMCircuit', 'QuantumTranspiler',
            'pauli_expectation', 'pauli_sum_expectation', 'pauli_hamiltonian_to_matrix', 'pauli_sum_matvec',
            'multiply_pauli_terms', 'pauli_sum_matvec_jax', 'pauli_sum_expectation_jax', 'PauliSumOperator',
            'sample_counts', 'statevector_fidelity', 'circuit_to_energy_fn', 'set_precision', 'NoiseModel',
-           'NoiseSpec', '__version__']
+           'NoiseSpec', 'config', '__version__']

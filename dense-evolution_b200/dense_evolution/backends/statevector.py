@@ -19,6 +19,7 @@ import numpy as np
 import torch
 
 from .. import _native as N
+from .. import config
 from ..circuits.compiler import CompiledCircuit, QuantumTranspiler
 from ..circuits.gates import GATE_IDS
 
@@ -45,17 +46,18 @@ class DenseSVSimulator:
     Parameters
     ----------
     n_qubits    : number of qubits, 1..34
-    use_float32 : complex64 amplitudes (FP32 gate math, FP64 reductions) instead of complex128
+    use_float32 : complex64 amplitudes (FP32 gate math, FP64 reductions) instead of complex128;
+                  None (the default): complex128 unless ``config.set_precision(False)`` was called
     """
 
     _PLAN_CACHE_SIZE = 32
 
-    def __init__(self, n_qubits: int, use_float32: bool = False):
+    def __init__(self, n_qubits: int, use_float32: Optional[bool] = None):
         if n_qubits < 1 or n_qubits > 34:
             raise ValueError(f"n_qubits must be in [1, 34], got {n_qubits}")
         self.n = int(n_qubits)
         self.dim = 1 << self.n
-        self.use_float32 = bool(use_float32)
+        self.use_float32 = config.default_use_float32(use_float32)
         self.dtype = np.complex64 if self.use_float32 else np.complex128
         self.tdtype = torch.complex64 if self.use_float32 else torch.complex128
         self.device = N.require_cuda()

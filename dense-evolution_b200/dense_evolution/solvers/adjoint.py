@@ -148,6 +148,33 @@ class AdjointProgram:
         self.forward.run(psi, theta=theta)
         return psi
 
+    def norm_ratio(self, psi: torch.Tensor, stato_zero=None) -> float:
+        """<psi0|psi0> / <psi|psi> in FP64 for a complex64 program, 1 otherwise.
+
+        The circuit is unitary, so in exact arithmetic the ratio is 1; in
+        complex64 the rounding of the gate passes drifts the norm by about
+        1e-7.  Multiplying E = <psi|H|psi> and its gradient by the ratio
+        removes the first-order effect of that drift on both (the reference's
+        energy is the unnormalised <psi|H|psi> of a state whose norm is the
+        initial state's, so the ratio keeps unnormalised initial states
+        exact too)."""
+        if self.dtype != torch.complex64:
+            return 1.0
+        if stato_zero is None:
+            n0 = 1.0
+        elif isinstance(stato_zero, torch.Tensor):
+            n0 = float(torch.linalg.vector_norm(stato_zero.detach().to(torch.complex128)).item()) ** 2
+        else:
+            a = np.asarray(stato_zero).astype(np.complex128).reshape(-1)
+            n0 = float(np.vdot(a, a).real)
+        out = torch.empty(2, dtype=torch.float64, device=psi.device)
+        sc = N.scratch(self.n, psi.device)
+        N.check(N.lib().desv_norm2(ctypes.c_void_p(psi.data_ptr()), self.n, N.dtype_code(psi),
+                                   ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(sc.data_ptr()), sc.numel() * 8,
+                                   ctypes.c_void_p(N.stream_ptr())), 'norm')
+        nn = float(out[0].item())
+        return n0 / nn if nn > 0 else 1.0
+
     def hamiltonian(self, h):
         """('pauli', PauliPlan) or ('dense', tensor)."""
         if isinstance(h, PauliSumOperator):
@@ -267,8 +294,11 @@ class AdjointProgram:
         psi = self.forward_state(th, stato_zero)
         if noise is not None:
             psi, _ = self.apply_noise(psi, noise)
+            ratio = 1.0        # the noisy state is normalised in FP64 already
+        else:
+            ratio = self.norm_ratio(psi, stato_zero)
         _, e = self.apply_h(h, psi, need_lambda=False)
-        return torch.tensor(e, dtype=torch.float64), psi
+        return torch.tensor(e * ratio, dtype=torch.float64), psi
 
     def apply_noise(self, psi: torch.Tensor, noise):
         """(noisy normalised copy of psi, Pauli errors or None for damping channels)."""
@@ -294,8 +324,9 @@ class AdjointProgram:
         """(E, dE/dtheta as NumPy float64, psi) without autograd bookkeeping."""
         th = _as_theta(theta)
         psi = self.forward_state(th, stato_zero)
+        ratio = self.norm_ratio(psi, stato_zero)
         lam, e = self.apply_h(h, psi, need_lambda=True)
-        return e, self.gradient(th, psi, lam), psi
+        return e * ratio, self.gradient(th, psi, lam) * ratio, psi
 
     def parameter_shift_grad(self, theta, h, stato_zero=None) -> np.ndarray:
         """Parameter-shift gradient on the same kernels: two forward runs + <H> per
@@ -308,7 +339,7 @@ class AdjointProgram:
 
         def f(t):
             psi = self.forward_state(t, stato_zero)
-            return self.apply_h(h, psi, need_lambda=False)[1]
+            return self.apply_h(h, psi, need_lambda=False)[1] * self.norm_ratio(psi, stato_zero)
 
         grad = np.zeros(self.nparams)
         for k in range(self.nparams):
@@ -353,8 +384,11 @@ class _EnergyFunction(torch.autograd.Function):
         th = _as_theta(theta_t)
         psi = prog.forward_state(th, stato_zero)
         ctx.differentiable = True
+        ctx.ratio = 1.0
         if noise is None:
             lam, e = prog.apply_h(h, psi, need_lambda=True)
+            ctx.ratio = prog.norm_ratio(psi, stato_zero)
+            e *= ctx.ratio
             box['sv'] = psi
         else:
             noisy, errs = prog.apply_noise(psi, noise)
@@ -375,6 +409,6 @@ class _EnergyFunction(torch.autograd.Function):
         if not ctx.differentiable:
             raise NotImplementedError('the gradient through an amplitude-damping channel (amplitude_damping, '
                                       'combined) is not supported; the Pauli channels are')
-        grad = ctx.prog.gradient(ctx.th, ctx.psi, ctx.lam)
+        grad = ctx.prog.gradient(ctx.th, ctx.psi, ctx.lam) * ctx.ratio
         gt = torch.from_numpy(grad).to(device=ctx.tdev, dtype=ctx.tdtype)
         return g * gt, None, None, None, None, None

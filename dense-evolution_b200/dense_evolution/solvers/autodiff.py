@@ -16,6 +16,7 @@ import numpy as np
 import torch
 
 from .. import _native as N
+from .. import config
 from ..circuits.compiler import QuantumTranspiler
 from ..circuits.gates import GATE_IDS
 from ..circuits.parser import QASMCircuit
@@ -68,13 +69,15 @@ def build_template(circuit, n_qubits: int):
     return rows, slots, n_params
 
 
-def circuit_to_energy_fn(circuit, n_qubits: int, use_float32: bool = False) -> Tuple[Callable, int]:
+def circuit_to_energy_fn(circuit, n_qubits: int, use_float32: Optional[bool] = None) -> Tuple[Callable, int]:
     """(energy_fn, n_params) for a QASMCircuit (or gate-tuple list).
 
     ``use_float32`` runs the state in complex64 with FP64 reductions; the
-    default is complex128 like the reference."""
+    default (None) is complex128 like the reference, or complex64 after an
+    explicit ``config.set_precision(False)``."""
     rows, slots, n_params = build_template(circuit, n_qubits)
-    prog = adjoint.AdjointProgram(rows, slots, n_qubits, torch.complex64 if use_float32 else torch.complex128)
+    f32 = config.default_use_float32(use_float32)
+    prog = adjoint.AdjointProgram(rows, slots, n_qubits, torch.complex64 if f32 else torch.complex128)
 
     def energy_fn(theta, h_matrix, stato_zero=None, noise=None):
         return prog.energy(theta, h_matrix, stato_zero, noise)

@@ -290,9 +290,6 @@ int desv_jit_free(void *handle);
  * compiled tile_bits); mats_dev is the same matrix pool desv_apply_passes reads. */
 int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pass, const void *mats_dev,
                   void *stream);
-/* One adjoint backward pass (the work of desv_adjoint_passes for that pass,
- * including the gradient reduction into grad_dev[map_dev[map_begin + p]]);
- * ops_dev is the whole op array (the compiled source indexes it absolutely). */
 /* desv_pauli_expect (matvec == 0) or desv_pauli_matvec (matvec != 0) with the
  * tiled passes that have a specialised kernel (handles[p] != NULL, loaded with
  * kind 2 + the mode the pass runs in: 0 <H>; 1 the first H psi pass, 2 the
@@ -300,6 +297,9 @@ int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pas
 int desv_jit_pauli(void *const *handles, const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes,
                    int npasses, const desv_pauli_term *terms, double *expect, void *scratch, size_t scratch_bytes,
                    int matvec, void *stream);
+/* One adjoint backward pass (the work of desv_adjoint_passes for that pass,
+ * including the gradient reduction into grad_dev[map_dev[map_begin + p]]);
+ * ops_dev is the whole op array (the compiled source indexes it absolutely). */
 int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int dtype, const desv_adj_pass *pass,
                      const desv_op *ops_dev, const void *mats_dev, const int32_t *map_dev, double *grad_dev,
                      void *scratch, size_t scratch_bytes, void *stream);

@@ -2,7 +2,7 @@
 
 Run here (the reference checkout is not present on a GPU box):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference PATH_OF_REFERENCE_CHECKOUT
 
 It imports the reference's own hot-path modules -- gates.py, compiler.py,
 parser.py, backends/statevector.py, physics/observables.py,
@@ -105,7 +105,7 @@ def tfim_terms(n, h=1.0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', required=True, help='path of the reference checkout')
     ap.add_argument('--skip-config1', action='store_true')
     args = ap.parse_args()
     ref = load_reference(args.reference)

@@ -2,7 +2,7 @@
 
 Run here (the reference checkout is not present on a GPU box):
 
-    python tests/golden/make_noise_golden.py [--reference /root/reference]
+    python tests/golden/make_noise_golden.py --reference PATH_OF_REFERENCE_CHECKOUT
 
 It imports the reference's ``dense_evolution/noise/kraus_channels.py`` and
 ``dense_evolution/noise/kraus/*.py`` unmodified.  JAX is absent from this image,
@@ -50,7 +50,7 @@ def load_noise(root: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', required=True, help='path of the reference checkout')
     args = ap.parse_args()
     NoiseModel = load_noise(args.reference)
     rng0 = np.random.default_rng(77)

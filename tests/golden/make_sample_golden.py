@@ -4,7 +4,7 @@ stubs of make_golden.py.  Each case records a seeded state, the shot count, the
 generator seed and the reference's counts dict; the states are rebuilt from
 ``sample_states()`` (seeded NumPy draws), so only the counts are stored.
 
-    python tests/golden/make_sample_golden.py [--reference /root/reference]
+    python tests/golden/make_sample_golden.py --reference PATH_OF_REFERENCE_CHECKOUT
 """
 from __future__ import annotations
 
@@ -39,7 +39,7 @@ def sample_states():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', required=True, help='path of the reference checkout')
     args = ap.parse_args()
     ref = load_reference(args.reference)
     cases = []

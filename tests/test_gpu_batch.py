@@ -22,16 +22,17 @@ def test_batch_matches_single_circuit_adjoint(f32):
     for i, (circ, n, terms) in enumerate(items):
         fn, npar = de.circuit_to_energy_fn(circ, n, use_float32=f32)
         e1, g1, _ = fn.program.value_and_grad(thetas[i], terms)
-        tol = 1e-5 if f32 else 1e-10
-        assert e[i] == pytest.approx(e1, abs=tol)
-        assert np.allclose(g[i], g1, atol=tol)
+        # energies to the complex64 bar |dE| <= 1e-6 (both paths divide by the
+        # FP64 norm); gradients to 1e-5
+        assert e[i] == pytest.approx(e1, abs=1e-6 if f32 else 1e-10)
+        assert np.allclose(g[i], g1, atol=1e-5 if f32 else 1e-10)
     # oracle for the two smallest
     for i in (0, 5):
         circ, n, terms = items[i]
         rows, _ = O.energy_template([{'name': c[0], 'qubits': [q for q in c[1:] if isinstance(q, int)]}
                                      for c in circ], n)
         e_ref, _ = O.energy(thetas[i], rows, n, terms)
-        assert e[i] == pytest.approx(e_ref, abs=1e-5 if f32 else 1e-10)
+        assert e[i] == pytest.approx(e_ref, abs=1e-6 if f32 else 1e-10)
         fd = O.fd_gradient(thetas[i], rows, n, terms, h=1e-5, indices=[0, 7, 20])
         assert np.allclose(g[i][[0, 7, 20]], fd, atol=1e-4 if f32 else 1e-7)
     from dense_evolution import _native as N

@@ -49,7 +49,7 @@ def test_random_hamiltonians_vs_oracle(n):
     # complex64 device state: FP32 amplitude products, FP64 accumulation
     t = torch.from_numpy(psi.astype(np.complex64)).cuda()
     e32 = de.pauli_sum_expectation(t, terms)
-    assert e32 == pytest.approx(O.pauli_sum_expectation(psi.astype(np.complex64).astype(complex), terms), abs=1e-5)
+    assert e32 == pytest.approx(O.pauli_sum_expectation(psi.astype(np.complex64).astype(complex), terms), abs=1e-6)
     op = de.PauliSumOperator(terms, n)
     assert np.allclose((op @ t).cpu().numpy(), O.pauli_sum_matvec(psi, terms), atol=1e-5)
 

@@ -59,3 +59,17 @@ def test_iteration_and_validate():
     assert QASMParser().validate(QASMCircuit(1, 0, [])) == (False, 'No gate operations found in circuit.')
     bad = QASMCircuit(1, 0, [{'type': 'gate', 'name': 'x', 'qubits': [3], 'params': []}])
     assert QASMParser().validate(bad)[0] is False
+
+
+def test_package_transpiler_matches_reference_output():
+    """QuantumTranspiler.transpile of the package (not only the oracle) against
+    the reference's own transpile output on the same input: same gate tuples in
+    the same order, so the theta-slot order of run_batch_jit / energy_fn and
+    the global phases agree with the reference's."""
+    import json
+    import os
+    from dense_evolution.circuits.compiler import QuantumTranspiler
+    with open(os.path.join(os.path.dirname(__file__), 'golden', 'golden_transpile.json')) as f:
+        t = json.load(f)
+    out = QuantumTranspiler.transpile([tuple(c) for c in t['in']])
+    assert [list(c) for c in out] == t['out']

@@ -76,3 +76,57 @@ def test_noalloc_rejects_more_passes_than_the_fixed_array_holds():
                                       ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(0))
     assert r == N.DESV_EINVAL
     assert 'partial rows' in N.last_error()
+
+
+def test_noalloc_with_no_terms_writes_zero():
+    """A call whose passes all have empty term ranges launches no pass and
+    must still overwrite the caller's output with (0, 0)."""
+    import torch
+    from dense_evolution import _native as N
+    from dense_evolution.physics.observables import PauliPlan
+    lib = N.lib()
+    n = 12
+    t = torch.zeros(1 << n, dtype=torch.complex64, device='cuda')
+    t[0] = 1
+    plan = PauliPlan([(1.0, {0: 'X'})], n, tile_bits=10)
+    empty = plan.passes.copy()
+    empty['term_end'] = empty['term_begin']
+    out = torch.full((2,), float('nan'), dtype=torch.float64, device='cuda')
+    N.check(lib.desv_pauli_expect_noalloc(ctypes.c_void_p(t.data_ptr()), n, N.DESV_C64,
+                                          ctypes.c_void_p(empty.ctypes.data), len(empty),
+                                          ctypes.c_void_p(plan.terms_dev(t.device).data_ptr()),
+                                          ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(0)), 'noalloc expect')
+    assert out.cpu().tolist() == [0.0, 0.0]
+
+
+def test_noalloc_on_a_user_stream():
+    """The call is ordered on the caller's stream: run it on a freshly created
+    torch stream right after the state is written there, and compare with the
+    allocating entry point on the default stream."""
+    import torch
+    from dense_evolution import _native as N
+    from dense_evolution.physics.observables import PauliPlan
+    lib = N.lib()
+    n = 16
+    rng = np.random.default_rng(11)
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi /= np.linalg.norm(psi)
+    plan = PauliPlan(_terms(n), n, tile_bits=11)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        t = torch.from_numpy(psi).to('cuda').to(torch.complex64)
+        terms_dev = plan.terms_dev(t.device)
+        out = torch.full((2,), float('nan'), dtype=torch.float64, device='cuda')
+        N.check(lib.desv_pauli_expect_noalloc(ctypes.c_void_p(t.data_ptr()), n, N.DESV_C64,
+                                              ctypes.c_void_p(plan.passes.ctypes.data), len(plan.passes),
+                                              ctypes.c_void_p(terms_dev.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                              ctypes.c_void_p(s.cuda_stream)), 'noalloc expect')
+    s.synchronize()
+    ref = torch.zeros(2, dtype=torch.float64, device='cuda')
+    sc = torch.empty(int(lib.desv_scratch_bytes(n, N.DESV_C64)) // 8 + 1, dtype=torch.float64, device='cuda')
+    N.check(lib.desv_pauli_expect(ctypes.c_void_p(t.data_ptr()), n, N.DESV_C64, ctypes.c_void_p(plan.passes.ctypes.data),
+                                  len(plan.passes), ctypes.c_void_p(terms_dev.data_ptr()), ctypes.c_void_p(ref.data_ptr()),
+                                  ctypes.c_void_p(sc.data_ptr()), sc.numel() * 8,
+                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), 'expect')
+    assert np.allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=0, atol=1e-12)
+    N.device_status()
