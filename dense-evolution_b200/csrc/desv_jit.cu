@@ -90,7 +90,18 @@ struct JitKernel {
     CUdeviceptr_t status = 0;  // the module's desv_rtc_status word
     int kind = 0, K = 0, nbuf = 0, dtype = 0, blocks_per_sm = 1;
     size_t smem = 0;  // forward: the launch's dynamic shared memory; adjoint: without the accumulators
+    int threads = 0;      // rotation passes: threads per CTA
+    int param_floats = 0; // rotation passes: floats in the by-value parameter block
 };
+
+// kind of a rotation-pass kernel (desv_rot_load)
+constexpr int JIT_KIND_ROT = 5;
+constexpr int ROT_REG_BITS = 5;     // register slots per stage (rot_pass.cuh: 32 amplitudes per thread)
+constexpr int ROT_NBUF = 3;         // ring slots
+constexpr int ROT_MAX_PARAM_FLOATS = 7936;  // by-value parameter block <= 31 KiB (limit 32764 bytes)
+
+// padded stage layout of a 2^K tile: one spare amplitude after every 16
+static size_t rot_slot_elems(int K) { return ((size_t)1 << K) + ((size_t)1 << (K - 4)); }
 
 // Adjoint passes: at most this many gradient slots per pass and partial-sum
 // rows (the bounds of the interpreter k_adjoint_pass).
@@ -142,28 +153,10 @@ int jit_pauli_launch(void *handle, const void *psi, void *out, int dtype, int mo
     return DESV_OK;
 }
 
-}  // namespace desv
 
-using namespace desv;
-
-extern "C" int desv_jit_available(char *why, size_t len) {
-    const JitApi &a = api();
-    if (why && len) {
-        std::strncpy(why, a.ok ? "" : a.why.c_str(), len - 1);
-        why[len - 1] = 0;
-    }
-    return a.ok ? 1 : 0;
-}
-
-extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind, int tile_bits, int nbuf,
-                             int dtype, int device, void **handle, char *log, size_t loglen) {
-    if (!src || !include_dir || !handle) return fail(DESV_EINVAL, "jit load: null argument");
-    *handle = nullptr;
-    if (dtype != DESV_C64 && dtype != DESV_C128) return fail(DESV_EINVAL, "jit load: bad dtype");
-    if (kind < 0 || kind > 4)
-        return fail(DESV_EINVAL, "jit load: kind must be 0 (pass), 1 (adjoint) or 2..4 (Pauli pass, mode 0..2)");
-    if (tile_bits < 9 || tile_bits > (dtype == DESV_C64 ? 13 : 12) || nbuf < 2 || nbuf > 4)
-        return fail(DESV_EINVAL, "jit load: bad tile shape");
+// Compile CUDA source for sm_100a with NVRTC; the log (if any) goes to log.
+static int nvrtc_compile(const char *src, const char *include_dir, std::vector<char> &cubin, char *log,
+                         size_t loglen) {
     const JitApi &a = api();
     if (!a.ok) return fail(DESV_EUNSUPPORTED, "jit: " + a.why);
     nvrtcProgram_t prog = nullptr;
@@ -195,10 +188,38 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind,
     }
     size_t cs = 0;
     a.GetCUBINSize(prog, &cs);
-    std::vector<char> cubin(cs);
+    cubin.resize(cs);
     a.GetCUBIN(prog, cubin.data());
     a.DestroyProgram(&prog);
+    return DESV_OK;
+}
 
+}  // namespace desv
+
+using namespace desv;
+
+extern "C" int desv_jit_available(char *why, size_t len) {
+    const JitApi &a = api();
+    if (why && len) {
+        std::strncpy(why, a.ok ? "" : a.why.c_str(), len - 1);
+        why[len - 1] = 0;
+    }
+    return a.ok ? 1 : 0;
+}
+
+extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind, int tile_bits, int nbuf,
+                             int dtype, int device, void **handle, char *log, size_t loglen) {
+    if (!src || !include_dir || !handle) return fail(DESV_EINVAL, "jit load: null argument");
+    *handle = nullptr;
+    if (dtype != DESV_C64 && dtype != DESV_C128) return fail(DESV_EINVAL, "jit load: bad dtype");
+    if (kind < 0 || kind > 4)
+        return fail(DESV_EINVAL, "jit load: kind must be 0 (pass), 1 (adjoint) or 2..4 (Pauli pass, mode 0..2)");
+    if (tile_bits < 9 || tile_bits > (dtype == DESV_C64 ? 13 : 12) || nbuf < 2 || nbuf > 4)
+        return fail(DESV_EINVAL, "jit load: bad tile shape");
+    std::vector<char> cubin;
+    int r = nvrtc_compile(src, include_dir, cubin, log, loglen);
+    if (r) return r;
+    const JitApi &a = api();
     auto *k = new JitKernel();
     k->kind = kind;
     k->K = tile_bits;
@@ -311,5 +332,77 @@ extern "C" int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int d
     if (api().LaunchKernel(k->fn, grid, 1, 1, 1u << (k->K - 4), 1, 1, (unsigned)smem, stream, args, nullptr) != 0)
         return fail(DESV_ECUDA, "jit adjoint: launch failed");
     if (np > 0) return grad_reduce(part, (int)grid, np, map_dev + ps->map_begin, grad_dev, static_cast<cudaStream_t>(stream));
+    return DESV_OK;
+}
+
+extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile_bits, int param_floats, int device,
+                             void **handle, char *log, size_t loglen) {
+    if (!src || !include_dirs || !handle) return fail(DESV_EINVAL, "rotation pass load: null argument");
+    *handle = nullptr;
+    if (tile_bits < ROT_REG_BITS + 4 || tile_bits > 12)
+        return fail(DESV_EINVAL, "rotation pass load: tile_bits must be in [9, 12]");
+    if (param_floats < 1 || param_floats > ROT_MAX_PARAM_FLOATS)
+        return fail(DESV_EINVAL, "rotation pass load: parameter block size out of range");
+    std::vector<char> cubin;
+    int r = nvrtc_compile(src, include_dirs, cubin, log, loglen);
+    if (r) return r;
+    const JitApi &a = api();
+    auto *k = new JitKernel();
+    k->kind = JIT_KIND_ROT;
+    k->K = tile_bits;
+    k->nbuf = ROT_NBUF;
+    k->dtype = DESV_C64;
+    k->threads = 1 << (tile_bits - ROT_REG_BITS);
+    k->param_floats = param_floats;
+    k->smem = PIPE_HDR_BYTES + (size_t)ROT_NBUF * rot_slot_elems(tile_bits) * sizeof(float2);
+    size_t ssz = 0;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete k;
+        return check_launch("rotation pass load: cudaSetDevice");
+    }
+    if (a.ModuleLoadData(&k->mod, cubin.data()) != 0 || a.ModuleGetFunction(&k->fn, k->mod, "desv_rot_kernel") != 0 ||
+        a.ModuleGetGlobal(&k->status, &ssz, k->mod, "desv_rtc_status") != 0) {
+        if (k->mod) a.ModuleUnload(k->mod);
+        delete k;
+        return fail(DESV_ECUDA, "rotation pass load: loading the compiled pass failed (no current CUDA context?)");
+    }
+    if (a.FuncSetAttribute(k->fn, 8, (int)k->smem) != 0) {
+        a.ModuleUnload(k->mod);
+        delete k;
+        return fail(DESV_ECUDA, "rotation pass load: shared-memory attribute refused");
+    }
+    int b = 0;
+    a.OccupancyMaxActiveBlocksPerMultiprocessor(&b, k->fn, k->threads, k->smem);
+    k->blocks_per_sm = b > 0 ? b : 1;
+    {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        g_kernels.push_back(k);
+    }
+    *handle = k;
+    return DESV_OK;
+}
+
+extern "C" int desv_rot_pass(void *handle, void *sv, int n, const desv_pass *ps, const float *params,
+                             int param_floats, void *stream) {
+    if (!handle || !sv || !ps || !params) return fail(DESV_EINVAL, "rotation pass: null argument");
+    auto *k = static_cast<JitKernel *>(handle);
+    if (k->kind != JIT_KIND_ROT) return fail(DESV_EINVAL, "rotation pass: the kernel is not a rotation pass");
+    if (param_floats != k->param_floats)
+        return fail(DESV_EINVAL, "rotation pass: parameter block size differs from the compiled kernel's");
+    if (n < k->K || n > 34) return fail(DESV_EINVAL, "rotation pass: n out of range");
+    if (reinterpret_cast<uintptr_t>(sv) % 16) return fail(DESV_EINVAL, "rotation pass: state not 16-byte aligned");
+    TileGeom g;
+    if (ps->tile_bits != k->K || ps->low_bits < 5 || ps->tile_bits - ps->low_bits > 8 ||
+        !make_geom(g, n, ps->tile_bits, ps->low_bits, ps->high))
+        return fail(DESV_EINVAL, "rotation pass: tile geometry does not match the compiled kernel");
+    const uint64_t ntiles = 1ull << (n - k->K);
+    const uint64_t cap = (uint64_t)sm_count() * k->blocks_per_sm;
+    const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
+    // the parameter block is the kernel's third (by-value) argument: the
+    // launch copies it, so the caller's buffer is free again on return
+    void *args[] = {&sv, &g, const_cast<float *>(params)};
+    if (api().LaunchKernel(k->fn, grid, 1, 1, (unsigned)k->threads, 1, 1, (unsigned)k->smem, stream, args, nullptr) !=
+        0)
+        return fail(DESV_ECUDA, "rotation pass: launch failed");
     return DESV_OK;
 }

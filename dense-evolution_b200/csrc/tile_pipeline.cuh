@@ -81,15 +81,17 @@ template <typename T, int NARR> struct PipeArrays {
 };
 
 // Run `body(smem_slot_arrays, tile_base, tile_id)` over every tile.  Returns
-// false (after draining in-flight copies) if a bounded wait gave up.
+// false (after draining in-flight copies) if a bounded wait gave up.  SLOT is
+// the ring slot size in elements per array: the tile's 2^K by default, more
+// when the body re-lays the tile out in a padded layout inside its slot.
 //
 // Every thread issues the bulk copies of the 2^L-runs c = threadIdx.x,
 // threadIdx.x + blockDim.x, ...; each warp announces its own byte count on the
 // slot's mbarrier (initialised with one arrival per warp), so no warp
 // serialises the copy issue of the whole tile.
-template <typename T, int K, int NBUF, int NARR, class Body>
+template <typename T, int K, int NBUF, int NARR, uint32_t SLOT = (1u << K), class Body>
 __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body &body, unsigned char *smem) {
-    constexpr uint32_t TILE = 1u << K;
+    static_assert(SLOT >= (1u << K), "a ring slot holds at least one tile");
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     uint64_t *ctab = reinterpret_cast<uint64_t *>(smem + 128);
     T *bufs = reinterpret_cast<T *>(smem + PIPE_HDR_BYTES);
@@ -133,7 +135,7 @@ __device__ bool run_tiles(const TileGeom &g, const PipeArrays<T, NARR> &A, Body 
     uint64_t cbase = base0;  // base of the next tile to process
     auto next_base = [&](uint64_t b) { return ((b | ~rmask) + tstride) & rmask; };
 
-    auto slot_ptr = [&](uint32_t slot, int a) { return bufs + (size_t)(slot * NARR + a) * TILE; };
+    auto slot_ptr = [&](uint32_t slot, int a) { return bufs + (size_t)(slot * NARR + a) * SLOT; };
     auto issue_load = [&](uint32_t i) {
         const uint32_t slot = i % NBUF;
         const uint64_t base = lbase;

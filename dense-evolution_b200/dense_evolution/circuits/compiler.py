@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from .. import _native as N
-from . import fusion, jit
+from . import fusion, jit, rotation
 
 
 class QuantumTranspiler:
@@ -84,22 +84,61 @@ def default_tile_bits(n: int, dtype: torch.dtype) -> int:
 
 
 class CompiledCircuit:
-    """A circuit lowered, fused and packed for one qubit count and precision."""
+    """A circuit lowered, fused and packed for one qubit count and precision.
+
+    complex64 circuits of >= rotation.MIN_QUBITS qubits run as rotation passes
+    (``rotation.py``: real rotations in tangent form, diagonal groups, every
+    tile bit a register slot); the general fused passes (``fusion.py``) are
+    built lazily, for everything else."""
 
     def __init__(self, target: Sequence[tuple], n: int, dtype: torch.dtype = torch.complex128,
                  slots: Optional[Sequence[int]] = None, tile_bits: Optional[int] = None, merge_1q: bool = True):
         self.n = int(n)
         self.dtype = dtype
         self.tile_bits = tile_bits or default_tile_bits(self.n, dtype)
-        self.ir, self.fops, self.packed = fusion.build(target, self.n, self.tile_bits, slots, merge_1q)
+        self._target, self._slots, self._merge_1q = list(target), slots, merge_1q
+        self.ir = fusion.lower(self._target, self.n, slots)
+        self._fops = self._packed = None
+        self._built = False
+        self._rot = None
         self._dev_cache = None
         self._dev_theta_key = None
         self._host_arrays = None
         self._jit_kernels = None
 
+    def _build(self):
+        if not self._built:
+            _, self._fops, self._packed = fusion.build(self._target, self.n, self.tile_bits, self._slots,
+                                                       self._merge_1q)
+            self._built = True
+
+    @property
+    def fops(self):
+        self._build()
+        return self._fops
+
+    @property
+    def packed(self):
+        self._build()
+        return self._packed
+
+    @property
+    def rotation(self):
+        """The bound rotation program of this circuit, or None when the general
+        fused passes run it (complex128, fewer than rotation.MIN_QUBITS qubits,
+        DESV_ROT=0, no NVRTC, or a gate the rotation path does not lower)."""
+        if self._rot is None:
+            self._rot = False
+            if self.dtype == torch.complex64 and self.n >= fusion.MIN_FUSED_QUBITS and \
+                    rotation.enabled(self.n, True):
+                self._rot = rotation.program_for(self._target, self.n, min(12, self.n), self._slots) or False
+        return self._rot or None
+
     # ------------------------------------------------------------ stats
     @property
     def npasses(self) -> int:
+        if self.rotation is not None:
+            return len(self.rotation.plan.passes)
         return len(self.packed.passes) if self.packed is not None else len(self.fops)
 
     @property
@@ -138,6 +177,11 @@ class CompiledCircuit:
         lib = N.lib()
         st = ctypes.c_void_p(N.stream_ptr(stream))
         code = N.dtype_code(sv)
+        rot = self.rotation
+        if rot is not None:
+            dev = sv.device.index if sv.device.index is not None else torch.cuda.current_device()
+            rot.run(sv.data_ptr(), dev, st.value or 0, theta)
+            return sv
         if self.packed is None:
             for op in self.fops:
                 apply_fop(sv, self.n, op, theta, st)

@@ -297,6 +297,19 @@ int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pas
 int desv_jit_pauli(void *const *handles, const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes,
                    int npasses, const desv_pauli_term *terms, double *expect, void *scratch, size_t scratch_bytes,
                    int matvec, void *stream);
+/* Rotation passes (complex64 forward passes of circuits lowered to real
+ * rotations and diagonals; replaces the per-gate scan step of
+ * circuits/compiler.py:136-355 like desv_jit_pass).  desv_rot_load compiles
+ * one pass's generated source (entry point desv_rot_kernel, 2^(tile_bits-5)
+ * threads, a by-value parameter block of param_floats floats) for sm_100a;
+ * desv_rot_pass runs it over the 2^n complex64 state sv with the pass's tile
+ * geometry (tile_bits, low_bits, high[]; op_begin / op_end are not used) and
+ * the per-call values params[0..param_floats) (host memory, copied by the
+ * launch). */
+int desv_rot_load(const char *src, const char *include_dirs, int tile_bits, int param_floats, int device,
+                  void **handle, char *log, size_t loglen);
+int desv_rot_pass(void *handle, void *sv, int n, const desv_pass *pass, const float *params, int param_floats,
+                  void *stream);
 /* One adjoint backward pass (the work of desv_adjoint_passes for that pass,
  * including the gradient reduction into grad_dev[map_dev[map_begin + p]]);
  * ops_dev is the whole op array (the compiled source indexes it absolutely). */
