@@ -189,6 +189,47 @@ def cpu_baseline(n=N_QUBITS, layers=LAYERS, gates=2, npasses=None):
             'est_circuit_s': est}
 
 
+def config1_cpu(layers=20, n=20):
+    """Config 1 whole on the host cores: the 20-qubit, 20-layer brick circuit in
+    complex128 through the NumPy oracle (the reference's eager CPU path
+    restated), state and <Z_i>; seconds per circuit (one run after a warm-up of
+    the first layer)."""
+    from oracle import sv_oracle as O
+    from dense_evolution.workloads import brick_u3_circuit
+    circ = brick_u3_circuit(n, layers, SEED)
+    O.run_circuit(O.zero_state(n), n, circ[:n])
+    c0, t0 = time.process_time(), time.perf_counter()
+    sv = O.run_circuit(O.zero_state(n), n, circ)
+    p = np.abs(sv) ** 2
+    z = [float(np.sum(p.reshape(1 << q, 2, -1)[:, 0].sum() - p.reshape(1 << q, 2, -1)[:, 1].sum()))
+         for q in range(n)]
+    dt = time.perf_counter() - t0
+    return {'workload': f'{n}-qubit complex128 brick circuit, {layers} layers (config 1), state + <Z_i>',
+            'seconds_per_circuit': dt, 'cores': round((time.process_time() - c0) / dt, 2), 'kind': 'port',
+            'z0': z[0]}
+
+
+def config1_gpu(layers=20, n=20, reps=3):
+    """Config 1 whole on the GPU through the public API (DenseSVSimulator,
+    complex128): seconds per circuit, state resident, <Z_i> read back."""
+    import torch
+    import dense_evolution as de
+    from dense_evolution.workloads import brick_u3_circuit
+    circ = brick_u3_circuit(n, layers, SEED)
+    sim = de.DenseSVSimulator(n)
+    sim.run_circuit(circ)
+    z = sim.expectation_z()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        sim.set_initial_state(None)
+        sim.run_circuit(circ)
+        z = sim.expectation_z()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / reps
+    return {'seconds_per_circuit': dt, 'z0': float(z[0])}
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -202,7 +243,10 @@ def run_reference(args):
             cores.append(r['cores'])
         last = r
     v = float(np.mean(vals))
+    c1 = config1_cpu()
     line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'GB/s', 'n_gpus': args.gpus,
+            'value_kind': 'estimate: a one-gate sample of the 30-qubit circuit per step, extrapolated to all gates',
+            'config1_whole_circuit': c1,
             'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'complex64', 'data': 'synthetic',
             'config': {'workload': f'{args.qubits}-qubit complex64 random circuit, {args.layers} layers of U3 on every '
@@ -262,21 +306,33 @@ def run_headline(args, ws, local):
     circ = brick_u3_circuit(n, layers, SEED)
     t_c = time.perf_counter()
     plan = CompiledCircuit(de.QuantumTranspiler.transpile(circ), n, torch.complex64)
+    rot = plan.rotation
     compile_s = time.perf_counter() - t_c
-    npasses = len(plan.packed.passes)
+    npasses = plan.npasses
     sv = torch.empty(1 << n, dtype=torch.complex64, device=dev)
     lib = N.lib()
     N.check(lib.desv_init_basis(ctypes.c_void_p(sv.data_ptr()), n, N.DESV_C64, 0, ctypes.c_void_p(st.cuda_stream)),
             'init')
-    ops_t, mats_t = plan.device_arrays(dev)
-    passes = plan.device_passes
     pass_bytes = 2 * (1 << n) * 8
-    specialised = jit.enabled(n)
+    specialised = rot is None and jit.enabled(n)
     t_c = time.perf_counter()
-    kernels = plan.specialised_kernels(dev) if specialised else None
+    if rot is not None:
+        kernels = rot.prog.compile(torch.cuda.current_device())
+        blocks = rot.blocks()
+        rows = rot.prog.rows
+    else:
+        ops_t, mats_t = plan.device_arrays(dev)
+        passes = plan.device_passes
+        kernels = plan.specialised_kernels(dev) if specialised else None
     jit_compile_s = time.perf_counter() - t_c
 
     def one_pass(i):
+        if rot is not None:
+            N.check(lib.desv_rot_pass(kernels[i].handle, ctypes.c_void_p(sv.data_ptr()), n,
+                                      ctypes.c_void_p(rows.ctypes.data + i * rows.itemsize),
+                                      blocks[i].ctypes.data_as(ctypes.c_void_p), len(blocks[i]),
+                                      ctypes.c_void_p(st.cuda_stream)), 'rotation pass')
+            return
         if specialised:
             jit.run_passes(kernels[i:i + 1], sv.data_ptr(), n, N.DESV_C64, passes[i:i + 1], ops_t.data_ptr(),
                            mats_t.data_ptr(), st.cuda_stream)
@@ -329,12 +385,22 @@ def run_headline(args, ws, local):
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)
-            ops_i, mats_i = plan_i.device_arrays(dev)
-            h2d = int(ops_i.numel() + mats_i.numel() * 4)
+            if plan_i.rotation is not None:
+                h2d = int(sum(b.nbytes for b in plan_i.rotation.blocks()))
+            else:
+                ops_i, mats_i = plan_i.device_arrays(dev)
+                h2d = int(ops_i.numel() + mats_i.numel() * 4)
         sim._plans.clear()
     e2e_step = _max_over_ranks(float(np.mean(e2e_times)), ws)
     e2e_value = ws * npasses * pass_bytes / e2e_step / 1e9
-    del sv, sim, ops_t, mats_t
+    steps_ms = per_pass.reshape(args.steps, npasses).mean(axis=0)
+    if rot is not None:
+        st_ = rot.plan.stats()['per_pass']
+        table = [{'pass': i, 'rotations': r, 'stages': g_, 'diag_groups': d, 'ms': round(float(steps_ms[i]), 4)}
+                 for i, (r, g_, d) in enumerate(st_)]
+    else:
+        table = [{'pass': i, 'ms': round(float(steps_ms[i]), 4)} for i in range(npasses)]
+    del sv, sim
     torch.cuda.empty_cache()
     return {
         'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,
@@ -349,7 +415,8 @@ def run_headline(args, ws, local):
         'ms_per_layer': ms_step / layers, 'compile_s': compile_s, 'jit_compile_s': jit_compile_s,
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_src,
-                     'kernel': ('desv_jit_kernel (plan-specialised fused pass, NVRTC sm_100a)' if specialised
+                     'kernel': ('desv_rot_kernel (rotation pass, NVRTC sm_100a)' if rot is not None else
+                                'desv_jit_kernel (plan-specialised fused pass, NVRTC sm_100a)' if specialised
                                 else f'k_fused_pass<float2,{plan.tile_bits},3>'),
                      'algorithmic_bytes_per_launch': pass_bytes,
                      'avg_launch_ms': avg_pass_ms, 'min_launch_ms': float(per_pass.min()),
@@ -360,6 +427,7 @@ def run_headline(args, ws, local):
                         'expectation_z()'},
         'gpu_launches': args.steps * npasses,
         'clocks': clk.summary(),
+        'pass_table': table,
     }
 
 
@@ -387,6 +455,13 @@ def run_ours(args):
     npasses = line.get('passes_per_step')
     line['cpu_baseline'] = cpu_baseline(args.qubits, args.layers, gates=2, npasses=npasses) \
         if (rank == 0 and ws == 1 and not args.skip_cpu and not args.skip_headline) else None
+    if line['cpu_baseline'] is not None:
+        line['cpu_baseline']['value_kind'] = 'estimate (two-gate sample of the 30-qubit circuit, extrapolated)'
+        c1 = config1_cpu()
+        g1 = config1_gpu()
+        line['config1'] = {'cpu': c1, 'gpu_seconds_per_circuit': g1['seconds_per_circuit'],
+                           'speedup_gpu_over_cpu': c1['seconds_per_circuit'] / g1['seconds_per_circuit'],
+                           'z0_cpu': c1['z0'], 'z0_gpu': g1['z0']}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -403,16 +478,29 @@ def run_vqe(args):
     fn, npar = de.circuit_to_energy_fn(hea_circuit(n, layers), n, use_float32=True)
     prog = fn.program
     op = de.PauliSumOperator(tfim_terms(n), n)
-    theta = np.random.default_rng(SEED).uniform(-np.pi, np.pi, npar)
+    rng = np.random.default_rng(SEED)
+    theta = rng.uniform(-np.pi, np.pi, npar)
     for _ in range(max(1, args.warmup)):
-        prog.value_and_grad(theta, op)
+        prog.value_and_grad(rng.uniform(-np.pi, np.pi, npar), op)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    # a VQE loop: a fresh theta every gradient (host materialisation and upload
+    # of the forward and backward values inside the timed region)
     reps = max(3, args.steps)
-    for _ in range(reps):
-        e, g, _ = prog.value_and_grad(theta, op)
+    thetas = [rng.uniform(-np.pi, np.pi, npar) for _ in range(reps)]
+    t0 = time.perf_counter()
+    for th in thetas:
+        e, g, _ = prog.value_and_grad(th, op)
     torch.cuda.synchronize()
     adj_s = (time.perf_counter() - t0) / reps
+    # the same gradient with theta repeated: the values are cached, so this is
+    # (close to) the device time of the gradient's kernels
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        prog.value_and_grad(thetas[-1], op)
+    torch.cuda.synchronize()
+    cached_s = (time.perf_counter() - t0) / reps
+    theta = thetas[-1]
+    e, g, _ = prog.value_and_grad(theta, op)
     pauli = pauli_roofline(prog, theta, n)
     # parameter shift on the same kernels: 2 * npar forward runs + <H>
     if args.vqe_no_shift:
@@ -425,9 +513,12 @@ def run_vqe(args):
     ps_s = time.perf_counter() - t0
     return {'workload': f'{n}-qubit complex64 HEA, {layers} layers (RY,RZ + CX ladder), {npar} parameters, '
                         f'TFIM open chain', 'energy': e, 'adjoint_grads_per_s': 1.0 / adj_s,
+            'theta': 'fresh theta every timed gradient (a VQE loop); parameter shift changes theta on every run',
+            'adjoint_ms_repeated_theta': cached_s * 1e3,
+            'host_ms_per_gradient': (adj_s - cached_s) * 1e3,
             'parameter_shift_grads_per_s': 1.0 / ps_s, 'adjoint_over_parameter_shift': ps_s / adj_s,
             'max_abs_grad_diff_adjoint_vs_shift': float(np.max(np.abs(g - ps))),
-            'forward_passes': int(len(prog.forward.packed.passes)),
+            'forward_passes': int(prog.forward.npasses),
             'backward_passes': int(len(prog.back.passes)), 'adjoint_ms': adj_s * 1e3, 'shift_ms': ps_s * 1e3,
             'pauli': pauli}
 
@@ -538,7 +629,7 @@ def run_large(args, n=32, n_ref=30, layers=4):
     torch.cuda.empty_cache()
     out.update({'energy': e, 'grad_norm': float(np.linalg.norm(g)), 'seconds_per_gradient': dt,
                 'grads_per_s': 1.0 / dt, 'params': npar, 'peak_hbm_gib': peak,
-                'forward_passes': len(fn.program.forward.packed.passes), 'backward_passes': len(fn.program.back.passes)})
+                'forward_passes': fn.program.forward.npasses, 'backward_passes': len(fn.program.back.passes)})
     # accuracy of complex64 against complex128, same structure at 30 qubits
     th = np.random.default_rng(SEED).uniform(-np.pi, np.pi, 2 * n_ref * layers)
     r = {}

@@ -25,8 +25,8 @@ typedef void *CUfunction_t;
 typedef unsigned long long CUdeviceptr_t;
 
 struct JitApi {
-    bool tried = false, ok = false;
-    std::string why;
+    bool tried = false, ok = false, rtc_ok = false;  // ok: NVRTC and the driver; rtc_ok: NVRTC alone
+    std::string why, rtc_why;
     nvrtcResult_t (*CreateProgram)(nvrtcProgram_t *, const char *, const char *, int, const char *const *,
                                    const char *const *);
     nvrtcResult_t (*CompileProgram)(nvrtcProgram_t, int, const char *const *);
@@ -60,19 +60,25 @@ static const JitApi &api() {
     g_api.tried = true;
     void *rtc = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
     if (!rtc) rtc = dlopen("libnvrtc.so", RTLD_NOW | RTLD_LOCAL);
+    if (!rtc) {
+        g_api.why = g_api.rtc_why = "libnvrtc not found";
+        return g_api;
+    }
+    std::string &rw = g_api.rtc_why;
+    g_api.rtc_ok = sym(rtc, "nvrtcCreateProgram", g_api.CreateProgram, rw) &&
+                   sym(rtc, "nvrtcCompileProgram", g_api.CompileProgram, rw) &&
+                   sym(rtc, "nvrtcGetProgramLogSize", g_api.GetProgramLogSize, rw) &&
+                   sym(rtc, "nvrtcGetProgramLog", g_api.GetProgramLog, rw) &&
+                   sym(rtc, "nvrtcGetCUBINSize", g_api.GetCUBINSize, rw) &&
+                   sym(rtc, "nvrtcGetCUBIN", g_api.GetCUBIN, rw) &&
+                   sym(rtc, "nvrtcDestroyProgram", g_api.DestroyProgram, rw);
     void *drv = dlopen("libcuda.so.1", RTLD_NOW | RTLD_LOCAL);
-    if (!rtc || !drv) {
-        g_api.why = !rtc ? "libnvrtc not found" : "libcuda.so.1 not found";
+    if (!g_api.rtc_ok || !drv) {
+        g_api.why = !g_api.rtc_ok ? g_api.rtc_why : "libcuda.so.1 not found";
         return g_api;
     }
     std::string &w = g_api.why;
-    g_api.ok = sym(rtc, "nvrtcCreateProgram", g_api.CreateProgram, w) &&
-               sym(rtc, "nvrtcCompileProgram", g_api.CompileProgram, w) &&
-               sym(rtc, "nvrtcGetProgramLogSize", g_api.GetProgramLogSize, w) &&
-               sym(rtc, "nvrtcGetProgramLog", g_api.GetProgramLog, w) &&
-               sym(rtc, "nvrtcGetCUBINSize", g_api.GetCUBINSize, w) && sym(rtc, "nvrtcGetCUBIN", g_api.GetCUBIN, w) &&
-               sym(rtc, "nvrtcDestroyProgram", g_api.DestroyProgram, w) &&
-               sym(drv, "cuModuleLoadData", g_api.ModuleLoadData, w) &&
+    g_api.ok = sym(drv, "cuModuleLoadData", g_api.ModuleLoadData, w) &&
                sym(drv, "cuModuleUnload", g_api.ModuleUnload, w) &&
                sym(drv, "cuModuleGetFunction", g_api.ModuleGetFunction, w) &&
                sym(drv, "cuModuleGetGlobal_v2", g_api.ModuleGetGlobal, w) &&
@@ -158,7 +164,7 @@ int jit_pauli_launch(void *handle, const void *psi, void *out, int dtype, int mo
 static int nvrtc_compile(const char *src, const char *include_dir, std::vector<char> &cubin, char *log,
                          size_t loglen) {
     const JitApi &a = api();
-    if (!a.ok) return fail(DESV_EUNSUPPORTED, "jit: " + a.why);
+    if (!a.rtc_ok) return fail(DESV_EUNSUPPORTED, "jit: " + a.rtc_why);
     nvrtcProgram_t prog = nullptr;
     if (a.CreateProgram(&prog, src, "desv_pass.cu", 0, nullptr, nullptr) != 0)
         return fail(DESV_ECUDA, "nvrtcCreateProgram failed");
@@ -216,6 +222,7 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind,
         return fail(DESV_EINVAL, "jit load: kind must be 0 (pass), 1 (adjoint) or 2..4 (Pauli pass, mode 0..2)");
     if (tile_bits < 9 || tile_bits > (dtype == DESV_C64 ? 13 : 12) || nbuf < 2 || nbuf > 4)
         return fail(DESV_EINVAL, "jit load: bad tile shape");
+    if (!api().ok) return fail(DESV_EUNSUPPORTED, "jit: " + api().why);
     std::vector<char> cubin;
     int r = nvrtc_compile(src, include_dir, cubin, log, loglen);
     if (r) return r;
@@ -343,6 +350,7 @@ extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile
         return fail(DESV_EINVAL, "rotation pass load: tile_bits must be in [9, 12]");
     if (param_floats < 1 || param_floats > ROT_MAX_PARAM_FLOATS)
         return fail(DESV_EINVAL, "rotation pass load: parameter block size out of range");
+    if (!api().ok) return fail(DESV_EUNSUPPORTED, "jit: " + api().why);
     std::vector<char> cubin;
     int r = nvrtc_compile(src, include_dirs, cubin, log, loglen);
     if (r) return r;
@@ -405,4 +413,11 @@ extern "C" int desv_rot_pass(void *handle, void *sv, int n, const desv_pass *ps,
         0)
         return fail(DESV_ECUDA, "rotation pass: launch failed");
     return DESV_OK;
+}
+
+extern "C" int desv_jit_compile_check(const char *src, const char *include_dirs, char *log, size_t loglen) {
+    if (!src || !include_dirs) return fail(DESV_EINVAL, "jit compile check: null argument");
+    if (!api().rtc_ok) return fail(DESV_EUNSUPPORTED, "jit: " + api().rtc_why);
+    std::vector<char> cubin;
+    return nvrtc_compile(src, include_dirs, cubin, log, loglen);
 }

@@ -17,6 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, '_lib', 'libdesv.so')
 
 DESV_C64, DESV_C128 = 0, 1
+DESV_ELEM_F64, DESV_ELEM_C64, DESV_ELEM_C128 = 0, 1, 2
 DESV_OK, DESV_EINVAL, DESV_ENOMEM, DESV_ETIMEOUT, DESV_ECUDA, DESV_EUNSUPPORTED = 0, -1, -2, -3, -4, -5
 OP_STAGE, OP_M1, OP_M2, OP_DIAG, OP_GRAD = 0, 1, 2, 3, 4
 F_REAL, F_DIAG, F_PHASE1, F_ANTI, F_SIGN, F_PARAM = 1, 2, 4, 8, 16, 32
@@ -74,6 +75,8 @@ _SIGS = {
     'desv_jit_pass': ([_vp, _vp, _i, _i, _vp, _vp, _vp], _i),
     'desv_rot_load': ([ctypes.c_char_p, ctypes.c_char_p, _i, _i, _i, ctypes.POINTER(_vp), ctypes.c_char_p, _sz], _i),
     'desv_rot_pass': ([_vp, _vp, _i, _vp, _vp, _i, _vp], _i),
+    'desv_bit_reverse': ([_vp, _vp, _i, _i, _vp], _i),
+    'desv_jit_compile_check': ([ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _sz], _i),
 }
 OPTIONAL = set()
 

@@ -333,6 +333,18 @@ class DenseSVSimulator:
             probs /= total
         return probs
 
+    def probabilities_tensor(self) -> torch.Tensor:
+        """get_probabilities() as an FP64 CUDA tensor (|a|^2, clipped to [0, 1],
+        renormalised), left on the device."""
+        out = torch.empty(self.dim, dtype=torch.float64, device=self.device)
+        N.check(N.lib().desv_probabilities(self._ptr(), self.n, self._code(), ctypes.c_void_p(out.data_ptr()),
+                                           self._st()), 'probabilities')
+        out.clamp_(0.0, 1.0)
+        total = float(out.sum().item())
+        if total > 1e-12:
+            out /= total
+        return out
+
     def get_statevector(self) -> np.ndarray:
         return self.sv.detach().cpu().numpy().astype(self.dtype, copy=False)
 

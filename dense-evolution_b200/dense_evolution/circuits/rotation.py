@@ -829,15 +829,21 @@ def pass_source(plan: 'RotationPlan', pidx: int, nbuf: int = 3) -> str:
     NA = 1 << RB
     nthreads = 1 << (K - RB)
     gmap = [b if b < L else high[b - L] for b in range(K)]
-    lines = ['#include "rot_pass.cuh"', 'using namespace desv;',
+    check = os.environ.get('DESV_ROT_CHECK', '') == '1'
+    lines = ([f'#define DESV_ROT_CHECK 1', f'#define ROT_SLOT_ELEMS {slot_elems(K)}u'] if check else []) + \
+            ['#include "rot_pass.cuh"', 'using namespace desv;',
              f'struct RotParams {{ float v[{ps.n_floats}]; }};',
              f'extern "C" __global__ void __launch_bounds__({nthreads}, 2)',
-             'desv_rot_kernel(float2 *__restrict__ sv, TileGeom g, const __grid_constant__ RotParams P) {',
+             'desv_rot_kernel(float2 *__restrict__ sv, const TileGeom g, const RotParams P) {',
              '    extern __shared__ __align__(128) unsigned char smem[];',
              '    const uint32_t t = threadIdx.x;',
-             '    const float *pv = P.v;',
-             '    auto body = [&](float2 *const *sp, uint64_t tb, uint64_t) {',
-             '        float2 *s = sp[0];',
+             f'    RotRing<{K}, {nbuf}, {slot_elems(K)}u> ring;',
+             '    ring.init(g, sv, smem);',
+             '    uint32_t i = 0;',
+             '    for (; i < ring.cnt; ++i) {',
+             '        uint64_t tb;',
+             '        if (!ring.begin(i, tb)) break;',
+             '        float2 *s = ring.slot(i);',
              f'        float2 a[{NA}];']
     nst = len(ps.stages)
     for si, st in enumerate(ps.stages):
@@ -853,16 +859,16 @@ def pass_source(plan: 'RotationPlan', pidx: int, nbuf: int = 3) -> str:
         lines.append(f'        {{  // stage {si}: register slots at tile bits {regs}')
         lines.append(f'            const uint32_t lb = {loc};')
         if first:
-            lines += [f'            a[{j}] = s[lb + {offs[j]}u];' for j in range(NA)]
+            lines += [f'            ROT_SLD(a[{j}], s, lb + {offs[j]}u);' for j in range(NA)]
         else:
             lines.append('            const uint32_t pb = lb + (lb >> 4);')
-            lines += [f'            a[{j}] = s[pb + {padded(offs[j])}u];' for j in range(NA)]
+            lines += [f'            ROT_SLD(a[{j}], s, pb + {padded(offs[j])}u);' for j in range(NA)]
         if need_gi:
             lines.append(f'            const uint64_t gi = tb | {glob};')
         for kind, x in st.items:
             if kind == 'rot':
                 pi, slot, off = x
-                lines.append(f'            rot<{slot}>(a, pv + {off});')
+                lines.append(f'            rot<{slot}>(a, pv[{off}], pv[{off + 1}], pv[{off + 2}], pv[{off + 3}]);')
             else:
                 lines += ['            ' + ln for ln in _group_code(x)]
         if last:
@@ -872,23 +878,21 @@ def pass_source(plan: 'RotationPlan', pidx: int, nbuf: int = 3) -> str:
                     lines.append(f'            scale_all_c(a, pv[{o}], pv[{o + 1}]);')
                 else:
                     lines.append(f'            scale_all(a, pv[{o}]);')
-            lines += [f'            sv[gi + {goffs[j]}ull] = a[{j}];' for j in range(NA)]
+            lines += [f'            ROT_GST(sv, gi + {goffs[j]}ull, a[{j}]);' for j in range(NA)]
         else:
             if first:
                 lines.append('            __syncthreads();  // every natural-layout read is done')
                 lines.append('            const uint32_t pb = lb + (lb >> 4);')
-            lines += [f'            s[pb + {padded(offs[j])}u] = a[{j}];' for j in range(NA)]
+            lines += [f'            ROT_SST(s, pb + {padded(offs[j])}u, a[{j}]);' for j in range(NA)]
             lines.append('            fence_proxy_async_smem();')
             lines.append('            __syncthreads();')
         lines.append('        }')
-    lines += ['    };',
-              '    PipeArrays<float2, 1> A;',
-              '    A.ptr[0] = sv;',
-              '    A.load[0] = true;',
-              '    A.store[0] = false;',
-              f'    run_tiles<float2, {K}, {nbuf}, 1, {slot_elems(K)}u>(g, A, body, smem);',
+    lines += ['        __syncthreads();  // the slot is free for the load NBUF-1 tiles ahead',
+              '    }',
+              '    if (i < ring.cnt) ring.drain(i);',
               '}', '']
-    return '\n'.join(lines)
+    src = '\n'.join(lines)
+    return src.replace('pv[', 'P.v[')
 
 
 def _group_code(g: Group) -> List[str]:

@@ -286,6 +286,9 @@ int desv_jit_available(char *why, size_t len);
 int desv_jit_load(const char *src, const char *include_dirs, int kind, int tile_bits, int nbuf, int dtype,
                   int device, void **handle, char *log, size_t loglen);
 int desv_jit_free(void *handle);
+/* Compile a pass source with NVRTC for sm_100a without loading it (needs no
+ * GPU): DESV_OK or DESV_EINVAL with the compiler log in log. */
+int desv_jit_compile_check(const char *src, const char *include_dirs, char *log, size_t loglen);
 /* Run the loaded kernel over one pass (its tile geometry must match the
  * compiled tile_bits); mats_dev is the same matrix pool desv_apply_passes reads. */
 int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pass, const void *mats_dev,
@@ -297,6 +300,16 @@ int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pas
 int desv_jit_pauli(void *const *handles, const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes,
                    int npasses, const desv_pauli_term *terms, double *expect, void *scratch, size_t scratch_bytes,
                    int matvec, void *stream);
+/* ---- interop (replaces _to_qiskit_bit_order, interop/qiskit_pennylane.py:115-136) */
+/* element kinds of desv_bit_reverse */
+#define DESV_ELEM_F64 0  /* probabilities */
+#define DESV_ELEM_C64 1  /* complex64 amplitudes */
+#define DESV_ELEM_C128 2 /* complex128 amplitudes */
+/* out[rev_n(i)] = in[i] for i < 2^n: MSB-first (this engine, the reference)
+ * <-> little-endian (Qiskit, PennyLane) index order.  Out of place; both
+ * arrays on the device. */
+int desv_bit_reverse(const void *in, void *out, int n, int elem, void *stream);
+
 /* Rotation passes (complex64 forward passes of circuits lowered to real
  * rotations and diagonals; replaces the per-gate scan step of
  * circuits/compiler.py:136-355 like desv_jit_pass).  desv_rot_load compiles

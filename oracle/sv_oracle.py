@@ -472,3 +472,19 @@ def sample_counts(statevector, n_shots, rng=None):
     idx = rng.choice(dim, size=n_shots, p=probs / total)
     v, f = np.unique(idx, return_counts=True)
     return {format(int(a), f'0{n}b'): int(b) for a, b in zip(v, f)}
+
+
+# ---------------------------------------------------------------------------
+# interop bit order (interop/qiskit_pennylane.py:115-136, tests/_helpers.py:14-25)
+# ---------------------------------------------------------------------------
+
+def bit_reversal_perm(n_qubits: int) -> List[int]:
+    """MSB-first <-> little-endian index permutation, as the reference's test
+    helper writes it: the index's n-bit binary string reversed."""
+    return [int(format(i, f'0{n_qubits}b')[::-1], 2) for i in range(2 ** n_qubits)] if n_qubits else [0]
+
+
+def to_qiskit_bit_order(probs: np.ndarray, n_qubits: int) -> np.ndarray:
+    """probs reindexed into Qiskit's little-endian order (the reference's
+    _to_qiskit_bit_order: probs[perm] with perm the bit reversal)."""
+    return np.asarray(probs)[bit_reversal_perm(n_qubits)]

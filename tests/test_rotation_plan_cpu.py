@@ -160,3 +160,26 @@ def test_generated_sources_compile(tmp_path):
                             '-o', str(tmp_path / f'p{i}.o'), '-I', os.path.join(root, 'dense-evolution_b200', 'csrc'),
                             '-I', os.path.join(root, 'include')], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr[-3000:]
+
+
+def test_generated_sources_compile_with_nvrtc():
+    """The kernels are compiled at run time by NVRTC, whose headers differ from
+    nvcc's: compile the generated sources (normal and DESV_ROT_CHECK builds)
+    through libdesv's compile-only entry point, which needs no GPU."""
+    import ctypes
+    from dense_evolution import _native as N
+    from dense_evolution.circuits import jit
+    n = 21
+    plan = R.RotationPlan(QuantumTranspiler.transpile(_mixed_circuit(n, 150, 8)), n, 12, max_rots=24)
+    for check in ('0', '1'):
+        os.environ['DESV_ROT_CHECK'] = check
+        try:
+            for i in (0, len(plan.passes) - 1):
+                log = ctypes.create_string_buffer(16384)
+                r = N.lib().desv_jit_compile_check(R.pass_source(plan, i).encode(), jit.INCLUDE_PATH.encode(), log,
+                                                   16384)
+                if r == N.DESV_EUNSUPPORTED:
+                    pytest.skip('NVRTC not available: ' + N.last_error())
+                assert r == 0, log.value.decode()[-3000:]
+        finally:
+            os.environ.pop('DESV_ROT_CHECK', None)
