@@ -67,3 +67,33 @@ extern "C" int desv_bit_reverse(const void *in, void *out, int n, int elem, void
         default: return fail(DESV_EINVAL, "bit reversal: element kind must be DESV_ELEM_F64, _C64 or _C128");
     }
 }
+
+// ---------------------------------------------------------------------------
+// Block swap of two device arrays: a[i] <-> b[i] for i < count (16-byte
+// vectors; one read and one write of each element).  The split-state runner
+// exchanges the upper half of one chunk with the lower half of its partner
+// chunk with it when a chunk-select qubit trades places with the top local
+// qubit (both halves are contiguous).
+__global__ void __launch_bounds__(256) k_swap16(uint4 *a, uint4 *b, uint64_t count) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint4 x = a[i], y = b[i];
+        a[i] = y;
+        b[i] = x;
+    }
+}
+
+extern "C" int desv_swap_blocks(void *a, void *b, size_t bytes, void *stream) {
+    if (!a || !b) return fail(DESV_EINVAL, "block swap: null array");
+    if (bytes == 0) return DESV_OK;
+    if ((reinterpret_cast<uint64_t>(a) | reinterpret_cast<uint64_t>(b) | (uint64_t)bytes) & 15u)
+        return fail(DESV_EINVAL, "block swap: arrays and size must be multiples of 16 bytes");
+    const uint64_t a0 = reinterpret_cast<uint64_t>(a), b0 = reinterpret_cast<uint64_t>(b);
+    if (a0 < b0 + bytes && b0 < a0 + bytes) return fail(DESV_EINVAL, "block swap: the arrays overlap");
+    const uint64_t count = bytes / 16;
+    const uint64_t blocks = (count + 255) / 256;
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    k_swap16<<<(unsigned)(blocks < cap ? blocks : cap), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<uint4 *>(a), static_cast<uint4 *>(b), count);
+    return check_launch("block swap");
+}

@@ -77,6 +77,7 @@ _SIGS = {
     'desv_rot_pass': ([_vp, _vp, _i, _vp, _vp, _i, _vp], _i),
     'desv_bit_reverse': ([_vp, _vp, _i, _i, _vp], _i),
     'desv_jit_compile_check': ([ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _sz], _i),
+    'desv_swap_blocks': ([_vp, _vp, _sz, _vp], _i),
 }
 OPTIONAL = set()
 

@@ -310,6 +310,14 @@ int desv_jit_pauli(void *const *handles, const void *psi, void *out, int n, int 
  * arrays on the device. */
 int desv_bit_reverse(const void *in, void *out, int n, int elem, void *stream);
 
+/* ---- split states (replaces the chunk-select exchange of
+ *      backends/chunk/kernels.py:300-330, a ppermute per gate) -------------- */
+/* a[i] <-> b[i] over `bytes` bytes (multiples of 16, non-overlapping device
+ * arrays): the exchange of a chunk's upper half with its partner chunk's
+ * lower half when a chunk-select qubit trades places with the top local
+ * qubit. */
+int desv_swap_blocks(void *a, void *b, size_t bytes, void *stream);
+
 /* Rotation passes (complex64 forward passes of circuits lowered to real
  * rotations and diagonals; replaces the per-gate scan step of
  * circuits/compiler.py:136-355 like desv_jit_pass).  desv_rot_load compiles
