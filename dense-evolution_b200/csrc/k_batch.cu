@@ -207,18 +207,30 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_vqe(desv_batch_args 
         const uint64_t dim = 1ull << n;
         const bool resident = n <= BATCH_K;
         const double *theta = args.theta + cd.theta_off;
+        // forward only (run_batch_jit rows): no terms and no adjoint passes; the
+        // final state goes to the caller's output row (streamed states are
+        // evolved there in place)
+        const bool fwd_only = pl.term_end == pl.term_begin && pl.bwd_end == pl.bwd_begin && args.states != nullptr &&
+                              cd.state_off >= 0;
+        T *out_row = fwd_only ? static_cast<T *>(args.states) + cd.state_off : nullptr;
         // 1. matrices of this circuit
         for (int r = pl.rec_begin + tid; r < pl.rec_end; r += blockDim.x)
             run_recipe<T>(args.recipes[r], theta, static_cast<const T *>(args.cpool), pool);
         for (int i = tid; i < BATCH_NW * BATCH_MAXP; i += blockDim.x) acc[i] = 0.0;
         // 2. |0...0> and the forward passes
-        T *gpsi = resident ? sA : wpsi;
+        T *gpsi = resident ? sA : (fwd_only ? out_row : wpsi);
         T *glam = resident ? sB : wlam;
         for (uint64_t i = tid; i < dim; i += blockDim.x) gpsi[i] = cpx<T>(i == 0 ? 1.0 : 0.0, 0.0);
         __threadfence_block();
         __syncthreads();
         for (int p = pl.fwd_begin; p < pl.fwd_end; ++p)
             batch_pass<T, false>(gpsi, glam, sA, sB, resident, args.passes[p], n, args.ops, pool, acc, s_ctab);
+        if (fwd_only) {
+            if (resident)
+                for (uint64_t i = tid; i < dim; i += blockDim.x) out_row[i] = sA[i];
+            __syncthreads();
+            continue;
+        }
         // 3. lambda = H psi, E = <psi|lambda>; complex64 circuits divide E (and
         // later the gradient) by the FP64 norm <psi|psi>, which is 1 in exact
         // arithmetic: that removes the first-order effect of the complex64

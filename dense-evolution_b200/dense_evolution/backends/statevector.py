@@ -306,6 +306,20 @@ class DenseSVSimulator:
                     norm_target.append((name, cmd[1], 0.0))
             else:
                 norm_target.append(cmd)
+        if self.n >= 9 and pb.shape[0] > 0:
+            # every row in one persistent launch (the batched kernel's forward-only
+            # mode); structures it cannot build fall back to one plan run per row
+            key = ('batch_forward', _freeze(norm_target), tuple(slots), self.n, self.use_float32)
+            bf = self._plans.get(key)
+            if bf is None:
+                from ..batch import BatchForward
+                try:
+                    bf = BatchForward(norm_target, slots, self.n, self.tdtype)
+                except (RuntimeError, ValueError, KeyError):
+                    bf = False
+                self._plans[key] = bf
+            if bf:
+                return bf.run(pb)
         plan = CompiledCircuit(norm_target, self.n, self.tdtype, slots=slots)
         out = torch.empty((pb.shape[0], self.dim), dtype=self.tdtype, device=self.device)
         for r in range(pb.shape[0]):

@@ -42,8 +42,8 @@ RECIPE_DTYPE = np.dtype([('off', '<u4'), ('param', '<i4'), ('kind', '<u2'), ('co
 PLAN_DTYPE = np.dtype([(k, '<i4') for k in ('n', 'fwd_begin', 'fwd_end', 'bwd_begin', 'bwd_end', 'rec_begin',
                                             'rec_end', 'term_begin', 'term_end', 'nparams', 'pool_len', 'pad')])
 CIRC_DTYPE = np.dtype([('plan', '<i4'), ('out_index', '<i4'), ('theta_off', '<i8'), ('coef_off', '<i8'),
-                       ('grad_off', '<i8')])
-assert RECIPE_DTYPE.itemsize == 16 and PLAN_DTYPE.itemsize == 48 and CIRC_DTYPE.itemsize == 32
+                       ('grad_off', '<i8'), ('state_off', '<i8')])
+assert RECIPE_DTYPE.itemsize == 16 and PLAN_DTYPE.itemsize == 48 and CIRC_DTYPE.itemsize == 40
 
 
 class BatchArgs(ctypes.Structure):
@@ -53,7 +53,7 @@ class BatchArgs(ctypes.Structure):
                 ('recipes', ctypes.c_void_p), ('cpool', ctypes.c_void_p), ('theta', ctypes.c_void_p),
                 ('coef', ctypes.c_void_p), ('terms', ctypes.c_void_p), ('energy', ctypes.c_void_p),
                 ('grad', ctypes.c_void_p), ('workspace', ctypes.c_void_p), ('ws_amps', ctypes.c_uint64),
-                ('pool_ws', ctypes.c_void_p), ('pool_stride_bytes', ctypes.c_uint64)]
+                ('pool_ws', ctypes.c_void_p), ('pool_stride_bytes', ctypes.c_uint64), ('states', ctypes.c_void_p)]
 
 
 def _term_structure(terms, n):
@@ -82,7 +82,7 @@ def _term_structure(terms, n):
 class _Plan:
     """Forward + adjoint passes and matrix recipes of one circuit structure."""
 
-    def __init__(self, rows, slots, n, term_struct, dtype, tile_bits=None):
+    def __init__(self, rows, slots, n, term_struct, dtype, tile_bits=None, forward_only: bool = False):
         if n < fusion.MIN_FUSED_QUBITS:
             raise ValueError(f'batched VQE needs at least {fusion.MIN_FUSED_QUBITS} qubits per circuit')
         self.n = n
@@ -94,9 +94,9 @@ class _Plan:
         ir = fusion.lower(rows, n, slots)
         fops = fusion.fuse_1q(ir, merge=False)
         self.fwd = fusion.Packed(n, fops, fusion.schedule(fops, n, K))
-        bops = adjoint.backward_ops(ir)
-        self.bwd = fusion.Packed(n, bops, adjoint._split_params(fusion.schedule(bops, n, K), bops, 4096),
-                                 adjoint=True)
+        bops = [] if forward_only else adjoint.backward_ops(ir)
+        self.bwd = fusion.Packed(n, bops, adjoint._split_params(fusion.schedule(bops, n, K), bops, 4096)
+                                 if bops else [], adjoint=True)
         for p in list(self.fwd.passes) + list(self.bwd.passes):
             if int(p['tile_bits']) != (n if n <= RESIDENT_BITS else K):
                 raise RuntimeError('batched plan: unexpected tile geometry')
@@ -250,7 +250,7 @@ class BatchVQE:
             coefs[coef_off[i]:coef_off[i] + len(coef)] = coef
         for k, i in enumerate(order):
             pi = self.circ[i][0]
-            crow[k] = (pi, i, theta_off[i], coef_off[i], theta_off[i])
+            crow[k] = (pi, i, theta_off[i], coef_off[i], theta_off[i], -1)
         self.d_circ = up(crow)
         self.d_coef = torch.from_numpy(coefs).to(dev)
         self.d_theta = torch.zeros(max(t, 1), dtype=torch.float64, device=dev)
@@ -369,3 +369,69 @@ def gather_results(indices: Sequence[int], energies: Sequence[float], grads: Seq
     if any(g is None for g in g_all):
         raise RuntimeError('gather_results: some circuits were run by no rank')
     return e_all, g_all
+
+
+class BatchForward:
+    """run_batch_jit's rows in ONE persistent launch: one circuit structure, one
+    parameter row per circuit, every row's final state written to its row of a
+    (B, 2^n) tensor.  The batched VQE kernel runs in its forward-only mode:
+    each row's matrices are built from its theta on the device, states of
+    <= 12 qubits stay in shared memory until written out, wider ones are
+    evolved in place in their output rows.  Replaces the reference's vmap
+    over one circuit shape (backends/statevector.py:496-584)."""
+
+    def __init__(self, rows, slots, n: int, dtype=torch.complex64, tile_bits=None):
+        self.dtype = dtype
+        self.device = N.require_cuda()
+        self.n = int(n)
+        if tile_bits is None:
+            from . import autotune
+            tile_bits = autotune.batch_tile_bits(dtype)
+        self.plan = _Plan(rows, slots, self.n, (), dtype, int(tile_bits), forward_only=True)
+        self.nparams = self.plan.nparams
+
+    def run(self, parameter_batch: np.ndarray) -> torch.Tensor:
+        pb = np.asarray(parameter_batch, dtype=np.float64)
+        B = pb.shape[0]
+        p = self.plan
+        dev = self.device
+        rdt = np.float32 if self.dtype == torch.complex64 else np.float64
+        cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
+
+        def up(a):
+            return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+
+        prow = np.zeros(1, PLAN_DTYPE)
+        prow['n'] = p.n
+        prow['fwd_begin'], prow['fwd_end'] = 0, len(p.fwd.passes)
+        prow['bwd_begin'] = prow['bwd_end'] = len(p.fwd.passes)
+        prow['rec_begin'], prow['rec_end'] = 0, len(p.recipes)
+        prow['nparams'], prow['pool_len'] = p.nparams, p.pool_len
+        npar = max(p.nparams, 1)
+        theta = np.zeros((B, npar))
+        theta[:, :pb.shape[1]] = pb
+        crow = np.zeros(B, CIRC_DTYPE)
+        crow['plan'] = 0
+        crow['out_index'] = np.arange(B)
+        crow['theta_off'] = np.arange(B) * npar
+        crow['state_off'] = np.arange(B, dtype=np.int64) << p.n
+        out = torch.empty((B, 1 << p.n), dtype=self.dtype, device=dev)
+        bufs = dict(plans=up(prow), passes=up(p.fwd.passes), ops=up(p.fwd.ops), recipes=up(p.recipes),
+                    cpool=torch.from_numpy(p.cpool.astype(cdt).view(rdt).copy()).to(dev),
+                    theta=torch.from_numpy(theta.reshape(-1)).to(dev), circuits=up(crow),
+                    coef=torch.zeros(1, dtype=torch.float64, device=dev),
+                    terms=up(np.zeros(1, N.TERM_DTYPE)),
+                    energy=torch.zeros(B, dtype=torch.float64, device=dev),
+                    grad=torch.zeros(1, dtype=torch.float64, device=dev))
+        code = N.DESV_C64 if self.dtype == torch.complex64 else N.DESV_C128
+        wsb = int(N.lib().desv_batch_workspace_bytes(code, 9, p.pool_len))   # pools only: states are the rows
+        ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        a = BatchArgs()
+        a.ncirc = B
+        for f, t_ in bufs.items():
+            setattr(a, f, t_.data_ptr())
+        a.states = out.data_ptr()
+        N.check(N.lib().desv_batch_vqe(code, 9, p.pool_len, ctypes.byref(a), ctypes.c_void_p(ws.data_ptr()),
+                                       ws.numel(), ctypes.c_void_p(N.stream_ptr())), 'batched forward')
+        self._keep = (bufs, ws)        # alive until the stream has run the launch
+        return out

@@ -216,6 +216,8 @@ typedef struct desv_batch_circuit {
     int64_t theta_off;           /* first parameter in theta */
     int64_t coef_off;            /* first term coefficient in coef */
     int64_t grad_off;            /* first gradient entry in grad */
+    int64_t state_off;           /* forward-only plans (no terms, no adjoint passes): the circuit's
+                                    final state goes to states + state_off (amplitudes); -1: none */
 } desv_batch_circuit;
 
 /* device pointers of one batch; workspace fields are filled by desv_batch_vqe */
@@ -234,13 +236,18 @@ typedef struct desv_batch_args {
     uint64_t ws_amps;
     void *pool_ws;
     uint64_t pool_stride_bytes;
+    void *states;                       /* forward-only circuits' output states (may be NULL) */
 } desv_batch_args;
 
 size_t desv_batch_workspace_bytes(int dtype, int max_n, int max_pool_len);
 /* One persistent launch over every circuit of `args` (host struct of device
  * pointers).  Circuits of <= 12 qubits run in shared memory; larger ones
  * stream a per-CTA slice of `workspace`.  Capturable in a CUDA graph after a
- * first (warm-up) call. */
+ * first (warm-up) call.  Forward-only circuits (a plan without terms and
+ * adjoint passes, state_off >= 0, args->states set: run_batch_jit's rows)
+ * write their final state to args->states + state_off and, when wider than
+ * 12 qubits, are evolved there in place, so max_n (which sizes the per-CTA
+ * state slices) only has to cover the other circuits. */
 int desv_batch_vqe(int dtype, int max_n, int max_pool_len, const desv_batch_args *args, void *workspace,
                    size_t workspace_bytes, void *stream);
 

@@ -121,6 +121,27 @@ def test_run_batch_jit_matches_run_circuit(de):
         sim.run_parametric_batch_jit(base, pb)
 
 
+@pytest.mark.parametrize('n,f32', [(14, False), (14, True), (9, True)])
+def test_run_batch_jit_one_launch_rows(de, n, f32):
+    """run_batch_jit's rows in one persistent launch: resident (<= 12 qubits)
+    and streamed (evolved in place in their output rows) states, both
+    precisions, against the oracle per row."""
+    rng = np.random.default_rng(n)
+    base = [('h', q) for q in range(n)] + [('ry', q, 0.0) for q in range(n)] + \
+        [('cx', q, q + 1) for q in range(n - 1)] + [('rx', q, 0.0) for q in range(0, n, 2)] + \
+        [('cp', 1, n - 1, 0.0), ('crz', n - 2, 0, 0.0), ('t', 3), ('rz', n - 1, 0.0)]
+    npar = sum(1 for c in base if c[0] in ('ry', 'rx', 'rz', 'cp', 'crz'))
+    pb = rng.uniform(-np.pi, np.pi, (7, npar))
+    sim = de.DenseSVSimulator(n, use_float32=f32)
+    out = sim.run_batch_jit(base, pb).cpu().numpy()
+    assert out.shape == (7, 1 << n)
+    for r in range(7):
+        k = iter(pb[r])
+        circ = [(c[0], *c[1:-1], next(k)) if c[0] in ('ry', 'rx', 'rz', 'cp', 'crz') else c for c in base]
+        ref = O.run_circuit(O.zero_state(n), n, circ)
+        assert np.max(np.abs(out[r] - ref)) <= (1e-5 if f32 else 1e-12)
+
+
 def test_float32_matches_float64(de):
     n = 12
     circ = de.random_circuit(n, 300, seed=11)
