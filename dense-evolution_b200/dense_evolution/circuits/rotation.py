@@ -635,20 +635,130 @@ class RotationPlan:
                 sc[o[1]] = g
         return runs_, d2g, sc
 
+    _KIND = {'rx': 1, 'ry': 2, 'rz': 3, 'p': 4, 'u1': 4, 'phase': 4}
+
     def uop_matrices(self, theta=None, runs_=None) -> np.ndarray:
-        """FP64 2x2 matrix of every fused run for these parameters."""
-        M = np.tile(np.eye(2, dtype=np.complex128), (len(self.uops), 1, 1))
-        for i, u in enumerate(self.uops):
-            m = np.eye(2, dtype=np.complex128)
-            for g in (u.gates if runs_ is None else runs_[i]):
-                m = g.matrix(theta) @ m
-            M[i] = m
+        """FP64 2x2 matrix of every fused run for these parameters (vectorised:
+        every gate's matrix at once by kind, then the products along the runs
+        position by position)."""
+        runs_ = [u.gates for u in self.uops] if runs_ is None else runs_
+        R_ = len(runs_)
+        M = np.tile(np.eye(2, dtype=np.complex128), (R_, 1, 1))
+        if R_ == 0:
+            return M
+        lens = np.array([len(r) for r in runs_])
+        flat = [g for r in runs_ for g in r]
+        G = len(flat)
+        kind = np.zeros(G, np.int8)
+        val = np.zeros(G)
+        mats = np.tile(np.eye(2, dtype=np.complex128), (G, 1, 1))
+        th = None if theta is None else np.asarray(theta, dtype=np.float64)
+        for i, g in enumerate(flat):
+            if g.const is not None:
+                mats[i] = g.const
+            else:
+                kind[i] = self._KIND[g.name]
+                val[i] = g.value if g.slot < 0 or th is None else th[g.slot]
+        c, s_ = np.cos(val / 2), np.sin(val / 2)
+        k = kind == 1
+        mats[k] = np.stack([np.stack([c[k], -1j * s_[k]], -1), np.stack([-1j * s_[k], c[k]], -1)], -2)
+        k = kind == 2
+        mats[k] = np.stack([np.stack([c[k], -s_[k]], -1), np.stack([s_[k], c[k]], -1)], -2)
+        k = kind == 3
+        mats[k] = 0
+        mats[k, 0, 0], mats[k, 1, 1] = np.exp(-0.5j * val[k]), np.exp(0.5j * val[k])
+        k = kind == 4
+        mats[k] = 0
+        mats[k, 0, 0], mats[k, 1, 1] = 1.0, np.exp(1j * val[k])
+        start = np.concatenate([[0], np.cumsum(lens)[:-1]])
+        for pos in range(int(lens.max())):
+            sel = np.nonzero(lens > pos)[0]
+            M[sel] = mats[start[sel] + pos] @ M[sel]
         return M
+
+    # ------------------------------------------------------------ value program
+    def _prepare_values(self):
+        """Index arrays of the value program (once per plan): every table entry,
+        phase and two-bit diagonal value is a unit-modulus factor, so a call
+        only sums angles (np.bincount) and takes one complex exponential."""
+        if getattr(self, '_vp', None) is not None:
+            return self._vp
+        ph_idx = {pi: i for i, pi in enumerate(pi for pi, pr in enumerate(self.prims) if pr.kind == 'ph')}
+        d2_idx = {pi: i for i, pi in enumerate(pi for pi, pr in enumerate(self.prims) if pr.kind == 'd2')}
+        nph, nd2 = len(ph_idx), len(d2_idx)
+        fr_ph, fr_u, fr_k = [], [], []
+        for pi, i in ph_idx.items():
+            for u, kind in self.prims[pi].factors:
+                fr_ph.append(i)
+                fr_u.append(u)
+                fr_k.append({'pre': 0, 'post': 1, 'diag': 2}[kind])
+        SIGN = nph + 4 * nd2                    # angle source index of a -1 (pi)
+        offs = np.cumsum([0] + [ps.n_floats for ps in self.passes])
+        tab_ent, tab_src, ent_pos = [], [], []  # table entries: flat entry, angle source; entry -> float position
+        cval_src, cval_pos = [], []             # other unit values written as (re, im): source, float position
+        nent = 0
+        for pidx, ps in enumerate(self.passes):
+            base = int(offs[pidx])
+            for kind, x in ps.order:
+                if kind != 'grp':
+                    continue
+                g = x
+                if g.has_table:
+                    slots = [q for q in range(RB) if (g.reg_mask >> q) & 1]
+                    idx = {q: k for k, q in enumerate(slots)}
+                    ks = np.arange(1 << len(slots))
+                    for pi, sa, sb in g.table_items:
+                        ba = (ks >> idx[sa]) & 1
+                        if pi < 0:
+                            sel = ks[(ba & ((ks >> idx[sb]) & 1)) == 1]
+                            tab_ent += list(nent + sel)
+                            tab_src += [SIGN] * len(sel)
+                        elif sb < 0:
+                            sel = ks[ba == 1]
+                            tab_ent += list(nent + sel)
+                            tab_src += [ph_idx[pi]] * len(sel)
+                        else:
+                            e = ba + 2 * ((ks >> idx[sb]) & 1)
+                            tab_ent += list(nent + ks)
+                            tab_src += list(nph + 4 * d2_idx[pi] + e)
+                    ent_pos += list(base + g.t_off + 2 * ks)
+                    nent += len(ks)
+                for it in g.f_items:
+                    if it[0] == 'ph':
+                        cval_src.append(ph_idx[it[1]])
+                        cval_pos.append(base + it[3])
+                    else:
+                        for e in range(4):
+                            cval_src.append(nph + 4 * d2_idx[it[1]] + e)
+                            cval_pos.append(base + it[4] + 2 * e)
+                for pi, s_, x_, off in g.mixed_items:
+                    pr = self.prims[pi]
+                    # (x, y) -> d[y + 2 x] when the thread-fixed bit is the d2's second
+                    # bit, d[x + 2 y] when it is the first
+                    order = [0, 2, 1, 3] if pr.b == x_ else [0, 1, 2, 3]
+                    for e, dj in enumerate(order):
+                        cval_src.append(nph + 4 * d2_idx[pi] + dj)
+                        cval_pos.append(base + off + 2 * e)
+        rots = []                               # per pass: (uop indices, float positions) in program order
+        for pidx, ps in enumerate(self.passes):
+            base = int(offs[pidx])
+            us = [self.prims[pi].u for k, (pi, off) in ((k, x) for k, x in ps.order if k == 'rot')]
+            pos = [base + off for k, (pi, off) in ((k, x) for k, x in ps.order if k == 'rot')]
+            rots.append((np.array(us, np.int64), np.array(pos, np.int64)))
+        self._vp = dict(ph_idx=ph_idx, d2_idx=d2_idx, nph=nph, nd2=nd2, fr_ph=np.array(fr_ph, np.int64),
+                        fr_u=np.array(fr_u, np.int64), fr_k=np.array(fr_k, np.int64),
+                        tab_ent=np.array(tab_ent, np.int64), tab_src=np.array(tab_src, np.int64),
+                        ent_pos=np.array(ent_pos, np.int64), nent=nent, cval_src=np.array(cval_src, np.int64),
+                        cval_pos=np.array(cval_pos, np.int64), offs=offs, rots=rots,
+                        rot_u=np.array(sorted({pr.u for pr in self.prims if pr.kind == 'rot'}), np.int64),
+                        diag_u=np.array([i for i, u in enumerate(self.uops) if u.diag], np.int64))
+        return self._vp
 
     def materialize(self, theta=None, dtype=np.float32, ir=None) -> Tuple[List[np.ndarray], complex]:
         """Per-pass parameter blocks (float32 for the kernels; float64 for exact
         emulation in tests) for these parameters, and the circuit's global
         factor (applied by the last pass's end factor)."""
+        vp = self._prepare_values()
         if ir is not None:
             runs_, d2g, scalars = self.bind(ir)
         else:
@@ -662,101 +772,68 @@ class RotationPlan:
         s = np.abs(V[:, 1, 0])
         p = np.where(c > 1e-300, np.angle(V[:, 1, 1]), 0.0)
         m = np.where(s > 1e-300, np.angle(V[:, 1, 0]), 0.0)
-        pre = np.exp(1j * (p - m))
-        post = np.exp(1j * (p + m))
         d0 = M[:, 0, 0]
-        diag_ratio = M[:, 1, 1] / np.where(d0 == 0, 1, d0)
-        glob = 1.0 + 0j
-        for pr in self.prims:
-            if pr.kind == 'rot':
-                glob *= complex(g[pr.u] * np.exp(-1j * p[pr.u]))
-        for i, u in enumerate(self.uops):
-            if u.diag:
-                glob *= complex(d0[i])
+        # factor angles: pre e^{i(p-m)}, post e^{i(p+m)}, diagonal runs d1 / d0
+        fang = np.stack([p - m, p + m, np.angle(M[:, 1, 1]) - np.angle(d0)], 0)
+        ph_ang = np.bincount(vp['fr_ph'], weights=fang[vp['fr_k'], vp['fr_u']], minlength=vp['nph']) \
+            if vp['nph'] else np.zeros(0)
+        # global factor (every piece has modulus 1): rotation runs g e^{-ip}, diagonal runs d0, scalars, d2 d[0]
+        gang = float(np.sum(np.angle(g[vp['rot_u']]) - p[vp['rot_u']]) + np.sum(np.angle(d0[vp['diag_u']])))
         for sg in scalars:
-            glob *= complex(np.exp(1j * (sg.value if sg.slot < 0 or theta is None else float(theta[sg.slot]))))
-
-        def phase_value(pi: int) -> complex:
-            v = 1.0 + 0j
-            for ui, kind in self.prims[pi].factors:
-                v *= pre[ui] if kind == 'pre' else post[ui] if kind == 'post' else diag_ratio[ui]
-            return complex(v)
-
-        d2v: Dict[int, np.ndarray] = {}
-        for pi, pr in enumerate(self.prims):
-            if pr.kind == 'd2':
-                gt = d2g[pi]
-                if gt.const is not None:
-                    d = np.asarray(gt.const, dtype=np.complex128)
-                else:
-                    val = gt.value if gt.slot < 0 or theta is None else float(theta[gt.slot])
-                    d = np.asarray(fusion.gate_matrix_of('d2', gt.name, val), dtype=np.complex128)
-                glob *= complex(d[0])
-                d2v[pi] = d / d[0]
-
-        blocks = []
-        for ps in self.passes:
-            v = np.zeros(ps.n_floats, dtype=np.float64)
+            gang += sg.value if sg.slot < 0 or theta is None else float(theta[sg.slot])
+        d2_ang = np.zeros((vp['nd2'], 4))
+        for pi, i in vp['d2_idx'].items():
+            gt = d2g[pi]
+            if gt.const is not None:
+                d = np.asarray(gt.const, dtype=np.complex128)
+            else:
+                val = gt.value if gt.slot < 0 or theta is None else float(theta[gt.slot])
+                d = np.asarray(fusion.gate_matrix_of('d2', gt.name, val), dtype=np.complex128)
+            a = np.angle(d)
+            gang += a[0]
+            d2_ang[i] = a - a[0]
+        src = np.concatenate([ph_ang, d2_ang.reshape(-1), [np.pi]])
+        glob = complex(np.exp(1j * gang))
+        flat = np.zeros(int(vp['offs'][-1]), dtype=np.float64)
+        if vp['nent']:
+            T = np.exp(1j * np.bincount(vp['tab_ent'], weights=src[vp['tab_src']], minlength=vp['nent']))
+            flat[vp['ent_pos']] = T.real
+            flat[vp['ent_pos'] + 1] = T.imag
+        if len(vp['cval_src']):
+            cv = np.exp(1j * src[vp['cval_src']])
+            flat[vp['cval_pos']] = cv.real
+            flat[vp['cval_pos'] + 1] = cv.imag
+        for pidx, ps in enumerate(self.passes):
+            us, pos = vp['rots'][pidx]
             scale = 1.0
-            for kind, x in ps.order:
-                if kind == 'rot':
-                    pi, off = x
-                    ui = self.prims[pi].u
-                    ci, si = float(c[ui]), float(s[ui])
-                    t = si / ci if ci > 0 else np.inf
-                    if abs(t) <= TMAX and scale / ci <= SCALE_LIMIT:
-                        v[off:off + 4] = (t, ci, si, 0.0)
-                        scale /= ci
-                    else:
-                        v[off:off + 4] = (0.0, ci, si, 1.0)
-                elif kind == 'grp':
-                    self._group_values(x, v, phase_value, d2v, scale)
-                    if x.absorbs:
-                        scale = 1.0
+            if len(us):
+                ci, si = c[us], s[us]
+                with np.errstate(divide='ignore'):
+                    t = np.where(ci > 0, si / np.where(ci > 0, ci, 1.0), np.inf)
+                tan = np.abs(t) <= TMAX
+                grow = np.cumprod(np.where(tan, 1.0 / np.where(tan, ci, 1.0), 1.0))
+                if grow[-1] > SCALE_LIMIT or np.any(grow > SCALE_LIMIT):
+                    # rare: keep the pending scale bounded rotation by rotation
+                    tan = tan.copy()
+                    sc = 1.0
+                    for k in range(len(us)):
+                        if tan[k] and sc / ci[k] <= SCALE_LIMIT:
+                            sc /= ci[k]
+                        else:
+                            tan[k] = False
+                    scale = sc
                 else:
-                    f = complex(1.0 / scale) * (glob if ps.end_complex else 1.0)
-                    v[x:x + 2] = (f.real, f.imag)
-                    scale = 1.0
-            blocks.append(v.astype(dtype))
+                    scale = float(grow[-1])
+                flat[pos] = np.where(tan, t, 0.0)
+                flat[pos + 1] = ci
+                flat[pos + 2] = si
+                flat[pos + 3] = np.where(tan, 0.0, 1.0)
+            if ps.end_scale_off >= 0:
+                f = complex(1.0 / scale) * (glob if ps.end_complex else 1.0)
+                o = int(vp['offs'][pidx]) + ps.end_scale_off
+                flat[o], flat[o + 1] = f.real, f.imag
+        blocks = [flat[vp['offs'][i]:vp['offs'][i + 1]].astype(dtype) for i in range(len(self.passes))]
         return blocks, glob
-
-    def _group_values(self, grp: Group, v: np.ndarray, phase_value, d2v, scale: float):
-        if grp.has_table:
-            slots = [q for q in range(RB) if (grp.reg_mask >> q) & 1]
-            idx = {q: k for k, q in enumerate(slots)}
-            ks = np.arange(1 << len(slots))
-            T = np.ones(len(ks), dtype=np.complex128)
-            for pi, sa, sb in grp.table_items:
-                ba = (ks >> idx[sa]) & 1
-                if pi < 0:                                   # folded register-register cz
-                    T *= np.where(ba & ((ks >> idx[sb]) & 1), -1.0, 1.0)
-                elif sb < 0:                                  # phase on slot sa
-                    T *= np.where(ba == 1, phase_value(pi), 1.0)
-                else:                                         # d2: index bit(b) + 2 bit(b2)
-                    bb = (ks >> idx[sb]) & 1
-                    T *= d2v[pi][ba + 2 * bb]
-            v[grp.t_off:grp.t_off + 2 * len(T):2] = T.real
-            v[grp.t_off + 1:grp.t_off + 2 * len(T):2] = T.imag
-        for it in grp.f_items:
-            if it[0] == 'ph':
-                _, pi, x, off = it
-                e = phase_value(pi)
-                v[off:off + 2] = (e.real, e.imag)
-            else:
-                _, pi, a, b, off = it
-                d = d2v[pi]
-                v[off:off + 8] = np.stack([d.real, d.imag], -1).reshape(-1)
-        for pi, s_, x, off in grp.mixed_items:
-            pr = self.prims[pi]
-            d = d2v[pi]
-            # value for (x = bit of the thread-fixed global bit, y = bit of the slot)
-            if pr.b == x:          # the thread-fixed bit is the low index bit of d
-                f = [d[0 + 2 * 0], d[0 + 2 * 1], d[1 + 2 * 0], d[1 + 2 * 1]]
-            else:
-                f = [d[0], d[1], d[2], d[3]]
-                f = [f[0 + 0], f[1 + 0], f[0 + 2], f[1 + 2]]   # (x, y) -> d[y + 2 x]
-            vals = np.array(f, dtype=np.complex128)
-            v[off:off + 8] = np.stack([vals.real, vals.imag], -1).reshape(-1)
 
 
 # ---------------------------------------------------------------------------
