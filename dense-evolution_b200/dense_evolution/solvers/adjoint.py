@@ -229,8 +229,15 @@ class AdjointProgram:
             # plan-specialised backward passes (complex64: the complex128 pair of
             # register tiles does not fit the register file); sources, and so
             # kernels, change only with the records' dispatch codes
-            kernels = jit.compile_adjoint(self.back.ops, p, mats, self.dtype == torch.complex64,
-                                          dev.index if dev.index is not None else torch.cuda.current_device())
+            # the sources (and so the kernels) depend only on the op records: reuse
+            # them while the records stay the same (new angles change only values)
+            import hashlib
+            okey = (hashlib.sha1(self.back.ops.tobytes()).hexdigest(), dev.index)
+            if getattr(self, '_adj_kernels', None) is None or self._adj_kernels[0] != okey:
+                kernels = jit.compile_adjoint(self.back.ops, p, mats, self.dtype == torch.complex64,
+                                              dev.index if dev.index is not None else torch.cuda.current_device())
+                self._adj_kernels = (okey, kernels)
+            kernels = self._adj_kernels[1]
             jit.run_adjoint(kernels, mu.data_ptr(), lam.data_ptr(), self.n, N.dtype_code(mu), p, ops_t.data_ptr(),
                             mats_t.data_ptr(), map_t.data_ptr(), grad.data_ptr(), self._scratch.data_ptr(),
                             self._scratch.numel() * 8, N.stream_ptr())
