@@ -103,6 +103,10 @@ __device__ __forceinline__ void flip(float2 &v, uint32_t w) {
 // a 2^K tile as the bulk copies leave it, with room for the padded layout the
 // stages re-lay it into.  Loads run NBUF-1 tiles ahead.
 template <int K, int NBUF, uint32_t SLOT> struct RotRing {
+    // every slot must start on a 16-byte boundary (bulk-copy destinations) and
+    // hold the padded layout of a tile
+    static_assert(SLOT % 2 == 0, "ring slots of whole 16-byte units");
+    static_assert(SLOT >= (1u << K) + ((1u << K) - 1) / 16, "a slot holds the padded tile");
     uint64_t *full;
     float2 *bufs;
     uint32_t tid, nthr, lane, ntile, nchunks, chunk_bytes, warp_bytes, cnt;

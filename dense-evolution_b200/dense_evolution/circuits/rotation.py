@@ -876,8 +876,11 @@ def padded(i: int) -> int:
 
 
 def slot_elems(K: int) -> int:
-    """Amplitudes per ring slot: the padded layout of a 2^K tile."""
-    return padded((1 << K) - 1) + 1
+    """Amplitudes per ring slot: room for the padded layout of a 2^K tile
+    (positions up to padded(2^K - 1)), rounded so that every slot starts on a
+    16-byte boundary as the bulk copies into it require.  libdesv sizes the
+    kernel's shared memory with the same value (desv_jit.cu, rot_slot_elems)."""
+    return (1 << K) + (1 << (K - PAD_SHIFT))
 
 
 # ---------------------------------------------------------------------------

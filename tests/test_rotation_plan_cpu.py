@@ -130,9 +130,13 @@ def test_register_sets_are_bank_conflict_free():
                 assert R._bank_ok(st.regs, ps.K, padded=False)
             if si == len(ps.stages) - 1:
                 assert all(b >= 4 for b in st.regs)       # half-warp stores of 128 contiguous bytes
-    # the padded layout is injective and fits its slot
-    pos = [R.padded(i) for i in range(1 << 12)]
-    assert len(set(pos)) == 4096 and max(pos) < R.slot_elems(12)
+    # the padded layout is injective and fits its slot; slots start on 16-byte
+    # boundaries (bulk-copy destinations) and match libdesv's shared-memory size
+    for K in (9, 10, 11, 12):
+        pos = [R.padded(i) for i in range(1 << K)]
+        assert len(set(pos)) == 1 << K and max(pos) < R.slot_elems(K)
+        assert (R.slot_elems(K) * 8) % 16 == 0
+        assert R.slot_elems(K) == (1 << K) + (1 << (K - 4))
 
 
 def test_headline_schedule_shape():
