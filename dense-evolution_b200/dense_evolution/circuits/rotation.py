@@ -416,6 +416,11 @@ class RotationPlan:
                 L += 1
             high = [b for b in range(L, n) if (tile >> b) & 1]
             self.passes.append(self._stages(K, L, high, taken))
+        if not self.passes:
+            # no primitive at all (global phases or identities only): one pass
+            # whose end factor applies the circuit's global factor
+            L = K
+            self.passes.append(RotPass(K, L, [], [Stage(tuple(_candidate_regs(K, True, True)[0]))]))
 
     def _stages(self, K: int, L: int, high: List[int], ids: List[int]) -> RotPass:
         tl = {b: b for b in range(L)}

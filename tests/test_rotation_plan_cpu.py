@@ -78,6 +78,13 @@ def test_every_gate_kind_against_oracle(seed):
     _check(_mixed_circuit(n, 160, seed), n, cap=16)
 
 
+@pytest.mark.parametrize('circ', [[('gphase', 0, -1.9)], [('id', 3)], [('gphase', 0, 0.4), ('gphase', 2, 0.3)]])
+def test_circuits_without_rotations_or_diagonals(circ):
+    """A circuit of global phases (or identities) only still gets one pass,
+    whose end factor applies the global factor."""
+    _check(circ, 12)
+
+
 def test_gate_free_tail_and_trailing_phases():
     n = 12
     circ = [('h', q) for q in range(n)] + [('rz', q, 0.1 * q) for q in range(n)] + [('cp', 0, 11, 0.7), ('t', 5)]

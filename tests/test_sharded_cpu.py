@@ -99,3 +99,27 @@ def test_two_gloo_ranks_exchange_halves():
     for _, _, ex, full in got:
         assert ex > 0
         assert np.max(np.abs(full - ref)) <= 1e-12
+
+
+def test_split_state_with_rotation_plans_for_the_chunks():
+    """The per-chunk circuits (specialised gates, chunk-local phases, circuits of
+    a global phase alone) through the rotation planner and the tile emulator --
+    the path the chunks take on a GPU from 20 local qubits on."""
+    import rotation_emulator as E
+    from dense_evolution.backends.sharded import ShardedState
+    from dense_evolution.circuits import rotation as R
+    from dense_evolution.workloads import brick_u3_circuit
+
+    def applier(chunk, n_local, gates):
+        bp = R.program_for(list(gates), n_local, 12)
+        blocks, _ = bp.plan.materialize(None, np.float64, bp.ir)
+        sv = chunk.numpy().astype(np.complex128)
+        E.run(bp.plan, sv, blocks)
+        chunk.copy_(torch.from_numpy(sv))
+
+    n = 14
+    circ = brick_u3_circuit(n, 6, seed=11)
+    st = ShardedState(n, 2, torch.complex128, device='cpu', applier=applier)
+    st.run_circuit(circ)
+    ref = O.run_circuit(O.zero_state(n), n, circ)
+    assert np.max(np.abs(st.logical_state() - ref)) <= 1e-12
