@@ -235,9 +235,6 @@ extern "C" int desv_jit_load(const char *src, const char *include_dir, int kind,
     const size_t esz = dtype == DESV_C64 ? 8 : 16;
     const int nw = (1 << (tile_bits - 4)) / 32 > 0 ? (1 << (tile_bits - 4)) / 32 : 1;
     k->smem = PIPE_HDR_BYTES + (size_t)nbuf * (kind == 1 ? 2 : 1) * ((size_t)1 << tile_bits) * esz;
-    // complex64 Pauli passes keep an FP64 copy of the current tile after the ring
-    // (every amplitude is converted once, then read as a partner by each group)
-    if (kind >= 2 && dtype == DESV_C64) k->smem += ((size_t)1 << tile_bits) * sizeof(double2);
     // adjoint kernels: room for the per-warp gradient accumulators of the largest pass
     const size_t smem_max = k->smem + (kind == 1 ? (size_t)nw * JIT_ADJ_MAX_PARAMS * sizeof(double) : 0);
     size_t ssz = 0;

@@ -252,14 +252,6 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
              f'desv_jit_kernel(const {T} *psi, {T} *out, TileGeom g, int want_e, double *part) {{',
              '    extern __shared__ __align__(128) unsigned char smem[];',
              f'    auto body = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L, double &ere, double &eim) {{']
-    if complex64:
-        # every amplitude converted to FP64 once per tile, into a copy after the
-        # ring; the term groups then read FP64 partners without conversions
-        lines += [f'        double2 *d = reinterpret_cast<double2 *>(smem + PIPE_HDR_BYTES + 4 * {1 << K} * sizeof(float2));',
-                  '#pragma unroll 4',
-                  f'        for (uint32_t j = threadIdx.x; j < {1 << K}u; j += 256u) {{ const float2 q = s[j]; '
-                  'd[j] = make_double2((double)q.x, (double)q.y); }',
-                  '        __syncthreads();']
     groups = {}
     for k, t in enumerate(terms):
         groups.setdefault(int(t['xmask']), []).append(k)
@@ -312,11 +304,8 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
         lines.append('            {')
         lines.append('                double2 p[4];')
         lines.append('#pragma unroll')
-        if complex64:
-            lines.append(f'                for (int r = 0; r < 4; ++r) p[r] = d[(j0 + r * 256u) ^ {xl}u];')
-        else:
-            lines.append(f'                for (int r = 0; r < 4; ++r) {{ const {T} q = s[(j0 + r * 256u) ^ {xl}u]; '
-                         'p[r] = make_double2((double)q.x, (double)q.y); }')
+        lines.append(f'                for (int r = 0; r < 4; ++r) {{ const {T} q = s[(j0 + r * 256u) ^ {xl}u]; '
+                     'p[r] = make_double2((double)q.x, (double)q.y); }')
         lines.append('#pragma unroll')
         lines.append('                for (int r = 0; r < 4; ++r) {')
         lines.append(f'                    const uint32_t jx = (j0 + r * 256u) ^ {xl}u;')
@@ -341,9 +330,8 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
     lines += ['#pragma unroll',
               '            for (int r = 0; r < 4; ++r) {',
               '                const uint32_t j = j0 + r * 256u;']
-    aread = 'const double2 a = d[j];' if complex64 else f'const {T} a = s[j];'
     if mode != 0:
-        lines.append('                { ' + aread + ' ere += (double)a.x * v[r].x + (double)a.y * v[r].y; '
+        lines.append('                { const ' + T + ' a = s[j]; ere += (double)a.x * v[r].x + (double)a.y * v[r].y; '
                      'eim += (double)a.x * v[r].y - (double)a.y * v[r].x; }')
         lines.append('                const uint64_t gi = base + tl2g(ctab, L, j);')
         if mode == 1:
@@ -352,12 +340,9 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
             lines.append(f'                {{ {T} o = out[gi]; o.x = ({R})((double)o.x + v[r].x); '
                          f'o.y = ({R})((double)o.y + v[r].y); out[gi] = o; }}')
     else:
-        lines.append('                if (want_e) { ' + aread + ' ere += (double)a.x * v[r].x + '
+        lines.append('                if (want_e) { const ' + T + ' a = s[j]; ere += (double)a.x * v[r].x + '
                      '(double)a.y * v[r].y; eim += (double)a.x * v[r].y - (double)a.y * v[r].x; }')
-    lines += ['            }', '        }']
-    if complex64:
-        lines.append('        __syncthreads();  // the FP64 copy is rewritten by the next tile')
-    lines += ['    };',
+    lines += ['            }', '        }', '    };',
               f'    jit_pauli_kernel<{T}, {K}, 4>(psi, g, want_e, part, smem, body);', '}', '']
     return '\n'.join(lines)
 
