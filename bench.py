@@ -373,7 +373,7 @@ def run_headline(args, ws, local):
     # circuit transpile + fusion + H2D of the op/matrix tables, run, <Z_i> read back
     sim = de.DenseSVSimulator(n, use_float32=True)
     e2e_times, h2d = [], 0
-    for i in range(args.warmup + args.steps):
+    for i in range(0 if args.skip_e2e else args.warmup + args.steps):
         c = brick_u3_circuit(n, layers, SEED + 1 + i)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -391,7 +391,7 @@ def run_headline(args, ws, local):
                 ops_i, mats_i = plan_i.device_arrays(dev)
                 h2d = int(ops_i.numel() + mats_i.numel() * 4)
         sim._plans.clear()
-    e2e_step = _max_over_ranks(float(np.mean(e2e_times)), ws)
+    e2e_step = _max_over_ranks(float(np.mean(e2e_times)), ws) if e2e_times else float('nan')
     e2e_value = ws * npasses * pass_bytes / e2e_step / 1e9
     steps_ms = per_pass.reshape(args.steps, npasses).mean(axis=0)
     if rot is not None:
@@ -444,7 +444,7 @@ def run_ours(args):
     line = run_headline(args, ws, local) if not args.skip_headline else {
         'metric': METRIC, 'value': None, 'unit': 'GB/s', 'n_gpus': ws, 'steps': args.steps,
         'warmup': args.warmup, 'higher_is_better': True, 'skipped': 'headline (--skip-headline)'}
-    if not args.skip_headline and args.qubits == N_QUBITS:
+    if not args.skip_headline and args.qubits == N_QUBITS and not args.skip_fidelity:
         line['fidelity_28q'] = fidelity_check(28, args.layers)
     line['vqe'] = run_vqe(args) if not args.skip_vqe else None
     torch.cuda.empty_cache()
@@ -655,6 +655,8 @@ def main():
     ap.add_argument('--skip-batch', action='store_true')
     ap.add_argument('--skip-large', action='store_true')
     ap.add_argument('--skip-headline', action='store_true')
+    ap.add_argument('--skip-fidelity', action='store_true', help='headline without the 28-qubit accuracy check')
+    ap.add_argument('--skip-e2e', action='store_true', help='headline without the end-to-end leg')
     ap.add_argument('--vqe-qubits', type=int, default=VQE_N, help='VQE block width (default 24)')
     ap.add_argument('--vqe-no-shift', action='store_true', help='VQE block without the parameter-shift leg')
     ap.add_argument('--batch-circuits', type=int, default=4096, help='batch block size (default 4096)')

@@ -103,7 +103,6 @@ struct JitKernel {
 // kind of a rotation-pass kernel (desv_rot_load)
 constexpr int JIT_KIND_ROT = 5;
 constexpr int ROT_REG_BITS = 5;     // register slots per stage (rot_pass.cuh: 32 amplitudes per thread)
-constexpr int ROT_NBUF = 3;         // ring slots
 constexpr int ROT_MAX_PARAM_FLOATS = 7936;  // by-value parameter block <= 31 KiB (limit 32764 bytes)
 
 // padded stage layout of a 2^K tile: one spare amplitude after every 16
@@ -342,12 +341,13 @@ extern "C" int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int d
     return DESV_OK;
 }
 
-extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile_bits, int param_floats, int device,
-                             void **handle, char *log, size_t loglen) {
+extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile_bits, int nbuf, int param_floats,
+                             int device, void **handle, char *log, size_t loglen) {
     if (!src || !include_dirs || !handle) return fail(DESV_EINVAL, "rotation pass load: null argument");
     *handle = nullptr;
     if (tile_bits < ROT_REG_BITS + 4 || tile_bits > 12)
         return fail(DESV_EINVAL, "rotation pass load: tile_bits must be in [9, 12]");
+    if (nbuf < 2 || nbuf > 3) return fail(DESV_EINVAL, "rotation pass load: nbuf must be 2 or 3");
     if (param_floats < 1 || param_floats > ROT_MAX_PARAM_FLOATS)
         return fail(DESV_EINVAL, "rotation pass load: parameter block size out of range");
     if (!api().ok) return fail(DESV_EUNSUPPORTED, "jit: " + api().why);
@@ -358,11 +358,11 @@ extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile
     auto *k = new JitKernel();
     k->kind = JIT_KIND_ROT;
     k->K = tile_bits;
-    k->nbuf = ROT_NBUF;
+    k->nbuf = nbuf;
     k->dtype = DESV_C64;
     k->threads = 1 << (tile_bits - ROT_REG_BITS);
     k->param_floats = param_floats;
-    k->smem = PIPE_HDR_BYTES + (size_t)ROT_NBUF * rot_slot_elems(tile_bits) * sizeof(float2);
+    k->smem = PIPE_HDR_BYTES + (size_t)nbuf * rot_slot_elems(tile_bits) * sizeof(float2);
     size_t ssz = 0;
     if (cudaSetDevice(device) != cudaSuccess) {
         delete k;

@@ -73,7 +73,8 @@ _SIGS = {
     'desv_jit_adjoint': ([_vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp], _i),
     'desv_jit_free': ([_vp], _i),
     'desv_jit_pass': ([_vp, _vp, _i, _i, _vp, _vp, _vp], _i),
-    'desv_rot_load': ([ctypes.c_char_p, ctypes.c_char_p, _i, _i, _i, ctypes.POINTER(_vp), ctypes.c_char_p, _sz], _i),
+    'desv_rot_load': ([ctypes.c_char_p, ctypes.c_char_p, _i, _i, _i, _i, ctypes.POINTER(_vp), ctypes.c_char_p, _sz],
+                      _i),
     'desv_rot_pass': ([_vp, _vp, _i, _vp, _vp, _i, _vp], _i),
     'desv_bit_reverse': ([_vp, _vp, _i, _i, _vp], _i),
     'desv_jit_compile_check': ([ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _sz], _i),

@@ -67,6 +67,17 @@ TMAX = 16.0            # tangent form while |tan| <= TMAX
 SCALE_LIMIT = 2.0 ** 60  # pending tangent scale above which rotations switch to the general form
 MAX_ROTS_PER_PASS = 48
 PAD_SHIFT = 4          # padded stage layout: physical = i + (i >> 4)
+NBUF = 3               # ring slots per CTA (3: two CTAs per SM; 2: three)
+
+
+def tuning() -> Tuple[int, int]:
+    """(rotations per pass at most, ring slots): MAX_ROTS_PER_PASS and NBUF,
+    overridden by DESV_ROT_MAX_ROTS / DESV_ROT_NBUF (for tuning sweeps)."""
+    cap = int(os.environ.get('DESV_ROT_MAX_ROTS', MAX_ROTS_PER_PASS))
+    nb = int(os.environ.get('DESV_ROT_NBUF', NBUF))
+    if cap < 1 or nb not in (2, 3):
+        raise ValueError('DESV_ROT_MAX_ROTS must be >= 1 and DESV_ROT_NBUF 2 or 3')
+    return cap, nb
 
 _H = GATES['h']
 _S = GATES['s']
@@ -358,7 +369,7 @@ class RotationPlan:
     """Passes, stages and groups of one circuit structure, plus the value program."""
 
     def __init__(self, target: Sequence[tuple], n: int, kmax: int = 12, slots=None,
-                 max_rots: int = MAX_ROTS_PER_PASS, low_fixed: int = LOW_FIXED):
+                 max_rots: Optional[int] = None, low_fixed: int = LOW_FIXED):
         low = lower_program(target, n, slots)
         if low is None:
             raise ValueError('rotation passes: the circuit holds a gate this path does not lower')
@@ -368,7 +379,8 @@ class RotationPlan:
         self.K = min(kmax, n)
         if self.K < RB + 4 or n < self.K:
             raise ValueError('rotation passes need at least 9 qubits')
-        self.max_rots = max_rots
+        cap, self.nbuf = tuning()
+        self.max_rots = cap if max_rots is None else max_rots
         self.low_fixed = min(low_fixed, self.K)
         self.passes: List[RotPass] = []
         self._schedule()
@@ -907,9 +919,10 @@ def _f(x: float) -> str:
     return repr(float(x)) + 'f'
 
 
-def pass_source(plan: 'RotationPlan', pidx: int, nbuf: int = 3) -> str:
+def pass_source(plan: 'RotationPlan', pidx: int, nbuf: Optional[int] = None) -> str:
     """CUDA source of one rotation pass (entry point desv_rot_kernel)."""
     ps = plan.passes[pidx]
+    nbuf = nbuf or plan.nbuf
     K, L, high = ps.K, ps.L, ps.high
     NA = 1 << RB
     nthreads = 1 << (K - RB)
@@ -918,7 +931,7 @@ def pass_source(plan: 'RotationPlan', pidx: int, nbuf: int = 3) -> str:
     lines = ([f'#define DESV_ROT_CHECK 1', f'#define ROT_SLOT_ELEMS {slot_elems(K)}u'] if check else []) + \
             ['#include "rot_pass.cuh"', 'using namespace desv;',
              f'struct RotParams {{ float v[{ps.n_floats}]; }};',
-             f'extern "C" __global__ void __launch_bounds__({nthreads}, 2)',
+             f'extern "C" __global__ void __launch_bounds__({nthreads}, {3 if nbuf == 2 else 2})',
              'desv_rot_kernel(float2 *__restrict__ sv, const TileGeom g, const RotParams P) {',
              '    extern __shared__ __align__(128) unsigned char smem[];',
              '    const uint32_t t = threadIdx.x;',
@@ -1093,7 +1106,7 @@ def enabled(n: int, complex64: bool) -> bool:
     return n >= MIN_QUBITS and jit.available()
 
 
-def _load(src: str, K: int, n_floats: int, device: int) -> _RotKernel:
+def _load(src: str, K: int, nbuf: int, n_floats: int, device: int) -> _RotKernel:
     import ctypes
     from .. import _native as N
     from . import jit
@@ -1104,8 +1117,8 @@ def _load(src: str, K: int, n_floats: int, device: int) -> _RotKernel:
         return k
     h = ctypes.c_void_p()
     log = ctypes.create_string_buffer(8192)
-    N.check(N.lib().desv_rot_load(src.encode(), jit.INCLUDE_PATH.encode(), K, n_floats, device, ctypes.byref(h),
-                                  log, 8192), 'desv_rot_load')
+    N.check(N.lib().desv_rot_load(src.encode(), jit.INCLUDE_PATH.encode(), K, nbuf, n_floats, device,
+                                  ctypes.byref(h), log, 8192), 'desv_rot_load')
     k = _RotKernel(h, n_floats)
     with _kcache_lock:
         _kcache.setdefault(key, k)
@@ -1135,8 +1148,9 @@ class RotationProgram:
             from concurrent.futures import ThreadPoolExecutor
             jobs = [(src, ps.K, ps.n_floats) for src, ps in zip(self.sources, self.plan.passes)]
             workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
+            nb = self.plan.nbuf
             with ThreadPoolExecutor(max_workers=workers) as ex:
-                self.kernels[device] = list(ex.map(lambda j: _load(j[0], j[1], j[2], device), jobs))
+                self.kernels[device] = list(ex.map(lambda j: _load(j[0], j[1], nb, j[2], device), jobs))
         return self.kernels[device]
 
     def run_blocks(self, sv_ptr: int, device: int, stream: int, blocks: list):
@@ -1162,7 +1176,7 @@ def structure_key(ir: Sequence[fusion.IRGate], n: int, kmax: int) -> str:
     name, bits, theta slot, and for constant gates whether the matrix is
     diagonal (it decides the run's kind).  Plans and kernels depend on it only."""
     h = hashlib.sha1()
-    h.update(f'{n}:{kmax}:{MAX_ROTS_PER_PASS}:{LOW_FIXED}:{RB}|'.encode())
+    h.update(f'{n}:{kmax}:{tuning()}:{LOW_FIXED}:{RB}|'.encode())
     for g in ir:
         cz = g.kind == 'd2' and g.const is not None and np.array_equal(g.const, _CZ)
         h.update(repr((g.kind, g.name, g.t, g.t2, g.cbits, g.slot, _is_const_diag(g) if g.kind == 'm1' else cz))
