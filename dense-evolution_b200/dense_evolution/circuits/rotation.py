@@ -65,9 +65,9 @@ RB = 5                 # register bits per stage (32 amplitudes per thread)
 LOW_FIXED = 5          # index bits 0..LOW_FIXED-1 are in every tile (contiguous bulk-copy runs)
 TMAX = 16.0            # tangent form while |tan| <= TMAX
 SCALE_LIMIT = 2.0 ** 60  # pending tangent scale above which rotations switch to the general form
-MAX_ROTS_PER_PASS = 48
+MAX_ROTS_PER_PASS = 32  # measured on the 30-qubit, 40-layer brick circuit: 24 -> 246 ms, 32 -> 233, 48 -> 236
 PAD_SHIFT = 4          # padded stage layout: physical = i + (i >> 4)
-NBUF = 3               # ring slots per CTA (3: two CTAs per SM; 2: three)
+NBUF = 2               # ring slots per CTA: 2 -> three CTAs (12 warps) per SM, 233 ms; 3 -> two CTAs, 274 ms
 
 
 def tuning() -> Tuple[int, int]:
