@@ -51,8 +51,9 @@ def _peaks():
 
 
 def _profile_traffic():
-    """DRAM bytes per fused-pass launch from the committed ncu summary (or None)."""
-    path = os.path.join(ROOT, 'profiles', 'fused_pass_30q_c64.txt')
+    """DRAM bytes per 30-qubit rotation-pass launch from the committed ncu summary
+    (a 28-qubit capture scaled by the state size), or None."""
+    path = os.path.join(ROOT, 'profiles', 'rotation_pass_28q_c64.txt')
     try:
         with open(path) as f:
             for line in f:
@@ -593,11 +594,23 @@ def run_batch(args, layers=6):
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) / reps * 1e3
     amps = float(np.sum(2.0 ** ns))
+    # algorithmic HBM bytes of the streamed (> 12-qubit) circuits: forward passes
+    # 2 2^n B, backward passes 4 2^n B (psi and lambda), lambda = H psi 2 2^n B;
+    # circuits of <= 12 qubits never leave shared memory
+    hbm = 0.0
+    for i, (pi, _, _) in enumerate(b.circ):
+        p = b.plans[pi]
+        if p.n > 12:
+            hbm += (2 * len(p.fwd.passes) + 4 * len(p.bwd.passes) + 2) * (1 << p.n) * 8
+    hbm_gbs = hbm / (ms / 1e3) / 1e9
     return {'workload': f'{ncirc} circuits, qubits uniform in 10..20, HEA {layers} layers (RY,RZ + CX ladder), '
                         f'XXZ open chain J_xy=1, J_z~U[0.5,1.5]; energy + adjoint gradient per circuit',
             'ms_per_batch': ms, 'circuits_per_s': ncirc / (ms / 1e3), 'grads_per_s': ncirc / (ms / 1e3),
             'e2e_ms_per_batch': e2e_ms, 'plans': len(b.plans), 'launches_per_batch': 1,
             'total_amplitudes': amps, 'resident_circuits': int(np.sum(ns <= 12)),
+            'streamed_algorithmic_bytes': hbm, 'achieved_gbs_streamed': hbm_gbs,
+            'frac_of_hbm_streamed': hbm_gbs / _peaks()[0],
+            'register_bound_ctas_per_sm': int(os.environ.get('DESV_BATCH_MINB', '2')),
             'plan_build_s': build_s, 'energy_mean': float(np.mean(e)), 'tile_bits': b.tile_bits,
             'autotune_ms_per_launch_256': {str(k): v for k, v in tune.items()}}
 
@@ -627,7 +640,17 @@ def run_large(args, n=32, n_ref=30, layers=4):
     peak = torch.cuda.max_memory_allocated() / 2**30
     del psi
     torch.cuda.empty_cache()
+    # algorithmic HBM bytes of one gradient: forward passes 2 2^n B, the norm read
+    # 2^n B, H psi (every Pauli pass reads psi, writes or accumulates lambda),
+    # the mu = psi copy 2 2^n B, backward passes 4 2^n B
+    from dense_evolution.physics.observables import plan_for
+    S = (1 << n) * 8
+    pp = plan_for(xxx_terms(n), n, dtype=torch.complex64)
+    nb = len(fn.program.back.passes)
+    gbytes = (2 * fn.program.forward.npasses + 1 + (pp.npasses + 1 + 2 * (pp.npasses - 1)) + 2 + 4 * nb) * S
     out.update({'energy': e, 'grad_norm': float(np.linalg.norm(g)), 'seconds_per_gradient': dt,
+                'algorithmic_bytes_per_gradient': gbytes, 'achieved_gbs': gbytes / dt / 1e9,
+                'frac_of_hbm': gbytes / dt / 1e9 / _peaks()[0],
                 'grads_per_s': 1.0 / dt, 'params': npar, 'peak_hbm_gib': peak,
                 'forward_passes': fn.program.forward.npasses, 'backward_passes': len(fn.program.back.passes)})
     # accuracy of complex64 against complex128, same structure at 30 qubits

@@ -15,6 +15,8 @@
 // Circuits of <= 2^RES amplitudes keep psi and lambda resident in shared memory
 // for all four steps (no HBM traffic); larger ones stream tiles of a per-CTA
 // workspace in HBM through shared memory pass by pass.
+#include <cstdlib>
+
 #include "desv_common.cuh"
 #include "stage_ops.cuh"
 #include "grad_ops.cuh"
@@ -181,8 +183,11 @@ __device__ void batch_pass(T *gpsi, T *glam, T *spsi, T *slam, bool resident, co
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_vqe(desv_batch_args args, int *queue) {
+// MINB: CTAs per SM the register allocation is bounded for (2: 128 registers
+// a thread, two CTAs per SM; 1: up to 255 registers, no spills in the adjoint
+// stages, one CTA per SM).  DESV_BATCH_MINB picks the instance at run time.
+template <typename T, int MINB>
+__global__ void __launch_bounds__(BATCH_THREADS, MINB) k_batch_vqe(desv_batch_args args, int *queue) {
     extern __shared__ __align__(128) unsigned char smem[];
     T *sA = reinterpret_cast<T *>(smem);
     T *sB = sA + (1u << BATCH_K);
@@ -292,15 +297,36 @@ static size_t batch_smem_bytes(int dtype) {
     return 2 * ((size_t)1 << BATCH_K) * es + (size_t)BATCH_NW * BATCH_MAXP * 8 + 32 * 8;
 }
 
+// CTAs per SM of the register bound (DESV_BATCH_MINB=1 or 2, read once)
+static int batch_minb() {
+    static int v = 0;
+    if (!v) {
+        const char *e = getenv("DESV_BATCH_MINB");
+        v = (e && e[0] == '1') ? 1 : 2;
+    }
+    return v;
+}
+
+template <typename T, int MINB> static void batch_attrs_t(size_t smem) {
+    cudaFuncSetAttribute(k_batch_vqe<T, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 static void batch_attrs(int dtype) {
     static bool done[2][64] = {{false}};
     int dev = 0;
     cudaGetDevice(&dev);
     if (done[dtype][dev & 63]) return;
     const size_t smem = batch_smem_bytes(dtype);
-    if (dtype == DESV_C64) cudaFuncSetAttribute(k_batch_vqe<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else cudaFuncSetAttribute(k_batch_vqe<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool one = batch_minb() == 1;
+    if (dtype == DESV_C64) { if (one) batch_attrs_t<float2, 1>(smem); else batch_attrs_t<float2, 2>(smem); }
+    else { if (one) batch_attrs_t<double2, 1>(smem); else batch_attrs_t<double2, 2>(smem); }
     done[dtype][dev & 63] = true;
+}
+
+template <typename T, int MINB> static int batch_occ(size_t smem) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_vqe<T, MINB>, BATCH_THREADS, smem);
+    return b;
 }
 
 int batch_max_ctas(int dtype) {
@@ -309,10 +335,10 @@ int batch_max_ctas(int dtype) {
     cudaGetDevice(&dev);
     if (cache[dtype][dev & 63]) return cache[dtype][dev & 63];
     batch_attrs(dtype);
-    int b = 0;
     const size_t smem = batch_smem_bytes(dtype);
-    if (dtype == DESV_C64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_vqe<float2>, BATCH_THREADS, smem);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_vqe<double2>, BATCH_THREADS, smem);
+    const bool one = batch_minb() == 1;
+    const int b = dtype == DESV_C64 ? (one ? batch_occ<float2, 1>(smem) : batch_occ<float2, 2>(smem))
+                                    : (one ? batch_occ<double2, 1>(smem) : batch_occ<double2, 2>(smem));
     cache[dtype][dev & 63] = (b > 0 ? b : 1) * sm_count();
     return cache[dtype][dev & 63];
 }
@@ -320,8 +346,14 @@ int batch_max_ctas(int dtype) {
 int batch_vqe(int dtype, const desv_batch_args &args, int *queue, int grid, cudaStream_t st) {
     batch_attrs(dtype);
     const size_t smem = batch_smem_bytes(dtype);
-    if (dtype == DESV_C64) k_batch_vqe<float2><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
-    else k_batch_vqe<double2><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
+    const bool one = batch_minb() == 1;
+    if (dtype == DESV_C64) {
+        if (one) k_batch_vqe<float2, 1><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
+        else k_batch_vqe<float2, 2><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
+    } else {
+        if (one) k_batch_vqe<double2, 1><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
+        else k_batch_vqe<double2, 2><<<grid, BATCH_THREADS, smem, st>>>(args, queue);
+    }
     return check_launch("batched VQE");
 }
 
