@@ -318,8 +318,8 @@ def run_headline(args, ws, local):
     specialised = rot is None and jit.enabled(n)
     t_c = time.perf_counter()
     if rot is not None:
-        kernels = rot.prog.compile(torch.cuda.current_device())
         blocks = rot.blocks()
+        kernels = rot.prog.pass_kernels(torch.cuda.current_device(), blocks)
         rows = rot.prog.rows
     else:
         ops_t, mats_t = plan.device_arrays(dev)

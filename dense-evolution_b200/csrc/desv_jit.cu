@@ -347,7 +347,7 @@ extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile
     *handle = nullptr;
     if (tile_bits < ROT_REG_BITS + 4 || tile_bits > 12)
         return fail(DESV_EINVAL, "rotation pass load: tile_bits must be in [9, 12]");
-    if (nbuf < 2 || nbuf > 3) return fail(DESV_EINVAL, "rotation pass load: nbuf must be 2 or 3");
+    if (nbuf < 1 || nbuf > 3) return fail(DESV_EINVAL, "rotation pass load: nbuf must be 1, 2 or 3");
     if (param_floats < 1 || param_floats > ROT_MAX_PARAM_FLOATS)
         return fail(DESV_EINVAL, "rotation pass load: parameter block size out of range");
     if (!api().ok) return fail(DESV_EUNSUPPORTED, "jit: " + api().why);

@@ -48,6 +48,21 @@ __device__ __forceinline__ void rot(float2 (&a)[ROT_NA], float t, float c, float
     }
 }
 
+// The tangent form alone: the pass variant run when every rotation of the
+// call takes the tangent form (the usual case), without the general form's
+// code, which doubles the size of a pass.
+template <int S>
+__device__ __forceinline__ void rot_t(float2 (&a)[ROT_NA], float t) {
+    const float2 pt = make_float2(t, t), nt = make_float2(-t, -t);
+#pragma unroll
+    for (int j = 0; j < ROT_NA; ++j) {
+        if (j & (1 << S)) continue;
+        const float2 x0 = a[j], x1 = a[j | (1 << S)];
+        a[j] = __ffma2_rn(nt, x1, x0);
+        a[j | (1 << S)] = __ffma2_rn(pt, x0, x1);
+    }
+}
+
 // Shared-memory and global accesses of the generated stages.  With
 // DESV_ROT_CHECK defined (a diagnostic build of a pass) every index is checked
 // against its array first; an access out of range is skipped and recorded in
@@ -101,7 +116,8 @@ __device__ __forceinline__ void flip(float2 &v, uint32_t w) {
 // its stage code reads the per-call values straight from the kernel's
 // parameter block): ring slots of SLOT amplitudes hold the natural layout of
 // a 2^K tile as the bulk copies leave it, with room for the padded layout the
-// stages re-lay it into.  Loads run NBUF-1 tiles ahead.
+// stages re-lay it into.  Loads run NBUF-1 tiles ahead; with one slot the
+// next tile's load starts once the last stage has read the slot (release).
 template <int K, int NBUF, uint32_t SLOT> struct RotRing {
     // every slot must start on a 16-byte boundary (bulk-copy destinations) and
     // hold the padded layout of a tile
@@ -136,7 +152,7 @@ template <int K, int NBUF, uint32_t SLOT> struct RotRing {
         tstride = tile_base(geom, gridDim.x);
         lbase = cbase = tile_base(geom, blockIdx.x);
         __syncthreads();
-        for (uint32_t i = 0; i < NBUF - 1 && i < cnt; ++i) issue(i);
+        for (uint32_t i = 0; i < (NBUF > 1 ? NBUF - 1 : 1) && i < cnt; ++i) issue(i);
     }
     __device__ __forceinline__ uint64_t next(uint64_t b) const { return ((b | ~rmask) + tstride) & rmask; }
     __device__ __forceinline__ float2 *slot(uint32_t i) const { return bufs + (size_t)(i % NBUF) * SLOT; }
@@ -159,16 +175,23 @@ template <int K, int NBUF, uint32_t SLOT> struct RotRing {
             bulk_g2s(dst, from, chunk_bytes, &full[sl]);
         }
     }
-    // Wait for tile i and start the load NBUF-1 tiles ahead (into the slot of
-    // tile i-1, whose stages are done: the caller ends every tile with a
-    // barrier).  Returns false (for every thread) if a bounded wait gave up.
+    // Wait for tile i and, with NBUF >= 2, start the load NBUF-1 tiles ahead
+    // (into the slot of tile i-1, whose stages are done: the caller ends every
+    // tile with a barrier).  Returns false (for every thread) if a bounded wait
+    // gave up.
     __device__ __forceinline__ bool begin(uint32_t i, uint64_t &tb) {
         const bool waited = mbar_wait_bounded(&full[i % NBUF], (i / NBUF) & 1u);
         if (!__syncthreads_and(waited)) return false;
-        if (i + NBUF - 1 < cnt) issue(i + NBUF - 1);
+        if (NBUF > 1 && i + NBUF - 1 < cnt) issue(i + NBUF - 1);
         tb = cbase;
         cbase = next(cbase);
         return true;
+    }
+    // With one slot: the last stage of tile i has read the slot into registers
+    // (the caller has passed a barrier), so the load of tile i+1 can overwrite
+    // it while the last stage computes and stores to HBM.
+    __device__ __forceinline__ void release(uint32_t i) {
+        if (NBUF == 1 && i + 1 < cnt) issue(i + 1);
     }
     // after a failed wait: let the loads still in flight land (bounded)
     __device__ __forceinline__ void drain(uint32_t i) {

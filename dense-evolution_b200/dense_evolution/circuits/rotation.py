@@ -14,9 +14,15 @@ primitives on index bits (qubit q is bit n-1-q), plus one global factor:
   single-qubit gates.  On the device it runs in tangent form,
   x0 -= t x1, x1 += t x0 with t = s / c, which is ONE packed FP32
   instruction (fma.rn.f32x2) per amplitude; the cosines are collected into
-  a per-pass scale that a later multiply applies.  Where |t| > TMAX the
-  general form c x0 - s x1 (two instructions) is used instead; that choice
-  is made per call from the angles, so new angles never need a recompile.
+  a per-pass scale that a later multiply applies.  The tangent form keeps
+  FP32's relative accuracy for any finite t: each output is one fused
+  multiply-add, rounded once, and the pass-end factor 1/prod(1/c) restores
+  the scale exactly up to rounding.  Where |t| > TMAX (cos = 0, as in an X
+  gate) or the pending scale would pass SCALE_LIMIT, the general form
+  c x0 - s x1 (two instructions) is used instead.  That choice is made per
+  call from the angles: a pass has a tangent-only kernel for the calls that
+  need no general form and a kernel with a run-time form flag per rotation
+  for the rest, so new angles never change the plan.
 * ``PH(b)`` -- a diagonal diag(1, e^{ia}) on bit b: the outer ZYZ factors
   and every diagonal single-qubit gate.  Phases commute with every other
   diagonal, so the phases of a bit are merged and moved to just before the
@@ -63,11 +69,15 @@ from .gates import GATES
 
 RB = 5                 # register bits per stage (32 amplitudes per thread)
 LOW_FIXED = 5          # index bits 0..LOW_FIXED-1 are in every tile (contiguous bulk-copy runs)
-TMAX = 16.0            # tangent form while |tan| <= TMAX
+TMAX = 2.0 ** 20       # tangent form while |tan| <= TMAX (FP32 keeps its relative accuracy; see materialize)
 SCALE_LIMIT = 2.0 ** 60  # pending tangent scale above which rotations switch to the general form
 MAX_ROTS_PER_PASS = 32  # measured on the 30-qubit, 40-layer brick circuit: 24 -> 246 ms, 32 -> 233, 48 -> 236
 PAD_SHIFT = 4          # padded stage layout: physical = i + (i >> 4)
-NBUF = 2               # ring slots per CTA: 2 -> three CTAs (12 warps) per SM, 233 ms; 3 -> two CTAs, 274 ms
+# ring slots per CTA, measured on the 30-qubit, 40-layer brick circuit: 1 -> four CTAs (16 warps)
+# per SM, 207 ms (the next tile loads while the last stage computes and stores); 2 -> three CTAs,
+# 233 ms; 3 -> two CTAs, 274 ms
+NBUF = 1
+CTAS_PER_SM = {1: 4, 2: 3, 3: 2}   # register bound of the kernel per ring depth (shared memory allows as many)
 
 
 def tuning() -> Tuple[int, int]:
@@ -75,8 +85,8 @@ def tuning() -> Tuple[int, int]:
     overridden by DESV_ROT_MAX_ROTS / DESV_ROT_NBUF (for tuning sweeps)."""
     cap = int(os.environ.get('DESV_ROT_MAX_ROTS', MAX_ROTS_PER_PASS))
     nb = int(os.environ.get('DESV_ROT_NBUF', NBUF))
-    if cap < 1 or nb not in (2, 3):
-        raise ValueError('DESV_ROT_MAX_ROTS must be >= 1 and DESV_ROT_NBUF 2 or 3')
+    if cap < 1 or nb not in (1, 2, 3):
+        raise ValueError('DESV_ROT_MAX_ROTS must be >= 1 and DESV_ROT_NBUF 1, 2 or 3')
     return cap, nb
 
 _H = GATES['h']
@@ -919,8 +929,12 @@ def _f(x: float) -> str:
     return repr(float(x)) + 'f'
 
 
-def pass_source(plan: 'RotationPlan', pidx: int, nbuf: Optional[int] = None) -> str:
-    """CUDA source of one rotation pass (entry point desv_rot_kernel)."""
+def pass_source(plan: 'RotationPlan', pidx: int, nbuf: Optional[int] = None, general: bool = False) -> str:
+    """CUDA source of one rotation pass (entry point desv_rot_kernel).  With
+    general=False every rotation is compiled in tangent form only (the variant
+    for calls whose rotations all take it); with general=True each rotation
+    picks its form from its form flag at run time.  Both read the same
+    parameter block."""
     ps = plan.passes[pidx]
     nbuf = nbuf or plan.nbuf
     K, L, high = ps.K, ps.L, ps.high
@@ -931,7 +945,7 @@ def pass_source(plan: 'RotationPlan', pidx: int, nbuf: Optional[int] = None) -> 
     lines = ([f'#define DESV_ROT_CHECK 1', f'#define ROT_SLOT_ELEMS {slot_elems(K)}u'] if check else []) + \
             ['#include "rot_pass.cuh"', 'using namespace desv;',
              f'struct RotParams {{ float v[{ps.n_floats}]; }};',
-             f'extern "C" __global__ void __launch_bounds__({nthreads}, {3 if nbuf == 2 else 2})',
+             f'extern "C" __global__ void __launch_bounds__({nthreads}, {CTAS_PER_SM[nbuf]})',
              'desv_rot_kernel(float2 *__restrict__ sv, const TileGeom g, const RotParams P) {',
              '    extern __shared__ __align__(128) unsigned char smem[];',
              '    const uint32_t t = threadIdx.x;',
@@ -961,12 +975,18 @@ def pass_source(plan: 'RotationPlan', pidx: int, nbuf: Optional[int] = None) -> 
         else:
             lines.append('            const uint32_t pb = lb + (lb >> 4);')
             lines += [f'            ROT_SLD(a[{j}], s, pb + {padded(offs[j])}u);' for j in range(NA)]
+        if last and nbuf == 1:
+            lines.append('            __syncthreads();  // the slot is read: the next tile may load into it')
+            lines.append('            ring.release(i);')
         if need_gi:
             lines.append(f'            const uint64_t gi = tb | {glob};')
         for kind, x in st.items:
             if kind == 'rot':
                 pi, slot, off = x
-                lines.append(f'            rot<{slot}>(a, pv[{off}], pv[{off + 1}], pv[{off + 2}], pv[{off + 3}]);')
+                if general:
+                    lines.append(f'            rot<{slot}>(a, pv[{off}], pv[{off + 1}], pv[{off + 2}], pv[{off + 3}]);')
+                else:
+                    lines.append(f'            rot_t<{slot}>(a, pv[{off}]);')
             else:
                 lines += ['            ' + ln for ln in _group_code(x)]
         if last:
@@ -985,8 +1005,9 @@ def pass_source(plan: 'RotationPlan', pidx: int, nbuf: Optional[int] = None) -> 
             lines.append('            fence_proxy_async_smem();')
             lines.append('            __syncthreads();')
         lines.append('        }')
-    lines += ['        __syncthreads();  // the slot is free for the load NBUF-1 tiles ahead',
-              '    }',
+    if nbuf > 1:
+        lines.append('        __syncthreads();  // the slot is free for the load NBUF-1 tiles ahead')
+    lines += ['    }',
               '    if (i < ring.cnt) ring.drain(i);',
               '}', '']
     src = '\n'.join(lines)
@@ -1126,12 +1147,21 @@ def _load(src: str, K: int, nbuf: int, n_floats: int, device: int) -> _RotKernel
 
 
 class RotationProgram:
-    """A rotation plan with its compiled kernels, run on CUDA statevectors."""
+    """A rotation plan with its compiled kernels, run on CUDA statevectors.
+
+    Every pass has two kernels over the same parameter block: the tangent-only
+    variant, compiled up front, and the variant that picks each rotation's form
+    at run time, compiled the first time a call needs the general form in that
+    pass (a rotation with cos = 0, as in an X gate, or a pending scale past
+    SCALE_LIMIT)."""
 
     def __init__(self, plan: RotationPlan):
         self.plan = plan
         self.sources = [pass_source(plan, i) for i in range(len(plan.passes))]
         self.kernels: Dict[int, list] = {}
+        self.general: Dict[Tuple[int, int], _RotKernel] = {}
+        vp = plan._prepare_values()
+        self.form_idx = [pos - int(vp['offs'][i]) + 3 for i, (_, pos) in enumerate(vp['rots'])]
         rows = []
         from .. import _native as N
         for ps in plan.passes:
@@ -1153,11 +1183,29 @@ class RotationProgram:
                 self.kernels[device] = list(ex.map(lambda j: _load(j[0], j[1], nb, j[2], device), jobs))
         return self.kernels[device]
 
+    def needs_general(self, i: int, block: np.ndarray) -> bool:
+        """Whether pass i's parameter block sets the general form for a rotation."""
+        fi = self.form_idx[i]
+        return bool(len(fi)) and bool(np.any(block[fi] != 0))
+
+    def pass_kernels(self, device: int, blocks: list) -> list:
+        """The kernel of every pass for these parameter blocks."""
+        kernels = list(self.compile(device))
+        for i, b in enumerate(blocks):
+            if self.needs_general(i, b):
+                key = (device, i)
+                if key not in self.general:
+                    ps = self.plan.passes[i]
+                    self.general[key] = _load(pass_source(self.plan, i, general=True), ps.K, self.plan.nbuf,
+                                              ps.n_floats, device)
+                kernels[i] = self.general[key]
+        return kernels
+
     def run_blocks(self, sv_ptr: int, device: int, stream: int, blocks: list):
         """Every pass over the complex64 state at sv_ptr with these parameter blocks."""
         import ctypes
         from .. import _native as N
-        kernels = self.compile(device)
+        kernels = self.pass_kernels(device, blocks)
         lib = N.lib()
         st = ctypes.c_void_p(stream)
         base = self.rows.ctypes.data

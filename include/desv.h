@@ -329,7 +329,7 @@ int desv_swap_blocks(void *a, void *b, size_t bytes, void *stream);
  * rotations and diagonals; replaces the per-gate scan step of
  * circuits/compiler.py:136-355 like desv_jit_pass).  desv_rot_load compiles
  * one pass's generated source (entry point desv_rot_kernel, 2^(tile_bits-5)
- * threads, nbuf ring slots (2 or 3, as the source was generated for), a
+ * threads, nbuf ring slots (1, 2 or 3, as the source was generated for), a
  * by-value parameter block of param_floats floats) for sm_100a;
  * desv_rot_pass runs it over the 2^n complex64 state sv with the pass's tile
  * geometry (tile_bits, low_bits, high[]; op_begin / op_end are not used) and

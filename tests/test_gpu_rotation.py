@@ -127,3 +127,27 @@ def test_c_abi_rejects_bad_calls():
     r = lib.desv_rot_pass(k.handle, ctypes.c_void_p(sv.data_ptr() + 8), n, ctypes.c_void_p(row.ctypes.data),
                           blk.ctypes.data_as(ctypes.c_void_p), len(blk), st)
     assert r == N.DESV_EINVAL
+
+
+def test_general_form_variant():
+    """A call whose rotation has cos = 0 (ry(pi) alone on its qubit) runs the pass
+    variant with the run-time form choice; a later call of the same structure
+    with generic angles runs the tangent-only variant.  Both match the oracle."""
+    from dense_evolution.workloads import brick_u3_circuit
+    n = 20
+    base = brick_u3_circuit(n, 2, seed=5)
+    c1 = base + [('ry', 3, float(np.pi)), ('ry', 7, float(np.pi))]
+    c2 = base + [('ry', 3, 0.37), ('ry', 7, 1.1)]
+    for circ, general in ((c1, True), (c2, False)):
+        plan, sv = _run(circ, n)
+        prog = plan.rotation.prog
+        blocks = plan.rotation.blocks()
+        flags = [prog.needs_general(i, b) for i, b in enumerate(blocks)]
+        if general:
+            assert any(flags)
+        ref = O.run_circuit(O.zero_state(n), n, circ)
+        assert np.max(np.abs(sv.cpu().numpy().astype(np.complex128) - ref)) <= 1e-5
+        if general:
+            assert prog.general, 'the general variant was compiled for this call'
+        else:
+            assert not any(flags)

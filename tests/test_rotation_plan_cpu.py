@@ -159,14 +159,15 @@ def test_headline_schedule_shape():
 
 @pytest.mark.skipif(shutil.which('nvcc') is None and not os.path.exists('/usr/local/cuda/bin/nvcc'),
                     reason='nvcc not installed')
-def test_generated_sources_compile(tmp_path):
+@pytest.mark.parametrize('nbuf', [1, 2, 3])
+def test_generated_sources_compile(tmp_path, nbuf):
     nvcc = shutil.which('nvcc') or '/usr/local/cuda/bin/nvcc'
     n = 22
     plan = R.RotationPlan(QuantumTranspiler.transpile(_mixed_circuit(n, 200, 5)), n, 12, max_rots=24)
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     for i in (0, len(plan.passes) - 1):
         src = tmp_path / f'p{i}.cu'
-        src.write_text(R.pass_source(plan, i))
+        src.write_text(R.pass_source(plan, i, nbuf=nbuf))
         r = subprocess.run([nvcc, '-gencode', 'arch=compute_100a,code=sm_100a', '-std=c++17', '-c', str(src),
                             '-o', str(tmp_path / f'p{i}.o'), '-I', os.path.join(root, 'dense-evolution_b200', 'csrc'),
                             '-I', os.path.join(root, 'include')], capture_output=True, text=True)
@@ -182,13 +183,13 @@ def test_generated_sources_compile_with_nvrtc():
     from dense_evolution.circuits import jit
     n = 21
     plan = R.RotationPlan(QuantumTranspiler.transpile(_mixed_circuit(n, 150, 8)), n, 12, max_rots=24)
-    for check in ('0', '1'):
+    for check, general in (('0', False), ('0', True), ('1', False), ('1', True)):
         os.environ['DESV_ROT_CHECK'] = check
         try:
             for i in (0, len(plan.passes) - 1):
                 log = ctypes.create_string_buffer(16384)
-                r = N.lib().desv_jit_compile_check(R.pass_source(plan, i).encode(), jit.INCLUDE_PATH.encode(), log,
-                                                   16384)
+                r = N.lib().desv_jit_compile_check(R.pass_source(plan, i, general=general).encode(),
+                                                   jit.INCLUDE_PATH.encode(), log, 16384)
                 if r == N.DESV_EUNSUPPORTED:
                     pytest.skip('NVRTC not available: ' + N.last_error())
                 assert r == 0, log.value.decode()[-3000:]
