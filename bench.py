@@ -373,19 +373,23 @@ def run_headline(args, ws, local):
     # ---- end to end through the public API: fresh seeded angles every step,
     # circuit transpile + fusion + H2D of the op/matrix tables, run, <Z_i> read back
     sim = de.DenseSVSimulator(n, use_float32=True)
-    e2e_times, h2d = [], 0
+    e2e_times, h2d, parts = [], 0, []
     for i in range(0 if args.skip_e2e else args.warmup + args.steps):
         c = brick_u3_circuit(n, layers, SEED + 1 + i)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sim.set_initial_state(None)
         plan_i = sim.compile(c)
+        t1 = time.perf_counter()
         sim.run_circuit(c)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
         sim.expectation_z()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)
+            parts.append((t1 - t0, t2 - t1, t0 + dt - t2))
             if plan_i.rotation is not None:
                 h2d = int(sum(b.nbytes for b in plan_i.rotation.blocks()))
             else:
@@ -424,6 +428,9 @@ def run_headline(args, ws, local):
                      'max_launch_ms': float(per_pass.max())},
         'e2e': {'value': e2e_value, 'unit': 'GB/s', 'h2d_bytes_per_step': h2d,
                 'd2h_bytes_per_step': (n + 1) * 8, 'ms_per_step': e2e_step * 1e3,
+                'breakdown_ms': ({k: float(v) * 1e3 for k, v in zip(
+                    ('host_plan (transpile, plan lookup, angle values)', 'run (values upload + passes)',
+                     'readout (<Z_i> pass + read back)'), np.mean(parts, axis=0))} if parts else None),
                 'path': 'DenseSVSimulator.run_circuit (new angles each step: transpile + fusion + upload) + '
                         'expectation_z()'},
         'gpu_launches': args.steps * npasses,

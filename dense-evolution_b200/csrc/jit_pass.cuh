@@ -97,6 +97,88 @@ __device__ __forceinline__ double jit_grad_lane(const T (&a)[16], const T (&b)[1
     }
     return (double)acc;
 }
+// Probes whose generator is known when the pass is generated (the generators
+// of rx, ry, rz, p, cp and crz do not depend on the angle).  Four partial sums
+// keep the multiply-adds independent.
+//
+// Y type, G = [[0, -h], [h, 0]] with h real (ry): Re sum conj(b) G a over the
+// pairs on register slot S is h (Re conj(b1) a0 - Re conj(b0) a1).
+template <int S, int CS, typename T>
+__device__ __forceinline__ double jit_grad_y(const T (&a)[16], const T (&b)[16], decltype(T().x) h) {
+    typedef decltype(T().x) R;
+    R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if ((j >> S) & 1) continue;
+        if (CS >= 0 && !((j >> CS) & 1)) continue;
+        const int j1 = j | (1 << S);
+        s0 = fma(b[j1].x, a[j].x, s0);
+        s1 = fma(b[j1].y, a[j].y, s1);
+        s2 = fma(b[j].x, a[j1].x, s2);
+        s3 = fma(b[j].y, a[j1].y, s3);
+    }
+    return (double)(((s0 + s1) - (s2 + s3)) * h);
+}
+// X type, G = [[0, -i h], [-i h, 0]] with h real (rx): h (Im conj(b0) a1 + Im conj(b1) a0),
+// Im conj(b) a = b.x a.y - b.y a.x.
+template <int S, int CS, typename T>
+__device__ __forceinline__ double jit_grad_x(const T (&a)[16], const T (&b)[16], decltype(T().x) h) {
+    typedef decltype(T().x) R;
+    R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if ((j >> S) & 1) continue;
+        if (CS >= 0 && !((j >> CS) & 1)) continue;
+        const int j1 = j | (1 << S);
+        s0 = fma(b[j].x, a[j1].y, s0);
+        s1 = fma(b[j].y, a[j1].x, s1);
+        s2 = fma(b[j1].x, a[j].y, s2);
+        s3 = fma(b[j1].y, a[j].x, s3);
+    }
+    return (double)(((s0 - s1) + (s2 - s3)) * h);
+}
+// Imaginary diagonal, G = diag(i h_k) with k = bit(ga) + 2 bit(gb) (rz, p, cp,
+// crz): Re conj(b) (i h) a = h (b.y a.x - b.x a.y), summed per class k.  The
+// register part of k is a compile-time constant per amplitude; the bits on
+// thread-fixed positions (fa, fb) complete it per thread.
+template <int SA, int SB, typename T>
+__device__ __forceinline__ double jit_grad_dim(const T (&a)[16], const T (&b)[16], decltype(T().x) h0,
+                                               decltype(T().x) h1, decltype(T().x) h2, decltype(T().x) h3, int fa,
+                                               int fb) {
+    typedef decltype(T().x) R;
+    R s[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int kr = (SA >= 0 ? ((j >> SA) & 1) : 0) | (SB >= 0 ? (((j >> SB) & 1) << 1) : 0);
+        s[kr] = fma(b[j].y, a[j].x, s[kr]);
+        s[kr] = fma(-b[j].x, a[j].y, s[kr]);
+    }
+    const int kf = (SA >= 0 ? 0 : fa) | (SB >= 0 ? 0 : (fb << 1));
+    R acc = 0;
+#pragma unroll
+    for (int kr = 0; kr < 4; ++kr) {
+        if ((SA < 0 && (kr & 1)) || (SB < 0 && (kr & 2))) continue;
+        const int k = kr | kf;   // selects, not an indexed array: no local memory
+        const R hk = k == 0 ? h0 : k == 1 ? h1 : k == 2 ? h2 : h3;
+        acc = fma(hk, s[kr], acc);
+    }
+    return (double)acc;
+}
+
+// Controlled X on register slot S (control register slot CS, or none): a
+// swap of register pairs, no arithmetic.
+template <int S, int CS, typename T>
+__device__ __forceinline__ void swap_reg(T (&a)[16]) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if ((j >> S) & 1) continue;
+        if (CS >= 0 && !((j >> CS) & 1)) continue;
+        const T t = a[j];
+        a[j] = a[j | (1 << S)];
+        a[j | (1 << S)] = t;
+    }
+}
+
 template <int SA, int SB, typename T>
 __device__ __forceinline__ double jit_grad_diag(const T (&a)[16], const T (&b)[16], const T *mp, int fa, int fb) {
     const T d0 = mp[0], d1 = mp[1], d2 = mp[2], d3 = mp[3];

@@ -20,6 +20,7 @@ import hashlib
 import os
 import threading
 from concurrent.futures import ThreadPoolExecutor
+from typing import List, Optional
 
 import numpy as np
 
@@ -29,7 +30,7 @@ _PKG = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 CSRC = os.path.join(_PKG, 'csrc')
 INCLUDE = os.path.join(os.path.dirname(_PKG), 'include')
 INCLUDE_PATH = CSRC + ':' + INCLUDE
-V_BREAL = 5
+V_ANTI, V_BREAL = 4, 5   # m1_variant codes of stage_ops.cuh
 PRED = 0x8000
 
 
@@ -58,6 +59,36 @@ def _signs_code(words: np.ndarray, w0: int, npairs: int) -> str:
     return f'sign_flips(a, {" ^ ".join(terms)});'
 
 
+def mat_values(words: Optional[np.ndarray], off: int, wpe: int, count: int = 4) -> Optional[List[complex]]:
+    """The complex values mats[off:off+count] from the pool's 32-bit words
+    (wpe words per element: 2 for complex64, 4 for complex128)."""
+    if words is None or (off + count) * wpe > len(words):
+        return None
+    w = np.ascontiguousarray(words[off * wpe:(off + count) * wpe])
+    v = w.view(np.float32 if wpe == 2 else np.float64)
+    return [complex(float(v[2 * i]), float(v[2 * i + 1])) for i in range(count)]
+
+
+def _is_x(m: Optional[List[complex]]) -> bool:
+    return m is not None and m[0] == 0 and m[1] == 1 and m[2] == 1 and m[3] == 0
+
+
+def value_key(ops: np.ndarray, mats_host: np.ndarray) -> str:
+    """Digest of the pool values the generated sources depend on (X matrices
+    of anti-diagonal records become register swaps; generator values become
+    immediates): with the op records, it keys a cache of generated kernels."""
+    pool = np.ascontiguousarray(mats_host)
+    if not len(ops) or not len(pool):
+        return ''
+    c = ops['code'].astype(np.int64) & 0x7FFF
+    anti = ((c >= 1) & (c <= 20) & ((c - 1) % 5 == V_ANTI)) | ((c >= 21) & (c <= 52) & ((c - 21) % 2 == 0))
+    sel = ((ops['kind'] == N.OP_GRAD) | (anti & (ops['kind'] != N.OP_STAGE))).nonzero()[0]
+    if not len(sel):
+        return ''
+    idx = ops['mat'][sel].astype(np.int64)[:, None] + np.arange(4)
+    return hashlib.sha1(pool[np.clip(idx, 0, len(pool) - 1)].tobytes()).hexdigest()
+
+
 def _op_code(o, words: np.ndarray, wpe: int) -> str:
     c = int(o['code'])
     pred, c = c & PRED, c & 0x7FFF
@@ -67,11 +98,17 @@ def _op_code(o, words: np.ndarray, wpe: int) -> str:
     s1 = int(o['s1']) & 0xFF
     if 1 <= c <= 20:
         S, V = divmod(c - 1, 5)
-        call = f'm1_reg<{S}, {V}, -1>(a, load_m22({mp}));'
+        if V == V_ANTI and _is_x(mat_values(words, off, wpe)):
+            call = f'swap_reg<{S}, -1>(a);'
+        else:
+            call = f'm1_reg<{S}, {V}, -1>(a, load_m22({mp}));'
     elif 21 <= c <= 52:
         x = c - 21
         S, CS = divmod(x // 2, 4)
-        call = f'm1_ctl_case<{S}, {CS}>(a, load_m22({mp}), {"false" if x & 1 else "true"});'
+        if not x & 1 and S != CS and _is_x(mat_values(words, off, wpe)):
+            call = f'swap_reg<{S}, {CS}>(a);'
+        else:
+            call = f'm1_ctl_case<{S}, {CS}>(a, load_m22({mp}), {"false" if x & 1 else "true"});'
     elif 53 <= c <= 57:
         call = f'm1_lane_free<{c - 53}>(a, load_m22({mp}), {s0 - 16}, lane);'
     elif 58 <= c <= 107:
@@ -111,18 +148,30 @@ def _op_code(o, words: np.ndarray, wpe: int) -> str:
     return call
 
 
-def _grad_code(o) -> str:
-    """A GRAD probe with its generator's placement compiled in (grad_term's forms)."""
+def _grad_code(o, words: Optional[np.ndarray] = None, wpe: int = 2) -> str:
+    """A GRAD probe with its generator's placement compiled in (grad_term's
+    forms); generators of the known shapes (ry: real antisymmetric, rx: -i h X,
+    rz / p / cp / crz: imaginary diagonal) get probes with their values as
+    immediates and no complex products."""
     mp = f'mats + {int(o["mat"])}'
     cs = int(o['cslot'])
+    g = mat_values(words, int(o['mat']), wpe)
     if int(o['s1']) == 1:                          # diagonal generator over ga / gb
         sa, sb = int(o['sa']), int(o['sb'])
         ga, gb = int(o['ga']), int(o['gb'])
         fa = '0' if ga == 0xFF else f'(int)((tg >> {ga}) & 1ull)'
         fb = '0' if gb == 0xFF else f'(int)((tg >> {gb}) & 1ull)'
-        call = f'jit_grad_diag<{sa}, {sb}>(a, b, {mp}, {fa}, {fb})'
+        if g is not None and all(v.real == 0 for v in g):
+            hs = ', '.join(repr(float(v.imag)) for v in g)
+            call = f'jit_grad_dim<{sa}, {sb}>(a, b, {hs}, {fa}, {fb})'
+        else:
+            call = f'jit_grad_diag<{sa}, {sb}>(a, b, {mp}, {fa}, {fb})'
     elif int(o['s0']) >= 16:                       # lane-bit generator
         call = f'jit_grad_lane<{cs}>(a, b, {mp}, {int(o["s0"]) - 16}, lane)'
+    elif g is not None and g[0] == 0 and g[3] == 0 and g[1].imag == 0 and g[2].imag == 0 and g[1] == -g[2]:
+        call = f'jit_grad_y<{int(o["s0"])}, {cs}>(a, b, {float(g[2].real)!r})'
+    elif g is not None and g[0] == 0 and g[3] == 0 and g[1].real == 0 and g[2].real == 0 and g[1] == g[2]:
+        call = f'jit_grad_x<{int(o["s0"])}, {cs}>(a, b, {-float(g[1].imag)!r})'
     else:
         call = f'jit_grad_reg<{int(o["s0"])}, {cs}>(a, b, {mp})'
     pred = f'(tg & {_hex(o["cmask"])}) == {_hex(o["cval"])}'
@@ -162,12 +211,12 @@ def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: 
         for q in range(k + 1, k + 1 + cnt):
             o = ops[q]
             if int(o['kind']) == N.OP_GRAD:
-                lines.append('            ' + _grad_code(o))
+                lines.append('            ' + _grad_code(o, words, wpe))
                 continue
             code = _op_code(o, words, wpe)
             if code:
                 lines.append('            ' + code)
-                lines.append('            ' + code.replace('(a, ', '(b, '))
+                lines.append('            ' + code.replace('(a, ', '(b, ').replace('(a);', '(b);'))
         if last:
             lines.append('            S::store_global(a, phi, tg, ctab, L);')
             lines.append('            S::store_global(b, lam, tg, ctab, L);')

@@ -808,17 +808,26 @@ class RotationPlan:
         gang = float(np.sum(np.angle(g[vp['rot_u']]) - p[vp['rot_u']]) + np.sum(np.angle(d0[vp['diag_u']])))
         for sg in scalars:
             gang += sg.value if sg.slot < 0 or theta is None else float(theta[sg.slot])
-        d2_ang = np.zeros((vp['nd2'], 4))
-        for pi, i in vp['d2_idx'].items():
+        # constant two-bit diagonals (cz, the cx / cy rewrites) have the same
+        # angles in every circuit of this structure: computed once per plan
+        if vp.get('d2_const') is None:
+            const = np.zeros((vp['nd2'], 4))
+            cmask = np.zeros(vp['nd2'], bool)
+            for pi, i in vp['d2_idx'].items():
+                gt = d2g[pi]
+                if gt.const is not None:
+                    const[i] = np.angle(np.asarray(gt.const, dtype=np.complex128))
+                    cmask[i] = True
+            vp['d2_const'] = const
+            vp['d2_param'] = [(pi, i) for pi, i in vp['d2_idx'].items() if not cmask[i]]
+        d2_ang = vp['d2_const'].copy()
+        for pi, i in vp['d2_param']:
             gt = d2g[pi]
-            if gt.const is not None:
-                d = np.asarray(gt.const, dtype=np.complex128)
-            else:
-                val = gt.value if gt.slot < 0 or theta is None else float(theta[gt.slot])
-                d = np.asarray(fusion.gate_matrix_of('d2', gt.name, val), dtype=np.complex128)
-            a = np.angle(d)
-            gang += a[0]
-            d2_ang[i] = a - a[0]
+            val = gt.value if gt.slot < 0 or theta is None else float(theta[gt.slot])
+            d2_ang[i] = np.angle(np.asarray(fusion.gate_matrix_of('d2', gt.name, val), dtype=np.complex128))
+        if len(d2_ang):
+            gang += float(d2_ang[:, 0].sum())
+            d2_ang = d2_ang - d2_ang[:, :1]
         src = np.concatenate([ph_ang, d2_ang.reshape(-1), [np.pi]])
         glob = complex(np.exp(1j * gang))
         flat = np.zeros(int(vp['offs'][-1]), dtype=np.float64)

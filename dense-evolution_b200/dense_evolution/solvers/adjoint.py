@@ -122,10 +122,14 @@ class AdjointProgram:
             kb = _adjoint_tile_bits(self.n, dtype)
             specs = fusion.schedule(self.bops, self.n, kb)
             specs = _split_params(specs, self.bops, 1024)
+            if dtype == torch.complex64 and jit.enabled(self.n):
+                specs = _split_ops(specs, SPECIALISED_OPS_PER_PASS)
             self.back = fusion.Packed(self.n, self.bops, specs, adjoint=True)
         else:
             self.back = None
         self._back_dev = None
+        self._map_dev = None
+        self._stage: dict = {}
         self._scratch = None
 
     # ------------------------------------------------------------ helpers
@@ -160,20 +164,27 @@ class AdjointProgram:
         exact too)."""
         if self.dtype != torch.complex64:
             return 1.0
+        n0 = self._initial_norm2(stato_zero)
+        nn = float(self._norm_device(psi)[0].item())
+        return n0 / nn if nn > 0 else 1.0
+
+    @staticmethod
+    def _initial_norm2(stato_zero) -> float:
         if stato_zero is None:
-            n0 = 1.0
-        elif isinstance(stato_zero, torch.Tensor):
-            n0 = float(torch.linalg.vector_norm(stato_zero.detach().to(torch.complex128)).item()) ** 2
-        else:
-            a = np.asarray(stato_zero).astype(np.complex128).reshape(-1)
-            n0 = float(np.vdot(a, a).real)
+            return 1.0
+        if isinstance(stato_zero, torch.Tensor):
+            return float(torch.linalg.vector_norm(stato_zero.detach().to(torch.complex128)).item()) ** 2
+        a = np.asarray(stato_zero).astype(np.complex128).reshape(-1)
+        return float(np.vdot(a, a).real)
+
+    def _norm_device(self, psi: torch.Tensor) -> torch.Tensor:
+        """<psi|psi> in FP64 as a device tensor (element 0), queued only."""
         out = torch.empty(2, dtype=torch.float64, device=psi.device)
         sc = N.scratch(self.n, psi.device)
         N.check(N.lib().desv_norm2(ctypes.c_void_p(psi.data_ptr()), self.n, N.dtype_code(psi),
                                    ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(sc.data_ptr()), sc.numel() * 8,
                                    ctypes.c_void_p(N.stream_ptr())), 'norm')
-        nn = float(out[0].item())
-        return n0 / nn if nn > 0 else 1.0
+        return out
 
     def hamiltonian(self, h):
         """('pauli', PauliPlan) or ('dense', tensor)."""
@@ -201,26 +212,57 @@ class AdjointProgram:
     # ------------------------------------------------------------ gradient
     def gradient(self, theta: np.ndarray, psi: torch.Tensor, lam: torch.Tensor) -> np.ndarray:
         """dE/dtheta by the adjoint method; psi is not modified, lam is consumed."""
+        return self._gradient_device(theta, psi, lam)[:self.nparams].cpu().numpy()
+
+    def _gradient_device(self, theta: np.ndarray, psi: torch.Tensor, lam: torch.Tensor) -> torch.Tensor:
+        """The gradient as a float64 device tensor (launches only, no host read)."""
         mu = psi.clone()
         grad = torch.zeros(max(self.nparams, 1), dtype=torch.float64, device=psi.device)
         if self.back is None:
             self._gradient_per_gate(theta, mu, lam, grad)
         else:
             self._gradient_fused(theta, mu, lam, grad)
-        return grad[:self.nparams].cpu().numpy()
+        return grad
+
+    def _staged(self, name: str, data: np.ndarray, dev) -> torch.Tensor:
+        """data's bytes in a device buffer, copied from a pinned host buffer
+        without blocking the host (stream-ordered after the work already
+        queued); the pinned buffer is reused once its last copy has ended."""
+        raw = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+        nb = max(int(raw.size), 1)
+        ent = self._stage.get(name)
+        if ent is None or ent[0].numel() < nb or ent[1].device != dev:
+            cap = max(nb, 4096)
+            ent = (torch.empty(cap, dtype=torch.uint8, pin_memory=True), torch.empty(cap, dtype=torch.uint8,
+                                                                                      device=dev),
+                   torch.cuda.Event())
+            self._stage[name] = ent
+        host, devbuf, ev = ent
+        ev.synchronize()
+        host[:raw.size].numpy()[:] = raw
+        devbuf[:raw.size].copy_(host[:raw.size], non_blocking=True)
+        ev.record()
+        return devbuf
+
+    def _upload_backward(self, theta, dev):
+        """(key, ops, mats, map, host mats) of the backward passes for theta;
+        the host work and the uploads do not wait for the device, so they
+        overlap forward passes already queued."""
+        key = np.asarray(theta, dtype=np.float64).tobytes()
+        if self._back_dev is not None and self._back_dev[0] == key:
+            return self._back_dev
+        cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
+        mats = self.back.materialize(theta, cdt)
+        ops_t = self._staged('ops', self.back.ops, dev)
+        mats_t = self._staged('mats', mats, dev)
+        if self._map_dev is None or self._map_dev.device != dev:
+            self._map_dev = torch.tensor(self.back.param_map or [0], dtype=torch.int32, device=dev)
+        self._back_dev = (key, ops_t, mats_t, self._map_dev, mats)
+        return self._back_dev
 
     def _gradient_fused(self, theta, mu, lam, grad):
         dev = mu.device
-        key = np.asarray(theta, dtype=np.float64).tobytes()
-        rdt = np.float32 if self.dtype == torch.complex64 else np.float64
-        cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
-        if self._back_dev is None or self._back_dev[0] != key:
-            mats = self.back.materialize(theta, cdt)
-            ops_t = torch.from_numpy(self.back.ops.view(np.uint8).copy()).to(dev)
-            mats_t = torch.from_numpy(mats.view(rdt).copy()).to(dev)
-            map_t = torch.tensor(self.back.param_map or [0], dtype=torch.int32, device=dev)
-            self._back_dev = (key, ops_t, mats_t, map_t, mats)
-        _, ops_t, mats_t, map_t, mats = self._back_dev
+        _, ops_t, mats_t, map_t, mats = self._upload_backward(theta, dev)
         need = int(N.lib().desv_adjoint_scratch_bytes(max(self.back.max_params, 1)))
         if self._scratch is None or self._scratch.numel() * 8 < need:
             self._scratch = torch.empty((need + 7) // 8, dtype=torch.float64, device=dev)
@@ -229,10 +271,11 @@ class AdjointProgram:
             # plan-specialised backward passes (complex64: the complex128 pair of
             # register tiles does not fit the register file); sources, and so
             # kernels, change only with the records' dispatch codes
-            # the sources (and so the kernels) depend only on the op records: reuse
-            # them while the records stay the same (new angles change only values)
+            # the sources (and so the kernels) depend on the op records and on the
+            # pool values of generator and X records (jit.value_key), none of which
+            # change with the angles: reuse them while those stay the same
             import hashlib
-            okey = (hashlib.sha1(self.back.ops.tobytes()).hexdigest(), dev.index)
+            okey = (hashlib.sha1(self.back.ops.tobytes()).hexdigest(), jit.value_key(self.back.ops, mats), dev.index)
             if getattr(self, '_adj_kernels', None) is None or self._adj_kernels[0] != okey:
                 kernels = jit.compile_adjoint(self.back.ops, p, mats, self.dtype == torch.complex64,
                                               dev.index if dev.index is not None else torch.cuda.current_device())
@@ -328,12 +371,37 @@ class AdjointProgram:
         return out, None
 
     def value_and_grad(self, theta, h, stato_zero=None):
-        """(E, dE/dtheta as NumPy float64, psi) without autograd bookkeeping."""
+        """(E, dE/dtheta as NumPy float64, psi) without autograd bookkeeping.
+
+        Everything is queued before the host reads anything: the forward
+        passes, then (on the host, while they run) the backward passes' values
+        and their upload, then <psi|psi>, lambda = H psi with E, and the backward
+        sweep; one read at the end brings E, the norm and the gradient back."""
         th = _as_theta(theta)
+        if self.back is None:
+            psi = self.forward_state(th, stato_zero)
+            ratio = self.norm_ratio(psi, stato_zero)
+            lam, e = self.apply_h(h, psi, need_lambda=True)
+            return e * ratio, self.gradient(th, psi, lam) * ratio, psi
         psi = self.forward_state(th, stato_zero)
-        ratio = self.norm_ratio(psi, stato_zero)
-        lam, e = self.apply_h(h, psi, need_lambda=True)
-        return e * ratio, self.gradient(th, psi, lam) * ratio, psi
+        self._upload_backward(th, psi.device)
+        nrm = self._norm_device(psi) if self.dtype == torch.complex64 else None
+        kind, H = self.hamiltonian(h)
+        if kind == 'pauli':
+            lam, e_dev = H.matvec(psi, want_expect=True)
+        else:
+            lam = H @ psi
+            e_dev = torch.vdot(psi.to(torch.complex128), lam.to(torch.complex128)).real.reshape(1)
+        grad = self._gradient_device(th, psi, lam)
+        parts = [e_dev.reshape(-1)[:1].to(torch.float64),
+                 nrm[:1] if nrm is not None else torch.ones(1, dtype=torch.float64, device=psi.device),
+                 grad[:self.nparams]]
+        vals = torch.cat(parts).cpu().numpy()
+        ratio = 1.0
+        if nrm is not None:
+            n0 = self._initial_norm2(stato_zero)
+            ratio = n0 / vals[1] if vals[1] > 0 else 1.0
+        return float(vals[0]) * ratio, vals[2:] * ratio, psi
 
     def parameter_shift_grad(self, theta, h, stato_zero=None) -> np.ndarray:
         """Parameter-shift gradient on the same kernels: two forward runs + <H> per
@@ -381,6 +449,37 @@ def _split_params(specs, ops, cap):
             cur.append((g, ids))
             seen |= slots
         out.append(fusion.PassSpec(ps.K, ps.L, ps.high, cur))
+    return out
+
+
+# Backward passes with more op records than the code generator takes
+# (jit.MAX_OPS) would run on the interpreter.  Splitting them into passes of
+# at most this many gates keeps every pass specialised: measured on the
+# 24-qubit, 10-layer ansatz, the first backward pass (330 records, the last
+# layers of the circuit) took 15.8 ms interpreted, and the gradient went from
+# 30.0 ms to 19.4 ms (cap 60) and 17.5 ms (cap 40).
+SPECIALISED_OPS_PER_PASS = 40
+
+
+def _split_ops(specs, cap):
+    """Split passes (and, where needed, their stages, keeping the gate order)
+    so that every pass holds at most cap gates; each piece keeps its pass's
+    tile geometry, so it is a valid pass of its own."""
+    out = []
+    for ps in specs:
+        cur, cnt = [], 0
+        for g, ids in ps.stages:
+            ids = list(ids)
+            while ids:
+                if cnt >= cap:
+                    out.append(fusion.PassSpec(ps.K, ps.L, ps.high, cur))
+                    cur, cnt = [], 0
+                take = ids[:cap - cnt]
+                cur.append((g, take))
+                cnt += len(take)
+                ids = ids[len(take):]
+        if cur:
+            out.append(fusion.PassSpec(ps.K, ps.L, ps.high, cur))
     return out
 
 

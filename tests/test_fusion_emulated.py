@@ -71,8 +71,10 @@ def test_untranspiled_dense_two_qubit_gates():
     assert np.max(np.abs(got - ref)) < 1e-12
 
 
-@pytest.mark.parametrize('n', [9, 12])
-def test_adjoint_plan_gradient_matches_fd(n):
+@pytest.mark.parametrize('n,split', [(9, 0), (12, 0), (12, 7)])
+def test_adjoint_plan_gradient_matches_fd(n, split):
+    """split > 0: backward passes (and stages) split to at most `split` gates,
+    as the complex64 path does to keep every pass specialised."""
     layers = 2
     rng = np.random.default_rng(n)
     theta = rng.uniform(-np.pi, np.pi, 2 * n * layers)
@@ -88,6 +90,13 @@ def test_adjoint_plan_gradient_matches_fd(n):
     lam = O.pauli_sum_matvec(psi, terms)
     bops = adjoint.backward_ops(ir)
     specs = adjoint._split_params(fusion.schedule(bops, n, 10), bops, 1024)
+    if split:
+        pieces = adjoint._split_ops(specs, split)
+        assert len(pieces) > len(specs)
+        assert all(sum(len(ids) for _, ids in ps.stages) <= split for ps in pieces)
+        flat = [i for ps in specs for _, ids in ps.stages for i in ids]
+        assert [i for ps in pieces for _, ids in ps.stages for i in ids] == flat
+        specs = pieces
     back = fusion.Packed(n, bops, specs, adjoint=True)
     grad = np.zeros(npar)
     _, _, grad = run_passes(psi, n, back.passes, back.ops, back.materialize(theta, np.complex128), lam=lam,
