@@ -565,8 +565,10 @@ def pauli_roofline(prog, theta, n, reps=10):
 
 def run_batch(args, layers=6):
     """Config 4: 4096 circuits, n ~ U{10..20}, HEA of 6 layers, XXZ chain with J_z ~ U[0.5, 1.5];
-    energy + adjoint gradient of every circuit from one persistent launch (CUDA graph replay).
-    The tile width comes from the autotuner, tuned first on a seeded 256-circuit sample."""
+    energy + adjoint gradient of every circuit: one persistent launch over the circuits of <= 12
+    qubits, the wider ones as rows groups (one launch per pass over all circuits of a width), the
+    whole batch replayed from one CUDA graph.  The tile width comes from the autotuner, tuned
+    first on a seeded 256-circuit sample."""
     import torch
     from dense_evolution import autotune
     from dense_evolution.batch import BatchVQE, hea_xxz_batch
@@ -601,20 +603,45 @@ def run_batch(args, layers=6):
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) / reps * 1e3
     amps = float(np.sum(2.0 ** ns))
-    # algorithmic HBM bytes of the streamed (> 12-qubit) circuits: forward passes
-    # 2 2^n B, backward passes 4 2^n B (psi and lambda), lambda = H psi 2 2^n B;
+    # algorithmic HBM bytes of the circuits wider than 12 qubits (rows groups:
+    # BatchVQE.rows_algorithmic_bytes; persistent streamed circuits: forward
+    # passes 2 2^n B, backward passes 4 2^n B, lambda = H psi 2 2^n B);
     # circuits of <= 12 qubits never leave shared memory
     hbm = 0.0
     for i, (pi, _, _) in enumerate(b.circ):
+        if pi < 0:
+            continue
         p = b.plans[pi]
         if p.n > 12:
             hbm += (2 * len(p.fwd.passes) + 4 * len(p.bwd.passes) + 2) * (1 << p.n) * 8
+    hbm += sum(b.rows_algorithmic_bytes(g) for g in b.groups)
     hbm_gbs = hbm / (ms / 1e3) / 1e9
+    # device time of each part: the persistent launch (<= 12 qubits) and every
+    # rows group, CUDA events on the launching stream, eager launches
+    parts = {}
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(b.groups) + 2)]
+    evs[0].record()
+    b.launch_persistent()
+    evs[1].record()
+    for k, g in enumerate(b.groups):
+        g.launch(b.d_theta, b.d_grad, None)
+        evs[k + 2].record()
+    torch.cuda.synchronize()
+    parts['persistent_ms'] = evs[0].elapsed_time(evs[1])
+    rows_tab = []
+    for k, g in enumerate(b.groups):
+        gms = evs[k + 1].elapsed_time(evs[k + 2])
+        gb = b.rows_algorithmic_bytes(g)
+        rows_tab.append({'qubits': g.plan.n, 'rows': g.B, 'ms': gms, 'algorithmic_bytes': gb,
+                         'gbs': gb / (gms / 1e3) / 1e9, 'frac_of_hbm': gb / (gms / 1e3) / 1e9 / _peaks()[0]})
+    parts['rows_groups'] = rows_tab
     return {'workload': f'{ncirc} circuits, qubits uniform in 10..20, HEA {layers} layers (RY,RZ + CX ladder), '
                         f'XXZ open chain J_xy=1, J_z~U[0.5,1.5]; energy + adjoint gradient per circuit',
             'ms_per_batch': ms, 'circuits_per_s': ncirc / (ms / 1e3), 'grads_per_s': ncirc / (ms / 1e3),
-            'e2e_ms_per_batch': e2e_ms, 'plans': len(b.plans), 'launches_per_batch': 1,
+            'e2e_ms_per_batch': e2e_ms, 'plans': len(b.plans) + len(b.groups),
+            'launches_per_batch': b.launches_per_batch(),
             'total_amplitudes': amps, 'resident_circuits': int(np.sum(ns <= 12)),
+            'rows_from_qubits': b.rows_from, 'parts': parts,
             'streamed_algorithmic_bytes': hbm, 'achieved_gbs_streamed': hbm_gbs,
             'frac_of_hbm_streamed': hbm_gbs / _peaks()[0],
             'register_bound_ctas_per_sm': int(os.environ.get('DESV_BATCH_MINB', '2')),

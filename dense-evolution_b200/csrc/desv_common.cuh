@@ -62,7 +62,27 @@ static const int tu_status_registered = (register_status_reader(&tu_status_read_
 // so one pass writes at most PAULI_MAX_BLOCKS_PER_SM x SMs partial-sum rows.
 constexpr int PAULI_MAX_TERMS = 512;
 constexpr int PAULI_MAX_BLOCKS_PER_SM = 8;
+
+// CTAs per row of a rows launch: enough rows x CTAs for about two waves of
+// `resident` CTAs, at most one CTA per tile
+inline int rows_grid_x(uint64_t tiles_per_row, uint64_t resident, int rows) {
+    uint64_t gx = (2 * resident + (uint64_t)rows - 1) / (uint64_t)rows;
+    if (gx > tiles_per_row) gx = tiles_per_row;
+    return gx < 1 ? 1 : (int)gx;
+}
 #endif  // __CUDACC_RTC__
+
+// Rows: several states of one qubit count stored back to back, each with its
+// own matrix pool, term table and partial sums (one circuit structure run for
+// many parameter rows).  A rows launch has one grid row (blockIdx.y) per state;
+// its CTAs offset their pointers by blockIdx.y times these strides.  A
+// single-state launch passes zeros and one grid row.
+struct RowStrides {
+    int64_t amps;   // amplitudes from one state to the next
+    int64_t mats;   // complex matrix-pool elements from one row's pool to the next
+    int64_t terms;  // Pauli term records from one row's table to the next
+    int64_t part;   // doubles from one row's partial sums to the next
+};
 
 // ---------------------------------------------------------------- complex
 template <typename R> struct CT;

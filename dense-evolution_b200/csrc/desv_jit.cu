@@ -113,6 +113,8 @@ static size_t rot_slot_elems(int K) { return ((size_t)1 << K) + ((size_t)1 << (K
 constexpr int JIT_ADJ_MAX_PARAMS = 1024;
 constexpr int JIT_ADJ_MAX_ROWS = 1184;
 int grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad, cudaStream_t st);
+int grad_reduce_rows(const double *part, int rows_x, int np, const int32_t *map, double *grad, int nrows,
+                     int64_t grad_stride, cudaStream_t st);
 size_t adjoint_scratch_bytes(int max_params);
 
 static std::vector<JitKernel *> g_kernels;  // status words of live modules (under g_jit_mu)
@@ -297,9 +299,36 @@ extern "C" int desv_jit_pass(void *handle, void *sv, int n, int dtype, const des
     const uint64_t ntiles = 1ull << (n - k->K);
     const uint64_t cap = (uint64_t)sm_count() * k->blocks_per_sm;
     const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
-    void *args[] = {&sv, &g, const_cast<void **>(&mats_dev)};
+    RowStrides rs{0, 0, 0, 0};
+    void *args[] = {&sv, &g, const_cast<void **>(&mats_dev), &rs};
     if (api().LaunchKernel(k->fn, grid, 1, 1, 1u << (k->K - 4), 1, 1, (unsigned)k->smem, stream, args, nullptr) != 0)
         return fail(DESV_ECUDA, "jit pass: launch failed");
+    return DESV_OK;
+}
+
+extern "C" int desv_jit_pass_rows(void *handle, void *states, int n, int dtype, int rows, const desv_pass *ps,
+                                  const void *pools_dev, int64_t pool_stride, void *stream) {
+    if (!handle || !states || !ps || !pools_dev) return fail(DESV_EINVAL, "jit rows pass: null argument");
+    auto *k = static_cast<JitKernel *>(handle);
+    if (k->kind != 0) return fail(DESV_EINVAL, "jit rows pass: the kernel is not a fused pass");
+    if (dtype != k->dtype) return fail(DESV_EINVAL, "jit rows pass: dtype differs from the compiled kernel");
+    if (n < 1 || n > 34) return fail(DESV_EINVAL, "jit rows pass: n out of range");
+    if (rows < 1 || rows > 65535) return fail(DESV_EINVAL, "jit rows pass: row count must be in [1, 65535]");
+    if (pool_stride < 0) return fail(DESV_EINVAL, "jit rows pass: negative pool stride");
+    if (reinterpret_cast<uintptr_t>(states) % 16) return fail(DESV_EINVAL, "jit rows pass: states not 16-byte aligned");
+    TileGeom g;
+    if (ps->tile_bits != k->K || ps->tile_bits > n || ps->low_bits < 5 || ps->tile_bits - ps->low_bits > 8 ||
+        !make_geom(g, n, ps->tile_bits, ps->low_bits, ps->high))
+        return fail(DESV_EINVAL, "jit rows pass: tile geometry does not match the compiled kernel");
+    if (ps->op_end == ps->op_begin) return DESV_OK;
+    const uint64_t ntiles = 1ull << (n - k->K);
+    const uint64_t cap = (uint64_t)sm_count() * k->blocks_per_sm;
+    const unsigned gx = (unsigned)rows_grid_x(ntiles, cap, rows);
+    RowStrides rs{(int64_t)1 << n, pool_stride, 0, 0};
+    void *args[] = {&states, &g, const_cast<void **>(&pools_dev), &rs};
+    if (api().LaunchKernel(k->fn, gx, (unsigned)rows, 1, 1u << (k->K - 4), 1, 1, (unsigned)k->smem, stream, args,
+                           nullptr) != 0)
+        return fail(DESV_ECUDA, "jit rows pass: launch failed");
     return DESV_OK;
 }
 
@@ -334,10 +363,61 @@ extern "C" int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int d
     const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
     int np = ps->nparams;
     double *part = static_cast<double *>(scratch);
-    void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&mats_dev), &np, &part};
+    RowStrides rs{0, 0, 0, 0};
+    void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&mats_dev), &np, &part, &rs};
     if (api().LaunchKernel(k->fn, grid, 1, 1, 1u << (k->K - 4), 1, 1, (unsigned)smem, stream, args, nullptr) != 0)
         return fail(DESV_ECUDA, "jit adjoint: launch failed");
     if (np > 0) return grad_reduce(part, (int)grid, np, map_dev + ps->map_begin, grad_dev, static_cast<cudaStream_t>(stream));
+    return DESV_OK;
+}
+
+// CTAs per state of a rows adjoint pass (partial-sum rows per state; the
+// bound desv_rows_scratch_bytes sizes for)
+constexpr int JIT_ADJ_ROWS_X = 64;
+
+extern "C" int desv_jit_adjoint_rows(void *handle, void *phi, void *lam, int n, int dtype, int rows,
+                                     const desv_adj_pass *ps, const desv_op *ops_dev, const void *pools_dev,
+                                     int64_t pool_stride, const int32_t *map_dev, double *grad_dev,
+                                     int64_t grad_stride, void *scratch, size_t scratch_bytes, void *stream) {
+    if (!handle || !phi || !lam || !ps || !ops_dev || !pools_dev || !map_dev || !grad_dev || !scratch)
+        return fail(DESV_EINVAL, "jit rows adjoint: null argument");
+    if (phi == lam) return fail(DESV_EINVAL, "jit rows adjoint: phi and lambda must be distinct buffers");
+    auto *k = static_cast<JitKernel *>(handle);
+    if (k->kind != 1) return fail(DESV_EINVAL, "jit rows adjoint: the kernel is not an adjoint pass");
+    if (dtype != k->dtype) return fail(DESV_EINVAL, "jit rows adjoint: dtype differs from the compiled kernel");
+    if (n < 1 || n > 34) return fail(DESV_EINVAL, "jit rows adjoint: n out of range");
+    if (rows < 1 || rows > 65535) return fail(DESV_EINVAL, "jit rows adjoint: row count must be in [1, 65535]");
+    if (pool_stride < 0 || grad_stride < 0) return fail(DESV_EINVAL, "jit rows adjoint: negative stride");
+    if (reinterpret_cast<uintptr_t>(phi) % 16 || reinterpret_cast<uintptr_t>(lam) % 16)
+        return fail(DESV_EINVAL, "jit rows adjoint: states not 16-byte aligned");
+    if (ps->nparams < 0 || ps->nparams > JIT_ADJ_MAX_PARAMS || ps->map_begin < 0)
+        return fail(DESV_EINVAL, "jit rows adjoint: parameter range invalid");
+    if (scratch_bytes < (size_t)rows * JIT_ADJ_ROWS_X * (size_t)(ps->nparams > 0 ? ps->nparams : 1) * sizeof(double))
+        return fail(DESV_EINVAL, "jit rows adjoint: scratch smaller than desv_rows_scratch_bytes(rows, params, 0)");
+    TileGeom g;
+    if (ps->tile_bits != k->K || ps->tile_bits > n || ps->low_bits < 5 || ps->tile_bits - ps->low_bits > 8 ||
+        !make_geom(g, n, ps->tile_bits, ps->low_bits, ps->high))
+        return fail(DESV_EINVAL, "jit rows adjoint: tile geometry does not match the compiled kernel");
+    if (ps->op_end == ps->op_begin) return DESV_OK;
+    const int nw = (1 << (k->K - 4)) / 32 > 0 ? (1 << (k->K - 4)) / 32 : 1;
+    const size_t smem = k->smem + (size_t)nw * ps->nparams * sizeof(double);
+    int bps = 0;
+    api().OccupancyMaxActiveBlocksPerMultiprocessor(&bps, k->fn, 1 << (k->K - 4), smem);
+    if (bps < 1) bps = 1;
+    const uint64_t ntiles = 1ull << (n - k->K);
+    int gx = rows_grid_x(ntiles, (uint64_t)sm_count() * bps, rows);
+    if (gx > JIT_ADJ_ROWS_X) gx = JIT_ADJ_ROWS_X;
+    int np = ps->nparams;
+    double *part = static_cast<double *>(scratch);
+    RowStrides rs{(int64_t)1 << n, pool_stride, 0, (int64_t)gx * np};
+    void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&pools_dev), &np, &part,
+                    &rs};
+    if (api().LaunchKernel(k->fn, (unsigned)gx, (unsigned)rows, 1, 1u << (k->K - 4), 1, 1, (unsigned)smem, stream,
+                           args, nullptr) != 0)
+        return fail(DESV_ECUDA, "jit rows adjoint: launch failed");
+    if (np > 0)
+        return grad_reduce_rows(part, gx, np, map_dev + ps->map_begin, grad_dev, rows, grad_stride,
+                                static_cast<cudaStream_t>(stream));
     return DESV_OK;
 }
 

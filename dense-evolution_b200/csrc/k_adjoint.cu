@@ -19,8 +19,14 @@ namespace desv {
 
 template <typename T, int K, int NBUF>
 __global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam, TileGeom g, const desv_op *ops,
-                                                                int nops, const T *mats, int nparams, double *part) {
+                                                                int nops, const T *mats, int nparams, double *part,
+                                                                RowStrides rs) {
     extern __shared__ __align__(128) unsigned char smem[];
+    // rows: this grid row's (phi, lambda) pair, matrix pool and partial sums
+    phi += blockIdx.y * rs.amps;
+    lam += blockIdx.y * rs.amps;
+    mats += blockIdx.y * rs.mats;
+    part += blockIdx.y * rs.part;
     constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
     double *acc = reinterpret_cast<double *>(smem + PIPE_HDR_BYTES + (size_t)NBUF * 2 * (1u << K) * sizeof(T));
     for (int i = threadIdx.x; i < NW * nparams; i += blockDim.x) acc[i] = 0.0;
@@ -103,9 +109,13 @@ __global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam
     }
 }
 
-// grad[map[p]] += 2 * sum_r part[r * np + p]   (fixed summation order)
-__global__ void k_grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad) {
+// grad[map[p]] += 2 * sum_r part[r * np + p]   (fixed summation order); one
+// block per state of a rows launch (part and grad offset by the row strides)
+__global__ void k_grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad,
+                              int64_t part_stride, int64_t grad_stride) {
     __shared__ double sh[32];
+    part += blockIdx.x * part_stride;
+    grad += blockIdx.x * grad_stride;
     for (int p = 0; p < np; ++p) {
         double v = 0;
         for (int r = threadIdx.x; r < rows; r += blockDim.x) v += part[(size_t)r * np + p];
@@ -124,6 +134,7 @@ __global__ void k_grad_reduce(const double *part, int rows, int np, const int32_
 
 constexpr int ADJ_MAX_PARAMS = 1024;
 constexpr int ADJ_MAX_ROWS = 1184;  // partial-sum rows per pass (= grid bound)
+constexpr int ADJ_MAX_ROWS_X = 64;  // CTAs per state of a rows pass (partial-sum rows per state)
 
 template <typename T, int K, int NBUF> static size_t adj_smem(int nparams) {
     constexpr int NW = (1 << (K - 4)) / 32 > 0 ? (1 << (K - 4)) / 32 : 1;
@@ -132,7 +143,7 @@ template <typename T, int K, int NBUF> static size_t adj_smem(int nparams) {
 
 template <typename T, int K, int NBUF>
 static int launch_adj(T *phi, T *lam, const TileGeom &g, const desv_op *ops, int nops, const T *mats, int nparams,
-                      double *part, int *grid_out, cudaStream_t st) {
+                      double *part, int *grid_out, int nrows, RowStrides rs, cudaStream_t st) {
     static bool attr[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -148,39 +159,66 @@ static int launch_adj(T *phi, T *lam, const TileGeom &g, const desv_op *ops, int
     if (bps < 1) bps = 1;
     const uint64_t ntiles = 1ull << (g.n - K);
     uint64_t cap = (uint64_t)sm_count() * bps;
-    if (cap > ADJ_MAX_ROWS) cap = ADJ_MAX_ROWS;
-    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    int grid;
+    if (rs.amps != 0) {  // a rows launch (single-state launches pass zero strides)
+        grid = rows_grid_x(ntiles, cap, nrows);
+        if (grid > ADJ_MAX_ROWS_X) grid = ADJ_MAX_ROWS_X;
+        rs.part = (int64_t)grid * nparams;  // each state's partial-sum block: grid x nparams
+    } else {
+        if (cap > ADJ_MAX_ROWS) cap = ADJ_MAX_ROWS;
+        grid = (int)(ntiles < cap ? ntiles : cap);
+    }
     *grid_out = grid;
-    k_adjoint_pass<T, K, NBUF><<<grid, 1 << (K - 4), adj_smem<T, K, NBUF>(nparams), st>>>(phi, lam, g, ops, nops, mats,
-                                                                                          nparams, part);
+    k_adjoint_pass<T, K, NBUF><<<dim3(grid, nrows), 1 << (K - 4), adj_smem<T, K, NBUF>(nparams), st>>>(
+        phi, lam, g, ops, nops, mats, nparams, part, rs);
     return check_launch("adjoint pass");
 }
 
+// One adjoint pass over `nrows` (phi, lambda) pairs; rs.amps / rs.mats are the
+// state and pool strides (rs.part is set here: grid_out x nparams per state).
+int adjoint_pass_rows(void *phi, void *lam, int dtype, const TileGeom &g, const desv_op *ops, int nops,
+                      const void *mats, int nparams, double *part, int *grid_out, int nrows, const RowStrides &rs,
+                      cudaStream_t st);
+
 int adjoint_pass(void *phi, void *lam, int dtype, const TileGeom &g, const desv_op *ops, int nops, const void *mats,
                  int nparams, double *part, int *grid_out, cudaStream_t st) {
+    return adjoint_pass_rows(phi, lam, dtype, g, ops, nops, mats, nparams, part, grid_out, 1, RowStrides{0, 0, 0, 0},
+                             st);
+}
+
+int adjoint_pass_rows(void *phi, void *lam, int dtype, const TileGeom &g, const desv_op *ops, int nops,
+                      const void *mats, int nparams, double *part, int *grid_out, int nrows, const RowStrides &rs,
+                      cudaStream_t st) {
     if (nparams < 0 || nparams > ADJ_MAX_PARAMS) return fail(DESV_EINVAL, "adjoint pass: at most 1024 parameters");
     if (dtype == DESV_C64) {
         float2 *p = static_cast<float2 *>(phi), *l = static_cast<float2 *>(lam);
         const float2 *m = static_cast<const float2 *>(mats);
         switch (g.K) {
-            case 9: return launch_adj<float2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
-            case 10: return launch_adj<float2, 10, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
-            case 11: return launch_adj<float2, 11, 3>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+            case 9: return launch_adj<float2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, nrows, rs, st);
+            case 10: return launch_adj<float2, 10, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, nrows, rs, st);
+            case 11: return launch_adj<float2, 11, 3>(p, l, g, ops, nops, m, nparams, part, grid_out, nrows, rs, st);
             default: return fail(DESV_EINVAL, "adjoint pass: complex64 tile_bits must be 9..11");
         }
     }
     double2 *p = static_cast<double2 *>(phi), *l = static_cast<double2 *>(lam);
     const double2 *m = static_cast<const double2 *>(mats);
     switch (g.K) {
-        case 9: return launch_adj<double2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
-        case 10: return launch_adj<double2, 10, 3>(p, l, g, ops, nops, m, nparams, part, grid_out, st);
+        case 9: return launch_adj<double2, 9, 4>(p, l, g, ops, nops, m, nparams, part, grid_out, nrows, rs, st);
+        case 10: return launch_adj<double2, 10, 3>(p, l, g, ops, nops, m, nparams, part, grid_out, nrows, rs, st);
         default: return fail(DESV_EINVAL, "adjoint pass: complex128 tile_bits must be 9..10");
     }
 }
 
 int grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad, cudaStream_t st) {
-    k_grad_reduce<<<1, 256, 0, st>>>(part, rows, np, map, grad);
+    k_grad_reduce<<<1, 256, 0, st>>>(part, rows, np, map, grad, 0, 0);
     return check_launch("gradient reduce");
+}
+
+// the reduction of a rows adjoint pass: one block per state
+int grad_reduce_rows(const double *part, int rows_x, int np, const int32_t *map, double *grad, int nrows,
+                     int64_t grad_stride, cudaStream_t st) {
+    k_grad_reduce<<<nrows, 256, 0, st>>>(part, rows_x, np, map, grad, (int64_t)rows_x * np, grad_stride);
+    return check_launch("gradient reduce (rows)");
 }
 
 size_t adjoint_scratch_bytes(int max_params) {

@@ -360,4 +360,103 @@ int batch_vqe(int dtype, const desv_batch_args &args, int *queue, int grid, cuda
 int batch_max_params() { return BATCH_MAXP; }
 int batch_resident_bits() { return BATCH_K; }
 
+// ---------------------------------------------------------------------------
+// Rows: one circuit structure evaluated for many parameter rows, every row's
+// state a full-width tensor of its own (back to back), run by the tiled
+// passes over all SMs with one grid row per state (k_fused_pass, k_pauli,
+// k_adjoint_pass take RowStrides).  These kernels prepare the rows (matrix
+// pools from theta, |0...0>) and reduce per-row partial sums.
+
+// pools[r] <- recipes(theta[r]); states[r] <- |0...0> (states zeroed before)
+template <typename T>
+__global__ void k_rows_prepare(const desv_batch_recipe *rec, int nrec, const double *theta, int64_t theta_stride,
+                               const T *cpool, T *pools, int64_t pool_stride, T *states, int64_t amps) {
+    const int r = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nrec) run_recipe<T>(rec[i], theta + (size_t)r * theta_stride, cpool, pools + (size_t)r * pool_stride);
+    if (states && i == 0) states[(size_t)r * amps] = cpx<T>(1.0, 0.0);
+}
+
+// per-row partial sums of <psi|psi> (FP64): grid (gx, rows)
+template <typename T>
+__global__ void __launch_bounds__(256) k_rows_norm(const T *sv, uint64_t amps, double *part, int64_t part_stride) {
+    sv += blockIdx.y * amps;
+    double s = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < amps; i += (uint64_t)gridDim.x * blockDim.x) {
+        const T a = sv[i];
+        s += (double)a.x * a.x + (double)a.y * a.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double sh[8];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        part[blockIdx.y * part_stride + blockIdx.x] = t;
+    }
+}
+
+// out[r * width + c] = sum_s part[r * stride + s * width + c] for s < count (fixed order)
+__global__ void k_rows_sum(const double *part, int64_t stride, int count, int width, double *out) {
+    const int r = blockIdx.x;
+    const double *p = part + (size_t)r * stride;
+    __shared__ double sh[8];
+    for (int c = 0; c < width; ++c) {
+        double v = 0;
+        for (int s = threadIdx.x; s < count; s += blockDim.x) v += p[(size_t)s * width + c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+            out[(size_t)r * width + c] = t;
+        }
+    }
+}
+
+int rows_prepare(int dtype, const desv_batch_recipe *rec, int nrec, const double *theta, int64_t theta_stride,
+                 const void *cpool, void *pools, int64_t pool_stride, void *states, int n, int rows, cudaStream_t st) {
+    const size_t es = dtype == DESV_C64 ? 8 : 16;
+    const uint64_t amps = 1ull << n;
+    if (states && cudaMemsetAsync(states, 0, (size_t)rows * amps * es, st) != cudaSuccess)
+        return check_launch("rows: zero states");
+    const dim3 grid((unsigned)((nrec > 0 ? nrec : 1) + 127) / 128, (unsigned)rows);
+    if (dtype == DESV_C64)
+        k_rows_prepare<float2><<<grid, 128, 0, st>>>(rec, nrec, theta, theta_stride, static_cast<const float2 *>(cpool),
+                                                     static_cast<float2 *>(pools), pool_stride,
+                                                     static_cast<float2 *>(states), (int64_t)amps);
+    else
+        k_rows_prepare<double2><<<grid, 128, 0, st>>>(rec, nrec, theta, theta_stride,
+                                                      static_cast<const double2 *>(cpool),
+                                                      static_cast<double2 *>(pools), pool_stride,
+                                                      static_cast<double2 *>(states), (int64_t)amps);
+    return check_launch("rows: prepare");
+}
+
+// <psi_r|psi_r> for every row into out[r]; part holds rows x ROWS_NORM_X doubles
+constexpr int ROWS_NORM_X = 32;
+int rows_norm(const void *sv, int n, int dtype, int rows, double *part, double *out, cudaStream_t st) {
+    const uint64_t amps = 1ull << n;
+    const uint64_t blocks = (amps + 255) / 256;
+    const int gx = (int)(blocks < (uint64_t)ROWS_NORM_X ? blocks : (uint64_t)ROWS_NORM_X);
+    if (dtype == DESV_C64)
+        k_rows_norm<float2><<<dim3(gx, rows), 256, 0, st>>>(static_cast<const float2 *>(sv), amps, part, ROWS_NORM_X);
+    else
+        k_rows_norm<double2><<<dim3(gx, rows), 256, 0, st>>>(static_cast<const double2 *>(sv), amps, part, ROWS_NORM_X);
+    int r = check_launch("rows: norm");
+    if (r) return r;
+    k_rows_sum<<<rows, 256, 0, st>>>(part, ROWS_NORM_X, gx, 1, out);
+    return check_launch("rows: norm reduce");
+}
+
+int rows_sum(const double *part, int64_t stride, int count, int width, double *out, int rows, cudaStream_t st) {
+    k_rows_sum<<<rows, 256, 0, st>>>(part, stride, count, width, out);
+    return check_launch("rows: reduce");
+}
+
 }  // namespace desv

@@ -57,8 +57,10 @@ __device__ __forceinline__ void fused_tile_body(T *s, T *sv, uint64_t base, cons
 // no ring slot waits for a store to drain.
 template <typename T, int K, int NBUF>
 __global__ void __launch_bounds__(1 << (K - 4)) k_fused_pass(T *sv, TileGeom g, const desv_op *ops, int nops,
-                                                              const T *mats) {
+                                                              const T *mats, RowStrides rs) {
     extern __shared__ __align__(128) unsigned char smem[];
+    sv += blockIdx.y * rs.amps;
+    mats += blockIdx.y * rs.mats;
     PipeArrays<T, 1> A;
     A.ptr[0] = sv;
     A.load[0] = true;
@@ -71,7 +73,8 @@ __global__ void __launch_bounds__(1 << (K - 4)) k_fused_pass(T *sv, TileGeom g, 
 }
 
 template <typename T, int K, int NBUF>
-static int launch_fused(T *sv, const TileGeom &g, const desv_op *ops, int nops, const T *mats, cudaStream_t st) {
+static int launch_fused(T *sv, const TileGeom &g, const desv_op *ops, int nops, const T *mats, int rows,
+                        const RowStrides &rs, cudaStream_t st) {
     static int bps[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -84,34 +87,40 @@ static int launch_fused(T *sv, const TileGeom &g, const desv_op *ops, int nops, 
     }
     const uint64_t ntiles = 1ull << (g.n - K);
     const uint64_t cap = (uint64_t)sm_count() * bps[dev & 63];
-    const int grid = (int)(ntiles < cap ? ntiles : cap);
-    k_fused_pass<T, K, NBUF><<<grid, 1 << (K - 4), smem, st>>>(sv, g, ops, nops, mats);
+    const int grid = rs.amps != 0 ? rows_grid_x(ntiles, cap, rows) : (int)(ntiles < cap ? ntiles : cap);
+    k_fused_pass<T, K, NBUF><<<dim3(grid, rows), 1 << (K - 4), smem, st>>>(sv, g, ops, nops, mats, rs);
     return check_launch("fused pass");
 }
 
-int fused_pass(void *sv, int dtype, const TileGeom &g, const desv_op *ops, int nops, const void *mats,
-               cudaStream_t st) {
+// one fused pass over `rows` states (rs: their strides; rows = 1, rs = {} for one state)
+int fused_pass_rows(void *sv, int dtype, const TileGeom &g, const desv_op *ops, int nops, const void *mats, int rows,
+                    const RowStrides &rs, cudaStream_t st) {
     if (dtype == DESV_C64) {
         float2 *p = static_cast<float2 *>(sv);
         const float2 *m = static_cast<const float2 *>(mats);
         switch (g.K) {
-            case 9: return launch_fused<float2, 9, 4>(p, g, ops, nops, m, st);
-            case 10: return launch_fused<float2, 10, 4>(p, g, ops, nops, m, st);
-            case 11: return launch_fused<float2, 11, 4>(p, g, ops, nops, m, st);
-            case 12: return launch_fused<float2, 12, 3>(p, g, ops, nops, m, st);
-            case 13: return launch_fused<float2, 13, 3>(p, g, ops, nops, m, st);
+            case 9: return launch_fused<float2, 9, 4>(p, g, ops, nops, m, rows, rs, st);
+            case 10: return launch_fused<float2, 10, 4>(p, g, ops, nops, m, rows, rs, st);
+            case 11: return launch_fused<float2, 11, 4>(p, g, ops, nops, m, rows, rs, st);
+            case 12: return launch_fused<float2, 12, 3>(p, g, ops, nops, m, rows, rs, st);
+            case 13: return launch_fused<float2, 13, 3>(p, g, ops, nops, m, rows, rs, st);
             default: return fail(DESV_EINVAL, "fused pass: complex64 tile_bits must be 9..13");
         }
     }
     double2 *p = static_cast<double2 *>(sv);
     const double2 *m = static_cast<const double2 *>(mats);
     switch (g.K) {
-        case 9: return launch_fused<double2, 9, 4>(p, g, ops, nops, m, st);
-        case 10: return launch_fused<double2, 10, 4>(p, g, ops, nops, m, st);
-        case 11: return launch_fused<double2, 11, 4>(p, g, ops, nops, m, st);
-        case 12: return launch_fused<double2, 12, 3>(p, g, ops, nops, m, st);
+        case 9: return launch_fused<double2, 9, 4>(p, g, ops, nops, m, rows, rs, st);
+        case 10: return launch_fused<double2, 10, 4>(p, g, ops, nops, m, rows, rs, st);
+        case 11: return launch_fused<double2, 11, 4>(p, g, ops, nops, m, rows, rs, st);
+        case 12: return launch_fused<double2, 12, 3>(p, g, ops, nops, m, rows, rs, st);
         default: return fail(DESV_EINVAL, "fused pass: complex128 tile_bits must be 9..12");
     }
+}
+
+int fused_pass(void *sv, int dtype, const TileGeom &g, const desv_op *ops, int nops, const void *mats,
+               cudaStream_t st) {
+    return fused_pass_rows(sv, dtype, g, ops, nops, mats, 1, RowStrides{0, 0, 0, 0}, st);
 }
 
 }  // namespace desv

@@ -15,6 +15,7 @@
 namespace desv {
 
 constexpr int PAULI_THREADS = 256;
+constexpr int PAULI_MAX_ROWS_X = 64;  // CTAs per state of a rows pass (partial-sum rows per state and pass)
 // an SM holds at most 2048 threads, so the occupancy of a tiled pass can never
 // exceed the per-SM grid bound the partial-sum buffers are sized for
 static_assert(2048 / PAULI_THREADS <= PAULI_MAX_BLOCKS_PER_SM, "Pauli grid bound");
@@ -36,8 +37,13 @@ __device__ __forceinline__ uint32_t global_to_tile_local(const TileGeom &g, uint
 // MODE 0: expectation only; 1: matvec overwrite (+ optional expectation); 2: matvec accumulate
 template <typename T, int K, int NBUF, int MODE>
 __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, TileGeom g, const desv_pauli_term *terms,
-                                                         int nterms, int want_e, double *part) {
+                                                         int nterms, int want_e, double *part, RowStrides rs) {
     extern __shared__ __align__(128) unsigned char smem[];
+    // rows: this grid row's state, output, term table and partial sums
+    psi += blockIdx.y * rs.amps;
+    if (MODE != 0) out += blockIdx.y * rs.amps;
+    terms += blockIdx.y * rs.terms;
+    part += blockIdx.y * rs.part;
     // only psi travels through the shared-memory ring; H psi is written (MODE 1)
     // or accumulated (MODE 2) straight in HBM, amplitude j of a tile by thread
     // j mod 256, so consecutive threads touch consecutive addresses
@@ -153,7 +159,7 @@ __global__ void __launch_bounds__(PAULI_THREADS) k_pauli(const T *psi, T *out, T
 
 template <typename T, int K, int NBUF, int MODE>
 static int launch_pauli(const T *psi, T *out, const TileGeom &g, const desv_pauli_term *terms, int nterms, int want_e,
-                        double *part, int *grid_out, cudaStream_t st) {
+                        double *part, int *grid_out, int nrows, const RowStrides &rs, cudaStream_t st) {
     static int bps[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -167,9 +173,14 @@ static int launch_pauli(const T *psi, T *out, const TileGeom &g, const desv_paul
     }
     const uint64_t ntiles = 1ull << (g.n - K);
     const uint64_t cap = (uint64_t)sm_count() * bps[dev & 63];
-    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    int grid = (int)(ntiles < cap ? ntiles : cap);
+    if (rs.amps != 0) {  // a rows launch (single-state launches pass zero strides)
+        grid = rows_grid_x(ntiles, cap, nrows);
+        if (grid > PAULI_MAX_ROWS_X) grid = PAULI_MAX_ROWS_X;
+    }
     *grid_out = grid;
-    k_pauli<T, K, NBUF, MODE><<<grid, PAULI_THREADS, smem, st>>>(psi, out, g, terms, nterms, want_e, part);
+    k_pauli<T, K, NBUF, MODE><<<dim3(grid, nrows), PAULI_THREADS, smem, st>>>(psi, out, g, terms, nterms, want_e, part,
+                                                                             rs);
     return check_launch("pauli pass");
 }
 
@@ -179,7 +190,11 @@ static int launch_pauli(const T *psi, T *out, const TileGeom &g, const desv_paul
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_pauli_direct(const T *psi, T *out, uint64_t dim,
                                                       const desv_pauli_term *terms, int nterms, int want_e,
-                                                      double *part) {
+                                                      double *part, RowStrides rs) {
+    psi += blockIdx.y * rs.amps;
+    if (MODE != 0) out += blockIdx.y * rs.amps;
+    terms += blockIdx.y * rs.terms;
+    part += blockIdx.y * rs.part;
     double ere = 0, eim = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
         double2 v = make_double2(0.0, 0.0);
@@ -230,16 +245,21 @@ __global__ void __launch_bounds__(256) k_pauli_direct(const T *psi, T *out, uint
     }
 }
 
-int pauli_direct(const void *psi, void *out, int dtype, int mode, int n, const desv_pauli_term *terms, int nterms,
-                 int want_e, double *part, int *grid_out, cudaStream_t st) {
+int pauli_direct_rows(const void *psi, void *out, int dtype, int mode, int n, const desv_pauli_term *terms,
+                      int nterms, int want_e, double *part, int *grid_out, int nrows, const RowStrides &rs,
+                      cudaStream_t st) {
     const uint64_t dim = 1ull << n;
     uint64_t b = (dim + 255) / 256;
     const uint64_t cap = (uint64_t)sm_count() * PAULI_MAX_BLOCKS_PER_SM;
-    const int grid = (int)(b < cap ? b : cap);
+    int grid = (int)(b < cap ? b : cap);
+    if (rs.amps != 0) {  // a rows launch (single-state launches pass zero strides)
+        grid = rows_grid_x(b, cap, nrows);
+        if (grid > PAULI_MAX_ROWS_X) grid = PAULI_MAX_ROWS_X;
+    }
     *grid_out = grid;
-#define DESV_PD(T, M)                                                                                          \
-    k_pauli_direct<T, M><<<grid, 256, 0, st>>>(static_cast<const T *>(psi), static_cast<T *>(out), dim, terms, \
-                                               nterms, want_e, part)
+#define DESV_PD(T, M)                                                                                             \
+    k_pauli_direct<T, M><<<dim3(grid, nrows), 256, 0, st>>>(static_cast<const T *>(psi), static_cast<T *>(out), dim, \
+                                                            terms, nterms, want_e, part, rs)
     if (dtype == DESV_C64) {
         if (mode == 0) DESV_PD(float2, 0);
         else if (mode == 1) DESV_PD(float2, 1);
@@ -253,48 +273,62 @@ int pauli_direct(const void *psi, void *out, int dtype, int mode, int n, const d
     return check_launch("pauli direct pass");
 }
 
+int pauli_direct(const void *psi, void *out, int dtype, int mode, int n, const desv_pauli_term *terms, int nterms,
+                 int want_e, double *part, int *grid_out, cudaStream_t st) {
+    return pauli_direct_rows(psi, out, dtype, mode, n, terms, nterms, want_e, part, grid_out, 1,
+                             RowStrides{0, 0, 0, 0}, st);
+}
+
 template <typename T, int K, int MODE>
 static int pauli_k(const T *p, T *o, const TileGeom &g, const desv_pauli_term *terms, int nterms, int want_e,
-                   double *part, int *grid_out, cudaStream_t st) {
-    return launch_pauli<T, K, 4, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+                   double *part, int *grid_out, int nrows, const RowStrides &rs, cudaStream_t st) {
+    return launch_pauli<T, K, 4, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
 }
 
 template <typename T, int MODE>
 static int pauli_dispatch(const T *p, T *o, const TileGeom &g, const desv_pauli_term *terms, int nterms, int want_e,
-                          double *part, int *grid_out, cudaStream_t st, int kmax) {
+                          double *part, int *grid_out, int nrows, const RowStrides &rs, cudaStream_t st, int kmax) {
     if (g.K > kmax) return fail(DESV_EINVAL, "pauli pass: tile_bits too large for this precision");
     switch (g.K) {
-        case 1: return pauli_k<T, 1, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 2: return pauli_k<T, 2, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 3: return pauli_k<T, 3, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 4: return pauli_k<T, 4, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 5: return pauli_k<T, 5, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 6: return pauli_k<T, 6, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 7: return pauli_k<T, 7, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 8: return pauli_k<T, 8, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 9: return pauli_k<T, 9, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        case 10: return pauli_k<T, 10, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
-        default: return pauli_k<T, 11, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, st);
+        case 1: return pauli_k<T, 1, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 2: return pauli_k<T, 2, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 3: return pauli_k<T, 3, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 4: return pauli_k<T, 4, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 5: return pauli_k<T, 5, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 6: return pauli_k<T, 6, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 7: return pauli_k<T, 7, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 8: return pauli_k<T, 8, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 9: return pauli_k<T, 9, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        case 10: return pauli_k<T, 10, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
+        default: return pauli_k<T, 11, MODE>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st);
     }
 }
 
 // Tile of up to 2^11 amplitudes for complex64 and 2^10 for complex128 (16 KB).
-int pauli_pass(const void *psi, void *out, int dtype, int mode, const TileGeom &g, const desv_pauli_term *terms,
-               int nterms, int want_e, double *part, int *grid_out, cudaStream_t st) {
+// nrows states (rs: strides) in one launch; nrows = 1, rs = {} for one state.
+int pauli_pass_rows(const void *psi, void *out, int dtype, int mode, const TileGeom &g, const desv_pauli_term *terms,
+                    int nterms, int want_e, double *part, int *grid_out, int nrows, const RowStrides &rs,
+                    cudaStream_t st) {
     if (nterms > PAULI_MAX_TERMS) return fail(DESV_EINVAL, "pauli pass: more than 512 terms in one pass");
     if (g.K < 5 && g.K != g.n) return fail(DESV_EINVAL, "pauli pass: tile smaller than 2^5 must cover the state");
     if (dtype == DESV_C64) {
         const float2 *p = static_cast<const float2 *>(psi);
         float2 *o = static_cast<float2 *>(out);
-        if (mode == 0) return pauli_dispatch<float2, 0>(p, o, g, terms, nterms, want_e, part, grid_out, st, 11);
-        if (mode == 1) return pauli_dispatch<float2, 1>(p, o, g, terms, nterms, want_e, part, grid_out, st, 11);
-        return pauli_dispatch<float2, 2>(p, o, g, terms, nterms, want_e, part, grid_out, st, 11);
+        if (mode == 0) return pauli_dispatch<float2, 0>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st, 11);
+        if (mode == 1) return pauli_dispatch<float2, 1>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st, 11);
+        return pauli_dispatch<float2, 2>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st, 11);
     }
     const double2 *p = static_cast<const double2 *>(psi);
     double2 *o = static_cast<double2 *>(out);
-    if (mode == 0) return pauli_dispatch<double2, 0>(p, o, g, terms, nterms, want_e, part, grid_out, st, 10);
-    if (mode == 1) return pauli_dispatch<double2, 1>(p, o, g, terms, nterms, want_e, part, grid_out, st, 10);
-    return pauli_dispatch<double2, 2>(p, o, g, terms, nterms, want_e, part, grid_out, st, 10);
+    if (mode == 0) return pauli_dispatch<double2, 0>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st, 10);
+    if (mode == 1) return pauli_dispatch<double2, 1>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st, 10);
+    return pauli_dispatch<double2, 2>(p, o, g, terms, nterms, want_e, part, grid_out, nrows, rs, st, 10);
+}
+
+int pauli_pass(const void *psi, void *out, int dtype, int mode, const TileGeom &g, const desv_pauli_term *terms,
+               int nterms, int want_e, double *part, int *grid_out, cudaStream_t st) {
+    return pauli_pass_rows(psi, out, dtype, mode, g, terms, nterms, want_e, part, grid_out, 1, RowStrides{0, 0, 0, 0},
+                           st);
 }
 
 }  // namespace desv

@@ -79,6 +79,15 @@ _SIGS = {
     'desv_bit_reverse': ([_vp, _vp, _i, _i, _vp], _i),
     'desv_jit_compile_check': ([ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _sz], _i),
     'desv_swap_blocks': ([_vp, _vp, _sz, _vp], _i),
+    'desv_rows_scratch_bytes': ([_i, _i, _i], _sz),
+    'desv_rows_prepare': ([_vp, _i, _i, _i, _vp, _i, _vp, ctypes.c_int64, _vp, _vp, ctypes.c_int64, _vp], _i),
+    'desv_apply_passes_rows': ([_vp, _i, _i, _i, _vp, _i, _vp, _vp, ctypes.c_int64, _vp], _i),
+    'desv_pauli_matvec_rows': ([_vp, _vp, _i, _i, _i, _vp, _i, _vp, ctypes.c_int64, _vp, _vp, _vp, _sz, _vp], _i),
+    'desv_adjoint_passes_rows': ([_vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp, ctypes.c_int64, _vp, _vp,
+                                  ctypes.c_int64, _vp, _sz, _vp], _i),
+    'desv_jit_pass_rows': ([_vp, _vp, _i, _i, _i, _vp, _vp, ctypes.c_int64, _vp], _i),
+    'desv_jit_adjoint_rows': ([_vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp, ctypes.c_int64,
+                               _vp, _sz, _vp], _i),
 }
 OPTIONAL = set()
 

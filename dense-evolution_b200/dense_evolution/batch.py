@@ -13,8 +13,14 @@ circuit, ``solvers/autodiff.py:92-169``).  Here:
   can be rebuilt from theta on the device);
 * each circuit brings its theta and its real term coefficients (e.g. its own
   J_z of an XXZ chain);
-* circuits are ordered by decreasing cost and pulled from an atomic queue, one
-  per CTA; states of <= 12 qubits never leave shared memory.
+* circuits of <= 12 qubits are ordered by decreasing cost and pulled from an
+  atomic queue, one per CTA, in one persistent launch; their states never
+  leave shared memory;
+* wider circuits run as rows: all circuits of one structure form one set of
+  full-width states back to back, and every pass (forward, H psi with the
+  energy, adjoint with the gradient) covers all of them in one launch over
+  all SMs, with each row's own matrix pool (built from its theta on the
+  device) and its own term coefficients.
 
 Parameters are injected like the energy functions: into rx/ry/rz/u1/p/cp/crz
 in gate order (``solvers/autodiff.py:21,150-157``).
@@ -155,15 +161,209 @@ class _Plan:
         return (1 << self.n) * (len(self.fwd.ops) + 2 * len(self.bwd.ops))
 
 
+class _RowsPlan:
+    """One circuit structure planned for the rows path: every row (parameter
+    set) of the structure is a full-width state of its own, and each pass runs
+    over all rows in one launch over all SMs (``desv_apply_passes_rows``,
+    ``desv_pauli_matvec_rows``, ``desv_adjoint_passes_rows``).  Forward passes
+    use tiles of ``tile_bits``; adjoint passes the single-circuit adjoint tile
+    width; matrices come from theta on the device (recipes), one pool per row."""
+
+    def __init__(self, rows, slots, n, dtype, tile_bits, terms=None, forward_only: bool = False, use_jit=None):
+        import os
+        from .circuits import jit
+        if use_jit is None:
+            use_jit = os.environ.get('DESV_JIT', '') != '0' and jit.available()
+        self.use_jit = bool(use_jit)
+        self._kernels = {}
+        n = int(n)
+        if n < fusion.MIN_FUSED_QUBITS:
+            raise ValueError(f'rows path needs at least {fusion.MIN_FUSED_QUBITS} qubits per circuit')
+        self.n = n
+        self.dtype = dtype
+        self.nparams = 1 + max([s for s in slots if s >= 0], default=-1)
+        K = min(n, int(tile_bits))
+        ir = fusion.lower(rows, n, slots)
+        fops = fusion.fuse_1q(ir, merge=False)
+        self.fwd = fusion.Packed(n, fops, fusion.schedule(fops, n, K))
+        if forward_only:
+            self.bwd = None
+        else:
+            bops = adjoint.backward_ops(ir)
+            kb = adjoint._adjoint_tile_bits(n, dtype)
+            specs = adjoint._split_params(fusion.schedule(bops, n, kb), bops, 1024) if bops else []
+            if self.use_jit and dtype == torch.complex64:
+                # every backward pass short enough for a specialised kernel
+                specs = adjoint._split_ops(specs, adjoint.SPECIALISED_OPS_PER_PASS)
+            self.bwd = fusion.Packed(n, bops, specs, adjoint=True)
+        cdt = np.complex64 if dtype == torch.complex64 else np.complex128
+        th0 = 0.37 + 0.0137 * np.arange(max(self.nparams, 1))   # generic angles: flags valid for every theta
+        fpool = self.fwd.materialize(th0, cdt)
+        self.fwd_len = len(fpool)
+        recs = [_Plan._recipes(self.fwd, 0)]
+        pools = [fpool]
+        if self.bwd is not None:
+            bpool = self.bwd.materialize(th0, cdt)
+            bops_arr = self.bwd.ops
+            is_rec = bops_arr['kind'] != N.OP_STAGE
+            bops_arr['mat'][is_rec] += self.fwd_len
+            recs.append(_Plan._recipes(self.bwd, self.fwd_len))
+            pools.append(bpool)
+        self.cpool = np.concatenate(pools)
+        self.recipes = np.concatenate(recs)
+        # every row's pool starts on a 256-byte boundary
+        per = 256 // (8 if dtype == torch.complex64 else 16)
+        self.pool_stride = max(per, (len(self.cpool) + per - 1) // per * per)
+        self.pauli = None
+        if terms is not None and not forward_only:
+            from .physics.observables import plan_for
+            self.pauli = plan_for([(1.0, p) for _, p in terms], n, None, dtype)
+
+    def kernels(self, device: int):
+        """(forward, backward) lists of specialised kernels per pass (None: that
+        pass runs on the interpreter), compiled once per device.  The sources
+        read only pool values that no angle changes (generator and constant
+        records), so one set serves every row.  complex128 backward passes stay
+        on the interpreter (two double2 register tiles exceed the register file)."""
+        if not self.use_jit:
+            return None, None
+        got = self._kernels.get(device)
+        if got is None:
+            from .circuits import jit
+            c64 = self.dtype == torch.complex64
+            kf = jit.compile_passes(self.fwd.ops, self.fwd.passes, self.cpool, c64, device)
+            kb = jit.compile_adjoint(self.bwd.ops, self.bwd.passes, self.cpool, c64, device) \
+                if (self.bwd is not None and c64) else None
+            got = (kf, kb)
+            self._kernels[device] = got
+        return got
+
+    def term_rows(self, coefs: Sequence[Sequence[float]]) -> np.ndarray:
+        """(rows x terms) table of Pauli term records with every row's real
+        coefficients folded in, in the plan's packed term order."""
+        base = self.pauli.terms
+        co = np.asarray(coefs, dtype=np.float64)[:, self.pauli.order]     # (rows, terms)
+        out = np.zeros((co.shape[0], max(len(base), 1)), N.TERM_DTYPE)
+        if len(base):
+            out['xmask'][:, :len(base)] = base['xmask']
+            out['zmask'][:, :len(base)] = base['zmask']
+            out['cre'][:, :len(base)] = base['cre'] * co
+            out['cim'][:, :len(base)] = base['cim'] * co
+        return out
+
+
+def rows_forward(kernels, states: torch.Tensor, n: int, code: int, rows: int, passes: np.ndarray, d_ops: torch.Tensor,
+                 pools: torch.Tensor, pool_stride: int, st):
+    """Every forward pass over all rows: the specialised kernel of a pass where
+    there is one, the interpreter otherwise."""
+    lib, vp = N.lib(), ctypes.c_void_p
+    for i in range(len(passes)):
+        pp = vp(passes.ctypes.data + i * passes.itemsize)
+        k = kernels[i] if kernels is not None else None
+        if k is None:
+            N.check(lib.desv_apply_passes_rows(vp(states.data_ptr()), n, code, rows, pp, 1, vp(d_ops.data_ptr()),
+                                               vp(pools.data_ptr()), pool_stride, st), 'rows forward pass')
+        else:
+            N.check(lib.desv_jit_pass_rows(k.handle, vp(states.data_ptr()), n, code, rows, pp, vp(pools.data_ptr()),
+                                           pool_stride, st), 'rows forward pass (jit)')
+
+
+class _RowsGroup:
+    """Device buffers and launches of one structure's rows: psi and lambda
+    (rows x 2^n each), the per-row pools, term tables, <psi|H|psi> and
+    <psi|psi>; theta and the gradient are rows of ``nparams`` at ``theta_base``
+    in the batch's theta / gradient buffers.  Everything is allocated here, so
+    ``launch`` only queues work (capturable in a CUDA graph)."""
+
+    def __init__(self, plan: _RowsPlan, coefs, theta_base: int, dev, code: int):
+        self.plan = plan
+        self.B = B = len(coefs)
+        self.code = code
+        self.theta_base = theta_base
+        self.P = max(plan.nparams, 1)
+        n = plan.n
+        rdt = np.float32 if plan.dtype == torch.complex64 else np.float64
+        cdt = np.complex64 if plan.dtype == torch.complex64 else np.complex128
+
+        def up(a):
+            return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+
+        self.psi = torch.empty((B, 1 << n), dtype=plan.dtype, device=dev)
+        self.lam = torch.empty((B, 1 << n), dtype=plan.dtype, device=dev)
+        self.pools = torch.empty((B, plan.pool_stride), dtype=plan.dtype, device=dev)
+        self.d_cpool = torch.from_numpy(plan.cpool.astype(cdt).view(rdt).copy()).to(dev)
+        self.d_recipes = up(plan.recipes)
+        self.fwd_passes = np.ascontiguousarray(plan.fwd.passes)
+        self.d_fwd_ops = up(plan.fwd.ops if len(plan.fwd.ops) else np.zeros(1, N.OP_DTYPE))
+        self.bwd_passes = np.ascontiguousarray(plan.bwd.passes)
+        self.d_bwd_ops = up(plan.bwd.ops if len(plan.bwd.ops) else np.zeros(1, N.OP_DTYPE))
+        self.d_map = torch.tensor(plan.bwd.param_map or [0], dtype=torch.int32, device=dev)
+        tr = plan.term_rows(coefs)
+        self.term_stride = tr.shape[1]
+        self.d_terms = up(tr.reshape(-1))
+        self.ppasses = np.ascontiguousarray(plan.pauli.passes)
+        self.expect = torch.zeros((B, 2), dtype=torch.float64, device=dev)
+        self.norm = torch.ones(B, dtype=torch.float64, device=dev)
+        sb = int(N.lib().desv_rows_scratch_bytes(B, max(plan.bwd.max_params, 1), max(len(self.ppasses), 1)))
+        self.scratch = torch.empty((sb + 7) // 8, dtype=torch.float64, device=dev)
+        self.kf, self.kb = plan.kernels(dev.index if dev.index is not None else torch.cuda.current_device())
+
+    def launch(self, d_theta: torch.Tensor, d_grad: torch.Tensor, stream):
+        p, n, B, st = self.plan, self.plan.n, self.B, ctypes.c_void_p(N.stream_ptr(stream))
+        vp = ctypes.c_void_p
+        theta = vp(d_theta.data_ptr() + 8 * self.theta_base)
+        grad = d_grad[self.theta_base:self.theta_base + B * self.P]
+        N.check(N.lib().desv_rows_prepare(vp(self.psi.data_ptr()), n, self.code, B, vp(self.d_recipes.data_ptr()),
+                                          len(p.recipes), theta, self.P, vp(self.d_cpool.data_ptr()),
+                                          vp(self.pools.data_ptr()), p.pool_stride, st), 'rows prepare')
+        rows_forward(self.kf, self.psi, n, self.code, B, self.fwd_passes, self.d_fwd_ops, self.pools, p.pool_stride,
+                     st)
+        want_norm = p.dtype == torch.complex64
+        N.check(N.lib().desv_pauli_matvec_rows(vp(self.psi.data_ptr()), vp(self.lam.data_ptr()), n, self.code, B,
+                                               vp(self.ppasses.ctypes.data), len(self.ppasses),
+                                               vp(self.d_terms.data_ptr()), self.term_stride,
+                                               vp(self.expect.data_ptr()),
+                                               vp(self.norm.data_ptr()) if want_norm else None,
+                                               vp(self.scratch.data_ptr()), self.scratch.numel() * 8, st),
+                'rows H psi')
+        with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+            grad.zero_()
+        lib, sc, nsc = N.lib(), vp(self.scratch.data_ptr()), self.scratch.numel() * 8
+        for i in range(len(self.bwd_passes)):
+            pp = vp(self.bwd_passes.ctypes.data + i * self.bwd_passes.itemsize)
+            k = self.kb[i] if self.kb is not None else None
+            if k is None:
+                N.check(lib.desv_adjoint_passes_rows(vp(self.psi.data_ptr()), vp(self.lam.data_ptr()), n, self.code,
+                                                     B, pp, 1, vp(self.d_bwd_ops.data_ptr()),
+                                                     vp(self.pools.data_ptr()), p.pool_stride,
+                                                     vp(self.d_map.data_ptr()), vp(grad.data_ptr()), self.P, sc, nsc,
+                                                     st), 'rows adjoint pass')
+            else:
+                N.check(lib.desv_jit_adjoint_rows(k.handle, vp(self.psi.data_ptr()), vp(self.lam.data_ptr()), n,
+                                                  self.code, B, pp, vp(self.d_bwd_ops.data_ptr()),
+                                                  vp(self.pools.data_ptr()), p.pool_stride, vp(self.d_map.data_ptr()),
+                                                  vp(grad.data_ptr()), self.P, sc, nsc, st), 'rows adjoint pass (jit)')
+
+
 class BatchVQE:
     """Energies and adjoint gradients of many circuits in one launch.
 
     items: sequence of (circuit, n_qubits, terms) -- circuit as gate tuples or
     a QASMCircuit (parameters are ignored; theta is injected in gate order),
     terms as (real coefficient, Pauli term) pairs.  Circuits whose gate list
-    and term structure coincide share a plan."""
+    and term structure coincide share a plan.
 
-    def __init__(self, items: Sequence[Tuple], use_float32: bool = True, tile_bits=None):
+    Circuits of up to ``rows_from - 1`` qubits (default: those whose state fits
+    one CTA's shared memory, 12 qubits) run in the persistent launch, one CTA
+    each.  Wider ones run as rows: all circuits of one structure form one set
+    of full-width states, and each pass runs over all of them in one launch
+    over all SMs.  ``DESV_BATCH_ROWS_FROM`` overrides the default.  Rows passes
+    run on plan-specialised kernels (compiled once per structure) unless
+    ``rows_jit`` is False or ``DESV_JIT=0``."""
+
+    def __init__(self, items: Sequence[Tuple], use_float32: bool = True, tile_bits=None, rows_from=None,
+                 rows_jit=None):
+        import os
         self.dtype = torch.complex64 if use_float32 else torch.complex128
         self.device = N.require_cuda()
         N.lib()
@@ -171,13 +371,31 @@ class BatchVQE:
             from . import autotune
             tile_bits = autotune.batch_tile_bits(self.dtype)
         self.tile_bits = int(tile_bits)
+        if rows_from is None:
+            rows_from = int(os.environ.get('DESV_BATCH_ROWS_FROM', RESIDENT_BITS + 1))
+        self.rows_from = max(int(rows_from), fusion.MIN_FUSED_QUBITS)
         plans: Dict[tuple, int] = {}
+        rplans: Dict[tuple, int] = {}
         self.plans: List[_Plan] = []
-        self.circ = []          # (plan index, coefficients, nparams)
-        for circuit, n, terms in items:
+        self.rplans: List[list] = []     # [_RowsPlan, circuit indices, coefficient rows, nparams]
+        self.circ = []          # (plan index or -1, coefficients, nparams); rows circuits: -1
+        self.row_of = {}        # circuit index -> (rows group, row)
+        for i, (circuit, n, terms) in enumerate(items):
+            n = int(n)
             rows, slots, n_params = build_template(circuit, n)
             ts, coef = _term_structure(terms, n)
             key = (tuple(rows), tuple(slots), n, ts)
+            if n >= self.rows_from:
+                if key not in rplans:
+                    rplans[key] = len(self.rplans)
+                    self.rplans.append([_RowsPlan(rows, slots, n, self.dtype, tile_bits, terms, use_jit=rows_jit),
+                                        [], [], n_params])
+                g = self.rplans[rplans[key]]
+                self.row_of[i] = (rplans[key], len(g[1]))
+                g[1].append(i)
+                g[2].append(coef)
+                self.circ.append((-1, coef, n_params))
+                continue
             if key not in plans:
                 plans[key] = len(self.plans)
                 self.plans.append(_Plan(rows, slots, n, ts, self.dtype, tile_bits))
@@ -220,10 +438,46 @@ class BatchVQE:
         dev = self.device
         rdt = np.float32 if self.dtype == torch.complex64 else np.float64
         cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
+        code = N.DESV_C64 if self.dtype == torch.complex64 else N.DESV_C128
+        self.code = code
+        self.graph = None
 
         def up(a):
             return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
 
+        # parameters: the persistent launch's circuits first, then every rows
+        # group as (rows x nparams) at its base
+        pers = [i for i, c in enumerate(self.circ) if c[0] >= 0]
+        theta_off = np.zeros(len(self.circ), np.int64)
+        coef_off = np.zeros(len(self.circ), np.int64)
+        t = c = 0
+        for i in pers:
+            pi, coef, npar = self.circ[i]
+            theta_off[i], coef_off[i] = t, c
+            t += max(npar, self.plans[pi].nparams, 1)
+            c += max(len(coef), 1)
+        self.groups: List[_RowsGroup] = []
+        group_base = []
+        for plan, idx, coefs, npar in self.rplans:
+            P = max(npar, plan.nparams, 1)
+            group_base.append(t)
+            for r, i in enumerate(idx):
+                theta_off[i] = t + r * P
+            t += P * len(idx)
+        self.theta_off = theta_off
+        self.ntheta = t
+        self.d_theta = torch.zeros(max(t, 1), dtype=torch.float64, device=dev)
+        self.d_grad = torch.zeros(max(t, 1), dtype=torch.float64, device=dev)
+        self.d_energy = torch.zeros(max(len(self.circ), 1), dtype=torch.float64, device=dev)
+        for (plan, idx, coefs, npar), base in zip(self.rplans, group_base):
+            g = _RowsGroup(plan, coefs, base, dev, code)
+            g.P = max(npar, plan.nparams, 1)
+            self.groups.append(g)
+        self.npersistent = len(pers)
+        if not pers:
+            self.args = None
+            self.max_n, self.max_pool = 9, 0
+            return
         self.d_passes = up(np.concatenate(pass_rows))
         self.d_ops = up(np.concatenate(op_rows))
         self.d_recipes = up(np.concatenate(rec_rows))
@@ -234,43 +488,29 @@ class BatchVQE:
         self.d_terms = up(terms)
         self.d_plans = up(np.array(plan_rows, PLAN_DTYPE))
         # circuits in decreasing cost; outputs stay in the caller's order
-        order = sorted(range(len(self.circ)), key=lambda i: -self.plans[self.circ[i][0]].cost)
-        crow = np.zeros(len(self.circ), CIRC_DTYPE)
-        theta_off, coef_off = [], []
-        t = c = 0
-        for i, (pi, coef, npar) in enumerate(self.circ):
-            theta_off.append(t)
-            coef_off.append(c)
-            t += max(npar, self.plans[pi].nparams, 1)
-            c += max(len(coef), 1)
-        self.theta_off = np.array(theta_off)
-        self.ntheta = t
+        order = sorted(pers, key=lambda i: -self.plans[self.circ[i][0]].cost)
+        crow = np.zeros(len(pers), CIRC_DTYPE)
         coefs = np.zeros(max(c, 1))
-        for i, (pi, coef, npar) in enumerate(self.circ):
+        for i in pers:
+            coef = self.circ[i][1]
             coefs[coef_off[i]:coef_off[i] + len(coef)] = coef
         for k, i in enumerate(order):
             pi = self.circ[i][0]
             crow[k] = (pi, i, theta_off[i], coef_off[i], theta_off[i], -1)
         self.d_circ = up(crow)
         self.d_coef = torch.from_numpy(coefs).to(dev)
-        self.d_theta = torch.zeros(max(t, 1), dtype=torch.float64, device=dev)
-        self.d_energy = torch.zeros(len(self.circ), dtype=torch.float64, device=dev)
-        self.d_grad = torch.zeros(max(t, 1), dtype=torch.float64, device=dev)
         self.max_n = max(p.n for p in self.plans)
         self.max_pool = max(p.pool_len for p in self.plans)
-        code = N.DESV_C64 if self.dtype == torch.complex64 else N.DESV_C128
-        self.code = code
         wsb = int(N.lib().desv_batch_workspace_bytes(code, max(self.max_n, 9), self.max_pool))
         self.d_ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
         a = BatchArgs()
-        a.ncirc = len(self.circ)
+        a.ncirc = len(pers)
         for f, t_ in (('circuits', self.d_circ), ('plans', self.d_plans), ('passes', self.d_passes),
                       ('ops', self.d_ops), ('recipes', self.d_recipes), ('cpool', self.d_cpool),
                       ('theta', self.d_theta), ('coef', self.d_coef), ('terms', self.d_terms),
                       ('energy', self.d_energy), ('grad', self.d_grad)):
             setattr(a, f, t_.data_ptr())
         self.args = a
-        self.graph = None
 
     # ------------------------------------------------------------------ run
     def nparams_list(self) -> List[int]:
@@ -286,10 +526,47 @@ class BatchVQE:
         self.d_theta.copy_(torch.from_numpy(host))
 
     def launch(self, stream=None):
+        """Queue the whole batch: the persistent launch over the narrow circuits,
+        then every rows group (prepare, forward passes, H psi with E and the
+        norm, adjoint passes)."""
+        self.launch_persistent(stream)
+        for g in self.groups:
+            g.launch(self.d_theta, self.d_grad, stream)
+
+    def launch_persistent(self, stream=None):
+        """Queue the persistent launch over the narrow circuits (if any)."""
+        if self.args is None:
+            return
         st = ctypes.c_void_p(N.stream_ptr(stream))
         N.check(N.lib().desv_batch_vqe(self.code, max(self.max_n, 9), self.max_pool, ctypes.byref(self.args),
                                        ctypes.c_void_p(self.d_ws.data_ptr()), self.d_ws.numel(), st),
                 'batched VQE')
+
+    def rows_algorithmic_bytes(self, group: '_RowsGroup') -> float:
+        """HBM bytes a rows group must move: |0...0> written once, every forward
+        pass reads and writes psi, the first Pauli pass reads psi and writes
+        lambda and later ones also read lambda, the norm reads psi (complex64),
+        every adjoint pass reads and writes psi and lambda."""
+        p = group.plan
+        es = 8 if p.dtype == torch.complex64 else 16
+        nf = int(np.sum(group.fwd_passes['op_end'] > group.fwd_passes['op_begin']))
+        npl = int(np.sum(group.ppasses['term_end'] > group.ppasses['term_begin']))
+        nb = int(np.sum(group.bwd_passes['op_end'] > group.bwd_passes['op_begin']))
+        per = 1 + 2 * nf + (2 + 3 * (npl - 1) if npl else 1) + (1 if p.dtype == torch.complex64 else 0) + 4 * nb
+        return float(group.B) * float(1 << p.n) * es * per
+
+    def launches_per_batch(self) -> int:
+        """Kernel launches of one batch (the persistent launch, and per rows
+        group: prepare, forward passes, Pauli passes and their reductions,
+        gradient zeroing, adjoint passes and their reductions)."""
+        k = 1 if self.args is not None else 0
+        for g in self.groups:
+            nf = int(np.sum(g.fwd_passes['op_end'] > g.fwd_passes['op_begin']))
+            npl = int(np.sum(g.ppasses['term_end'] > g.ppasses['term_begin']))
+            nb = int(np.sum(g.bwd_passes['op_end'] > g.bwd_passes['op_begin']))
+            nbr = int(np.sum((g.bwd_passes['op_end'] > g.bwd_passes['op_begin']) & (g.bwd_passes['nparams'] > 0)))
+            k += 1 + nf + npl + 1 + (2 if g.plan.dtype == torch.complex64 else 0) + 1 + nb + nbr
+        return k
 
     def capture(self):
         """Capture the launch in a CUDA graph (after one eager warm-up launch)."""
@@ -314,8 +591,17 @@ class BatchVQE:
             self.graph.replay()
         else:
             self.launch()
-        e = self.d_energy.cpu().numpy()
+        e = self.d_energy.cpu().numpy()[:len(self.circ)].copy()
         g = self.d_grad.cpu().numpy()
+        for grp, (plan, idx, _, _) in zip(self.groups, self.rplans):
+            ex = grp.expect.cpu().numpy()
+            # complex64: divide out the FP64 norm drift (<psi|psi> is 1 in exact
+            # arithmetic), as the persistent launch does
+            ratio = 1.0 / grp.norm.cpu().numpy() if plan.dtype == torch.complex64 else np.ones(len(idx))
+            for r, i in enumerate(idx):
+                e[i] = ex[r, 0] * ratio[r]
+                o = self.theta_off[i]
+                g[o:o + grp.P] *= ratio[r]
         grads = [g[self.theta_off[i]:self.theta_off[i] + self.circ[i][2]].copy() for i in range(len(self.circ))]
         return e, grads
 
@@ -372,13 +658,15 @@ def gather_results(indices: Sequence[int], energies: Sequence[float], grads: Seq
 
 
 class BatchForward:
-    """run_batch_jit's rows in ONE persistent launch: one circuit structure, one
-    parameter row per circuit, every row's final state written to its row of a
-    (B, 2^n) tensor.  The batched VQE kernel runs in its forward-only mode:
-    each row's matrices are built from its theta on the device, states of
-    <= 12 qubits stay in shared memory until written out, wider ones are
-    evolved in place in their output rows.  Replaces the reference's vmap
-    over one circuit shape (backends/statevector.py:496-584)."""
+    """run_batch_jit's rows: one circuit structure, one parameter row per
+    circuit, every row's final state written to its row of a (B, 2^n) tensor,
+    each row's matrices built from its theta on the device.  Replaces the
+    reference's vmap over one circuit shape (backends/statevector.py:496-584).
+
+    States of <= 12 qubits run in ONE persistent launch (the batched VQE
+    kernel's forward-only mode; each state stays in one CTA's shared memory
+    until written out).  Wider states run as rows: the output rows are evolved
+    in place, every fused pass over all rows in one launch over all SMs."""
 
     def __init__(self, rows, slots, n: int, dtype=torch.complex64, tile_bits=None):
         self.dtype = dtype
@@ -387,11 +675,46 @@ class BatchForward:
         if tile_bits is None:
             from . import autotune
             tile_bits = autotune.batch_tile_bits(dtype)
+        if self.n > RESIDENT_BITS:
+            self.rplan = _RowsPlan(rows, slots, self.n, dtype, int(tile_bits), forward_only=True)
+            self.plan = None
+            self.nparams = self.rplan.nparams
+            return
+        self.rplan = None
         self.plan = _Plan(rows, slots, self.n, (), dtype, int(tile_bits), forward_only=True)
         self.nparams = self.plan.nparams
 
+    def _run_rows(self, pb: np.ndarray) -> torch.Tensor:
+        p, dev, B = self.rplan, self.device, pb.shape[0]
+        rdt = np.float32 if self.dtype == torch.complex64 else np.float64
+        cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
+        npar = max(p.nparams, 1)
+        theta = np.zeros((B, npar))
+        theta[:, :pb.shape[1]] = pb
+        code = N.DESV_C64 if self.dtype == torch.complex64 else N.DESV_C128
+        out = torch.empty((B, 1 << p.n), dtype=self.dtype, device=dev)
+        pools = torch.empty((B, p.pool_stride), dtype=self.dtype, device=dev)
+        bufs = dict(recipes=torch.from_numpy(p.recipes.view(np.uint8).copy()).to(dev),
+                    cpool=torch.from_numpy(p.cpool.astype(cdt).view(rdt).copy()).to(dev),
+                    theta=torch.from_numpy(theta.reshape(-1)).to(dev),
+                    ops=torch.from_numpy((p.fwd.ops if len(p.fwd.ops) else np.zeros(1, N.OP_DTYPE))
+                                         .view(np.uint8).copy()).to(dev))
+        passes = np.ascontiguousarray(p.fwd.passes)
+        vp = ctypes.c_void_p
+        st = vp(N.stream_ptr())
+        N.check(N.lib().desv_rows_prepare(vp(out.data_ptr()), p.n, code, B, vp(bufs['recipes'].data_ptr()),
+                                          len(p.recipes), vp(bufs['theta'].data_ptr()), npar,
+                                          vp(bufs['cpool'].data_ptr()), vp(pools.data_ptr()), p.pool_stride, st),
+                'rows prepare')
+        kf, _ = p.kernels(dev.index if dev.index is not None else torch.cuda.current_device())
+        rows_forward(kf, out, p.n, code, B, passes, bufs['ops'], pools, p.pool_stride, st)
+        self._keep = (bufs, pools)     # alive until the stream has run the launches
+        return out
+
     def run(self, parameter_batch: np.ndarray) -> torch.Tensor:
         pb = np.asarray(parameter_batch, dtype=np.float64)
+        if self.rplan is not None:
+            return self._run_rows(pb)
         B = pb.shape[0]
         p = self.plan
         dev = self.device

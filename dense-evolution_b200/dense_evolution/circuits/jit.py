@@ -189,8 +189,13 @@ def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: 
     lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
              f'extern "C" __global__ void __launch_bounds__({1 << (tile_bits - 4)}, 1)',
              f'desv_jit_kernel({T} *phi, {T} *lam, TileGeom g, const desv_op *__restrict__ ops, '
-             f'const {T} *__restrict__ mats, int nparams, double *part) {{',
+             f'const {T} *__restrict__ mats, int nparams, double *part, RowStrides rs) {{',
              '    extern __shared__ __align__(128) unsigned char smem[];',
+             '    // rows: this grid row\'s (phi, lambda), pool and partial sums (zero strides: one state)',
+             '    phi += blockIdx.y * rs.amps;',
+             '    lam += blockIdx.y * rs.amps;',
+             '    mats += blockIdx.y * rs.mats;',
+             '    part += blockIdx.y * rs.part;',
              '    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;',
              f'    auto stages = [=]({T} *sphi, {T} *slam, uint64_t base, const uint64_t *ctab, int L, double *acc) {{',
              f'        {T} a[16], b[16];']
@@ -242,8 +247,11 @@ def pass_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: int
     T = 'float2' if complex64 else 'double2'
     lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
              f'extern "C" __global__ void __launch_bounds__({1 << (tile_bits - 4)}, {2 if complex64 else 1})',
-             f'desv_jit_kernel({T} *sv, TileGeom g, const {T} *__restrict__ mats) {{',
+             f'desv_jit_kernel({T} *sv, TileGeom g, const {T} *__restrict__ mats, RowStrides rs) {{',
              '    extern __shared__ __align__(128) unsigned char smem[];',
+             '    // rows: this grid row\'s state and pool (zero strides: one state)',
+             '    sv += blockIdx.y * rs.amps;',
+             '    mats += blockIdx.y * rs.mats;',
              '    const int lane = threadIdx.x & 31;',
              f'    auto stages = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L) {{',
              f'        {T} a[16];']

@@ -88,13 +88,13 @@ class PauliPlan:
             c = complex(coeff) * (1j ** ny)
             if complex(coeff).imag != 0:
                 self.all_real = False
-            rows.append((x, z, c))
+            rows.append((x, z, c, len(rows)))
         self.nterms = len(rows)
         K = min(tile_bits, n)
         lane = min(5, K)
         groups: Dict[int, list] = {}
-        for x, z, c in rows:
-            groups.setdefault(x, []).append((x, z, c))
+        for x, z, c, i in rows:
+            groups.setdefault(x, []).append((x, z, c, i))
         # greedy first-fit of flip masks into tiles (high bits >= lane)
         bins: List[Tuple[set, list]] = []
         direct: List[int] = []        # flip masks wider than a tile
@@ -114,6 +114,7 @@ class PauliPlan:
             if not placed:
                 bins.append((set(need), [x]))
         term_rows, pass_rows = [], []
+        order = []          # packed term row -> index of the term in the caller's list
         for H, members in bins:
             L = lane
             while True:
@@ -125,8 +126,9 @@ class PauliPlan:
             high = sorted(h for h in H if h >= L)
             begin = len(term_rows)
             for x in sorted(members):
-                for (xx, z, c) in groups[x]:
+                for (xx, z, c, i) in groups[x]:
                     term_rows.append((xx, z, c.real, c.imag))
+                    order.append(i)
             r = np.zeros((), dtype=N.PPASS_DTYPE)
             r['tile_bits'], r['low_bits'], r['term_begin'], r['term_end'] = K, L, begin, len(term_rows)
             hb = np.zeros(16, np.uint8)
@@ -136,12 +138,14 @@ class PauliPlan:
         for i in range(0, len(direct), 64):
             begin = len(term_rows)
             for x in direct[i:i + 64]:
-                for (xx, z, c) in groups[x]:
+                for (xx, z, c, k) in groups[x]:
                     term_rows.append((xx, z, c.real, c.imag))
+                    order.append(k)
             r = np.zeros((), dtype=N.PPASS_DTYPE)
             r['tile_bits'], r['low_bits'], r['term_begin'], r['term_end'] = 0, 0, begin, len(term_rows)
             pass_rows.append(r)
-        self.terms =np.array(term_rows, dtype=N.TERM_DTYPE) if term_rows else np.zeros(0, N.TERM_DTYPE)
+        self.terms = np.array(term_rows, dtype=N.TERM_DTYPE) if term_rows else np.zeros(0, N.TERM_DTYPE)
+        self.order = np.array(order, dtype=np.int64)
         self.passes = np.array(pass_rows, dtype=N.PPASS_DTYPE) if pass_rows else np.zeros(0, N.PPASS_DTYPE)
         self._dev = {}
         self._jit = {}

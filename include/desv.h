@@ -251,6 +251,38 @@ size_t desv_batch_workspace_bytes(int dtype, int max_n, int max_pool_len);
 int desv_batch_vqe(int dtype, int max_n, int max_pool_len, const desv_batch_args *args, void *workspace,
                    size_t workspace_bytes, void *stream);
 
+/* ---- rows: one circuit structure for many parameter rows (replaces
+ *      run_batch_jit's vmap over one circuit shape, backends/statevector.py:
+ *      496-584, and energy_fn + jax.grad per row, solvers/autodiff.py:92-169,
+ *      for circuits too wide for one CTA's shared memory).  The rows' states
+ *      are full-width tensors back to back (row r at r * 2^n amplitudes); every
+ *      pass covers all rows in one launch over all SMs, one grid row per state.
+ *      rows is in [1, 65535]; pools, term tables and gradients are per row at
+ *      the given strides. ------------------------------------------------------ */
+/* scratch for the Pauli and adjoint rows calls below */
+size_t desv_rows_scratch_bytes(int rows, int max_params_per_pass, int max_pauli_passes);
+/* pools + r * pool_stride <- the recipes applied to theta + r * theta_stride
+ * (pool_stride in complex elements); if states != NULL, every row's state is
+ * set to |0...0>. */
+int desv_rows_prepare(void *states, int n, int dtype, int rows, const desv_batch_recipe *recipes_dev, int nrec,
+                      const double *theta_dev, int64_t theta_stride, const void *cpool_dev, void *pools_dev,
+                      int64_t pool_stride, void *stream);
+/* desv_apply_passes on every row, row r with the pool at pools + r * pool_stride */
+int desv_apply_passes_rows(void *states, int n, int dtype, int rows, const desv_pass *passes, int npasses,
+                           const desv_op *ops_dev, const void *pools_dev, int64_t pool_stride, void *stream);
+/* out_r = H_r psi_r with row r's terms at terms + r * term_stride (records);
+ * expect_dev[2r..2r+1] = <psi_r|H_r psi_r> and norm_dev[r] = <psi_r|psi_r>
+ * when those pointers are not NULL (both overwritten). */
+int desv_pauli_matvec_rows(const void *psi, void *out, int n, int dtype, int rows, const desv_pauli_pass *passes,
+                           int npasses, const desv_pauli_term *terms_dev, int64_t term_stride, double *expect_dev,
+                           double *norm_dev, void *scratch, size_t scratch_bytes, void *stream);
+/* desv_adjoint_passes on every row: grad_dev[r * grad_stride + map[...]] +=
+ * 2 Re<lambda_r|G|phi_r> (not zeroed here). */
+int desv_adjoint_passes_rows(void *phi, void *lam, int n, int dtype, int rows, const desv_adj_pass *passes,
+                             int npasses, const desv_op *ops_dev, const void *pools_dev, int64_t pool_stride,
+                             const int32_t *map_dev, double *grad_dev, int64_t grad_stride, void *scratch,
+                             size_t scratch_bytes, void *stream);
+
 /* ---- reductions (FP64 accumulation; statevector.py:141-147,272-358,599-607,
  *      utils/measurement.py:71-94) ------------------------------------------ */
 /* out_dev[0] = sum |a_i|^2 (double, device) */
@@ -300,6 +332,11 @@ int desv_jit_compile_check(const char *src, const char *include_dirs, char *log,
  * compiled tile_bits); mats_dev is the same matrix pool desv_apply_passes reads. */
 int desv_jit_pass(void *handle, void *sv, int n, int dtype, const desv_pass *pass, const void *mats_dev,
                   void *stream);
+/* desv_jit_pass on `rows` states back to back (row r at r * 2^n amplitudes),
+ * row r with its pool at pools_dev + r * pool_stride (complex elements): the
+ * specialised form of desv_apply_passes_rows for one pass. */
+int desv_jit_pass_rows(void *handle, void *states, int n, int dtype, int rows, const desv_pass *pass,
+                       const void *pools_dev, int64_t pool_stride, void *stream);
 /* desv_pauli_expect (matvec == 0) or desv_pauli_matvec (matvec != 0) with the
  * tiled passes that have a specialised kernel (handles[p] != NULL, loaded with
  * kind 2 + the mode the pass runs in: 0 <H>; 1 the first H psi pass, 2 the
@@ -345,6 +382,13 @@ int desv_rot_pass(void *handle, void *sv, int n, const desv_pass *pass, const fl
 int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int dtype, const desv_adj_pass *pass,
                      const desv_op *ops_dev, const void *mats_dev, const int32_t *map_dev, double *grad_dev,
                      void *scratch, size_t scratch_bytes, void *stream);
+/* desv_jit_adjoint on `rows` (phi, lambda) pairs back to back: the specialised
+ * form of desv_adjoint_passes_rows for one pass (pools at pool_stride, row r's
+ * gradient at grad_dev + r * grad_stride; scratch of desv_rows_scratch_bytes). */
+int desv_jit_adjoint_rows(void *handle, void *phi, void *lam, int n, int dtype, int rows, const desv_adj_pass *pass,
+                          const desv_op *ops_dev, const void *pools_dev, int64_t pool_stride,
+                          const int32_t *map_dev, double *grad_dev, int64_t grad_stride, void *scratch,
+                          size_t scratch_bytes, void *stream);
 
 /* ---- Pauli sums (replaces pauli_sum_expectation / pauli_sum_matvec,
  *      physics/observables.py:63-186,250-308) ------------------------------- */

@@ -51,3 +51,45 @@ def test_batch_plan_energy_and_gradient(n):
     assert float(np.real(np.vdot(psi, lam))) == pytest.approx(e_ref, abs=1e-12)
     fd = O.fd_gradient(theta, orows, n, terms, h=1e-5)
     assert np.allclose(grad, fd, atol=1e-7)
+
+
+@pytest.mark.parametrize('n,dtype_name', [(13, 'complex64'), (14, 'complex128')])
+def test_rows_plan_energy_and_gradient(n, dtype_name):
+    """The rows plan of one structure (forward tiles of 12 bits, adjoint tiles
+    of the single-circuit width, local gradient slots with a parameter map)
+    gives every row its energy and gradient: pools rebuilt from each row's
+    theta by the recipes, each row's term table with its own J_z folded into
+    the plan's packed term order."""
+    import torch
+    from dense_evolution.batch import _RowsPlan, hea_xxz_batch
+    from dense_evolution.solvers.autodiff import build_template
+    items = hea_xxz_batch([n, n], 2, [0.7, 1.3])
+    circ = items[0][0]
+    rows, slots, npar = build_template(circ, n)
+    p = _RowsPlan(rows, slots, n, getattr(torch, dtype_name), 12, terms=items[0][2])
+    assert all(int(ps['tile_bits']) == 12 for ps in p.fwd.passes)
+    coefs = [[float(c) for c, _ in it[2]] for it in items]
+    table = p.term_rows(coefs)
+    assert table.shape == (2, len(items[0][2]))
+    orows, _ = O.energy_template([{'name': c[0], 'qubits': [q for q in c[1:] if isinstance(q, int)]}
+                                  for c in circ], n)
+    for r, (_, _, terms) in enumerate(items):
+        theta = np.random.default_rng(100 + r).uniform(-np.pi, np.pi, npar)
+        pool = _recipe_pool(p, theta, p.cpool.astype(np.complex128))
+        psi = run_passes(O.zero_state(n), n, p.fwd.passes, p.fwd.ops, pool)
+        # H psi from the row's packed term table: (P psi)[i] = psi[i ^ x] c (-1)^popcount((i ^ x) & z)
+        lam = np.zeros_like(psi)
+        idx = np.arange(1 << n)
+        for t in table[r]:
+            src = idx ^ int(t['xmask'])
+            sign = 1 - 2 * (np.array([bin(v).count('1') for v in (src & int(t['zmask']))]) & 1)
+            lam += (t['cre'] + 1j * t['cim']) * sign * psi[src]
+        assert np.max(np.abs(lam - O.pauli_sum_matvec(psi, terms))) < 1e-12
+        grad = np.zeros(npar)
+        _, _, grad = run_passes(psi, n, p.bwd.passes, p.bwd.ops, pool, lam=lam, grad=grad,
+                                param_map=np.asarray(p.bwd.param_map))
+        e_ref, psi_ref = O.energy(theta, orows, n, terms)
+        assert np.max(np.abs(psi - psi_ref)) < 1e-12
+        assert float(np.real(np.vdot(psi, lam))) == pytest.approx(e_ref, abs=1e-12)
+        fd = O.fd_gradient(theta, orows, n, terms, h=1e-5, indices=[0, npar // 2, npar - 1])
+        assert np.allclose(grad[[0, npar // 2, npar - 1]], fd, atol=1e-7)

@@ -123,9 +123,9 @@ def test_run_batch_jit_matches_run_circuit(de):
 
 @pytest.mark.parametrize('n,f32', [(14, False), (14, True), (9, True)])
 def test_run_batch_jit_one_launch_rows(de, n, f32):
-    """run_batch_jit's rows in one persistent launch: resident (<= 12 qubits)
-    and streamed (evolved in place in their output rows) states, both
-    precisions, against the oracle per row."""
+    """run_batch_jit's rows: resident states (<= 12 qubits, one persistent
+    launch) and wider ones (the rows path: every pass over all output rows in
+    one launch), both precisions, against the oracle per row."""
     rng = np.random.default_rng(n)
     base = [('h', q) for q in range(n)] + [('ry', q, 0.0) for q in range(n)] + \
         [('cx', q, q + 1) for q in range(n - 1)] + [('rx', q, 0.0) for q in range(0, n, 2)] + \

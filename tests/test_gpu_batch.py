@@ -70,3 +70,33 @@ def test_batch_tile_widths_agree(k):
     assert np.allclose(e, e_ref, atol=1e-10)
     assert all(np.allclose(x, y, atol=1e-10) for x, y in zip(g, g_ref))
     assert N.device_status() in (None, 0)
+
+
+@pytest.mark.parametrize('f32', [False, True])
+def test_rows_groups_match_persistent_launch(f32):
+    """Circuits wider than 12 qubits run as rows (one launch per pass over all
+    circuits of a structure); forcing them into the persistent launch (one CTA
+    per circuit) must give the same energies and gradients: complex128 to
+    1e-10, complex64 energies to the 1e-6 bar and gradients to 1e-5."""
+    from dense_evolution import _native as N
+    from dense_evolution.batch import BatchVQE, hea_xxz_batch
+    rng = np.random.default_rng(21)
+    ns = [13, 16, 13, 9, 14, 16, 13, 12, 14]
+    items = hea_xxz_batch(ns, 3, rng.uniform(0.5, 1.5, len(ns)))
+    th = [rng.uniform(-np.pi, np.pi, 6 * n) for n in ns]
+    rows = BatchVQE(items, use_float32=f32)
+    assert len(rows.groups) == 3 and [len(g[1]) for g in rows.rplans] == [3, 2, 2]
+    pers = BatchVQE(items, use_float32=f32, rows_from=99)
+    assert not pers.groups
+    e_r, g_r = rows.run(th)
+    e_p, g_p = pers.run(th)
+    assert np.allclose(e_r, e_p, atol=1e-6 if f32 else 1e-10)
+    assert all(np.allclose(x, y, atol=1e-5 if f32 else 1e-10) for x, y in zip(g_r, g_p))
+    # graph replay of the rows launches with new angles
+    th2 = [t - 0.2 for t in th]
+    e_g, g_g = rows.run(th2, use_graph=True)
+    e_e, g_e = pers.run(th2)
+    assert np.allclose(e_g, e_e, atol=1e-6 if f32 else 1e-10)
+    assert all(np.allclose(x, y, atol=1e-5 if f32 else 1e-10) for x, y in zip(g_g, g_e))
+    assert N.device_status() in (None, 0)
+
