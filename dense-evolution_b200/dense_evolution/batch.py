@@ -525,13 +525,48 @@ class BatchVQE:
             host[self.theta_off[i]:self.theta_off[i] + th.size] = th
         self.d_theta.copy_(torch.from_numpy(host))
 
+    # streams the independent parts of a batch are spread over
+    LANES = 4
+
     def launch(self, stream=None):
-        """Queue the whole batch: the persistent launch over the narrow circuits,
-        then every rows group (prepare, forward passes, H psi with E and the
-        norm, adjoint passes)."""
-        self.launch_persistent(stream)
-        for g in self.groups:
-            g.launch(self.d_theta, self.d_grad, stream)
+        """Queue the whole batch: the persistent launch over the narrow circuits
+        and every rows group (prepare, forward passes, H psi with E and the
+        norm, adjoint passes).  The parts are independent, so they run on up to
+        LANES streams forked from `stream` and joined back into it (largest
+        parts first, each to the least loaded lane): small groups and the tails
+        of large passes fill the SMs that a single part leaves idle.  The
+        fork and join are events, so a CUDA graph captures them too."""
+        main = stream if stream is not None else torch.cuda.current_stream()
+        parts = [(float(self.rows_algorithmic_bytes(g)), k) for k, g in enumerate(self.groups)]
+        if self.args is not None:
+            parts.append((0.0, -1))
+        nl = min(self.LANES, len(parts))
+        if nl <= 1:
+            self.launch_persistent(main)
+            for g in self.groups:
+                g.launch(self.d_theta, self.d_grad, main)
+            return
+        side = getattr(self, '_lanes', None)
+        if side is None or len(side) < nl - 1 or side[0].device != main.device:
+            side = [torch.cuda.Stream(device=main.device) for _ in range(self.LANES - 1)]
+            self._lanes = side
+        lanes = [main] + side[:nl - 1]
+        fork = torch.cuda.Event()
+        fork.record(main)
+        for s in lanes[1:]:
+            s.wait_event(fork)
+        load = [0.0] * nl
+        for cost, k in sorted(parts, key=lambda x: -x[0]):
+            li = min(range(nl), key=lambda i: (load[i], i))
+            load[li] += cost
+            if k < 0:
+                self.launch_persistent(lanes[li])
+            else:
+                self.groups[k].launch(self.d_theta, self.d_grad, lanes[li])
+        for s in lanes[1:]:
+            join = torch.cuda.Event()
+            join.record(s)
+            main.wait_event(join)
 
     def launch_persistent(self, stream=None):
         """Queue the persistent launch over the narrow circuits (if any)."""
