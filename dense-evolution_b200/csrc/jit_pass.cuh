@@ -224,6 +224,13 @@ __device__ __forceinline__ void jit_adjoint_kernel(T *phi, T *lam, const TileGeo
     }
 }
 
+// n (|n| < 2^22) as a float without the conversion unit: 1.5 * 2^23 + n has
+// the bits 0x4B400000 + n, from which 1.5 * 2^23 is subtracted exactly
+__device__ __forceinline__ float small_int_to_float(int n) {
+    return __int_as_float(0x4B400000 + n) - 12582912.0f;
+}
+__device__ __forceinline__ double small_int_to_double(int n) { return (double)n; }
+
 // Pauli-sum pass over psi tiles (MODE 0: <H> only, 1: write H psi, 2: add
 // into H psi): `body(tile, base, ctab, L, ere, eim)` evaluates the pass's terms
 // (compiled in) for the tile's amplitudes.  The FP64 energy partials are

@@ -186,8 +186,9 @@ def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: 
     gate is applied to phi (a) and lambda (b); a GRAD op adds its probe
     2 Re<lambda|G|phi> (the factor 2 comes in the reduction) to its slot."""
     T = 'float2' if complex64 else 'double2'
+    minb = _adjoint_min_blocks(tile_bits, nbuf, complex64)
     lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
-             f'extern "C" __global__ void __launch_bounds__({1 << (tile_bits - 4)}, 1)',
+             f'extern "C" __global__ void __launch_bounds__({1 << (tile_bits - 4)}, {minb})',
              f'desv_jit_kernel({T} *phi, {T} *lam, TileGeom g, const desv_op *__restrict__ ops, '
              f'const {T} *__restrict__ mats, int nparams, double *part, RowStrides rs) {{',
              '    extern __shared__ __align__(128) unsigned char smem[];',
@@ -235,10 +236,23 @@ def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: 
 
 
 def adjoint_nbuf_for(tile_bits: int, complex64: bool) -> int:
-    """Ring depth of the adjoint interpreter for this tile width (k_adjoint.cu)."""
+    """Ring depth of the adjoint interpreter for this tile width (k_adjoint.cu);
+    DESV_ADJ_NBUF overrides it for the specialised complex64 kernels (tuning)."""
     if complex64:
+        v = os.environ.get('DESV_ADJ_NBUF', '')
+        if v in ('2', '3', '4'):
+            return int(v)
         return 3 if tile_bits >= 11 else 4
     return 3 if tile_bits >= 10 else 4
+
+
+def _adjoint_min_blocks(tile_bits: int, nbuf: int, complex64: bool) -> int:
+    """CTAs per SM the specialised adjoint kernel's registers are bounded for:
+    shared memory holds two CTAs of 11-bit tiles with three ring slots (no
+    register bound needed), three with two slots (at most 170 registers)."""
+    if complex64 and tile_bits == 11 and nbuf == 2:
+        return 3
+    return 1
 
 
 def pass_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: int, complex64: bool,
@@ -292,6 +306,128 @@ def _tile_local(m: int, L: int, high) -> int:
     return x
 
 
+def _expect_source(terms: np.ndarray, K: int, L: int, high, complex64: bool) -> str:
+    """CUDA source of one specialised <H> pass (mode 0).
+
+    Per amplitude only single-precision work: the product w = Re(conj(a) p)
+    with the partner p = psi[j ^ x] (and Im(conj(a) p) where a term needs it)
+    in the state's precision, added with its integer sign weight into
+    per-thread sums, one per coefficient class of the pass.  Once per tile each
+    sum is widened and multiplied by its FP64 coefficient into the FP64
+    energy.  The interpreter widens every partner to FP64 for every flip mask
+    (two conversions per mask and amplitude); those conversions bound it.
+
+    Terms: (P psi)[i] = psi[i ^ x] c (-1)^popcount((i ^ x) & z) with c the
+    coefficient times i^(number of Y).  S = sum_i sign conj(a_i) p_i is real
+    when the number of Y is even and imaginary when it is odd, so a term with a
+    real c and an even Y count adds c S_re to Re<H> and nothing to Im<H>; every
+    other term keeps both parts."""
+    T = 'float2' if complex64 else 'double2'
+    R = 'float' if complex64 else 'double'
+    high = [int(h) for h in high[:K - L]]
+    tile_mask = ((1 << L) - 1) | sum(1 << h for h in high)
+    lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
+             'extern "C" __global__ void __launch_bounds__(256)',
+             f'desv_jit_kernel(const {T} *psi, {T} *out, TileGeom g, int want_e, double *part) {{',
+             '    extern __shared__ __align__(128) unsigned char smem[];',
+             f'    auto body = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L, double &ere, double &eim) {{']
+    groups = {}
+    for k, t in enumerate(terms):
+        groups.setdefault(int(t['xmask']), []).append(k)
+    for k, t in enumerate(terms):
+        zo = int(t['zmask']) & ~tile_mask
+        if zo:
+            lines.append(f'        const uint32_t pb{k} = (uint32_t)__popcll(base & {_hex(zo)}) & 1u;')
+    plan = []
+    acc = []            # accumulator names
+    for gi, (x, ks) in enumerate(groups.items()):
+        xl = _tile_local(x, L, high)
+        classes, outside, single, cplx = [], [], [], []
+        for k in ks:
+            t = terms[k]
+            zl = _tile_local(int(t['zmask']) & tile_mask, L, high)
+            zo = int(t['zmask']) & ~tile_mask
+            cre, cim = float(t['cre']), float(t['cim'])
+            ny_odd = bin(int(t['xmask']) & int(t['zmask'])).count('1') & 1
+            if cim != 0.0 or ny_odd:
+                cplx.append((k, zl, zo, cre, cim))
+            elif zl == 0:
+                outside.append((k, zo, cre))
+            elif zo == 0 and bin(zl).count('1') <= 2:
+                lo = (zl & -zl).bit_length() - 1
+                d = zl.bit_length() - 1 - lo
+                for cl in classes:
+                    if cl[0] == cre and cl[1] == d and not (cl[2] >> lo) & 1:
+                        cl[2] |= 1 << lo
+                        cl[3] += 1
+                        break
+                else:
+                    classes.append([cre, d, 1 << lo, 1])
+            else:
+                single.append((k, zl, zo, cre))
+        plan.append((xl, classes, outside, single, cplx))
+    # per-thread sums of this tile's amplitudes
+    decl = []
+    for gi, (xl, classes, outside, single, cplx) in enumerate(plan):
+        if outside:
+            decl.append(f'so{gi}')
+        decl += [f'sc{gi}_{ci}' for ci in range(len(classes))]
+        decl += [f'ss{gi}_{si}' for si in range(len(single))]
+        for k, *_ in cplx:
+            decl += [f'sr{k}', f'si{k}']
+    lines += [f'        {R} {", ".join(n + " = 0" for n in decl)};'] if decl else []
+    lines += ['#pragma unroll',
+              f'        for (uint32_t j0 = threadIdx.x; j0 < {1 << K}u; j0 += 1024u) {{',
+              '#pragma unroll',
+              '            for (int r = 0; r < 4; ++r) {',
+              '                const uint32_t j = j0 + r * 256u;',
+              f'                const {T} a = s[j];']
+    for gi, (xl, classes, outside, single, cplx) in enumerate(plan):
+        lines.append('                {')
+        lines.append(f'                    const uint32_t jx = j ^ {xl}u;')
+        lines.append(f'                    const {T} q = s[jx];')
+        lines.append(f'                    const {R} w = a.x * q.x + a.y * q.y;')
+        if cplx:
+            lines.append(f'                    const {R} wi = a.x * q.y - a.y * q.x;')
+        if outside:
+            lines.append(f'                    so{gi} += w;')
+        for ci, (c, d, m, cnt) in enumerate(classes):
+            pc = f'__popc(jx & {m}u)' if d == 0 else f'__popc((jx ^ (jx >> {d})) & {m}u)'
+            lines.append(f'                    sc{gi}_{ci} += small_int_to_{R}({cnt} - 2 * (int){pc}) * w;')
+        for si, (k, zl, zo, c) in enumerate(single):
+            lines.append(f'                    ss{gi}_{si} += (__popc(jx & {zl}u) & 1u) ? -w : w;')
+        for k, zl, zo, cre, cim in cplx:
+            if zl:
+                lines.append(f'                    {{ const bool ng = (__popc(jx & {zl}u) & 1u) != 0; '
+                             f'sr{k} += ng ? -w : w; si{k} += ng ? -wi : wi; }}')
+            else:
+                lines.append(f'                    sr{k} += w; si{k} += wi;')
+        lines.append('                }')
+    lines += ['            }', '        }']
+    # widen once per tile: FP64 coefficients times the sums
+    er, ei = [], []
+    for gi, (xl, classes, outside, single, cplx) in enumerate(plan):
+        if outside:
+            const = sum(c for (_, zo, c) in outside if not zo)
+            ts = [f'(pb{k} ? {-c!r} : {c!r})' for (k, zo, c) in outside if zo]
+            er.append(f'({" + ".join(([repr(const)] if const else []) + ts) or "0.0"}) * (double)so{gi}')
+        for ci, (c, d, m, cnt) in enumerate(classes):
+            er.append(f'{c!r} * (double)sc{gi}_{ci}')
+        for si, (k, zl, zo, c) in enumerate(single):
+            cc = f'(pb{k} ? {-c!r} : {c!r})' if zo else repr(c)
+            er.append(f'{cc} * (double)ss{gi}_{si}')
+        for k, zl, zo, cre, cim in cplx:
+            sg = f'(pb{k} ? -1.0 : 1.0) * ' if zo else ''
+            er.append(f'{sg}({cre!r} * (double)sr{k} - {cim!r} * (double)si{k})')
+            ei.append(f'{sg}({cre!r} * (double)si{k} + {cim!r} * (double)sr{k})')
+    if er:
+        lines.append('        ere += ' + ' + '.join(er) + ';')
+    if ei:
+        lines.append('        eim += ' + ' + '.join(ei) + ';')
+    lines += ['    };', f'    jit_pauli_kernel<{T}, {K}, 4>(psi, g, want_e, part, smem, body);', '}', '']
+    return '\n'.join(lines)
+
+
 def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: int, complex64: bool) -> str:
     """CUDA source of one specialised Pauli pass (the interpreter k_pauli with
     the pass's terms compiled in): mode 0 <H> only, 1 write H psi, 2 add into
@@ -299,6 +435,8 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
     coefficients take the two-FMA form.  (P psi)[i] = psi[i ^ x] c
     (-1)^popcount((i ^ x) & z); the z bits outside the tile give a per-tile
     parity."""
+    if mode == 0:
+        return _expect_source(terms, tile_bits, low_bits, high, complex64)
     T = 'float2' if complex64 else 'double2'
     R = 'float' if complex64 else 'double'
     K, L = tile_bits, low_bits

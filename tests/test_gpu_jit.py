@@ -172,11 +172,16 @@ def test_specialised_pauli_passes_match_interpreter_and_oracle(n, dtname, monkey
         torch.cuda.synchronize()
         got[flag] = (e, out.cpu().numpy(), float(e2[0]))
     e_tol, v_tol = (1e-12, 1e-13) if dt == torch.complex128 else (1e-9, 1e-6)
-    assert got['1'][0] == pytest.approx(got['0'][0], abs=e_tol)
+    # complex64 <H> passes form each amplitude's products Re(conj(a) p) in FP32
+    # (sums widened to FP64 once per tile): random rounding of about 6e-8 of
+    # each product, which on this unit state of 2^13 amplitudes sums to a few
+    # 1e-9 per term; 1e-7 bounds it, ten times under the 1e-6 energy bar
+    x_tol = 1e-12 if dt == torch.complex128 else 1e-7
+    assert got['1'][0] == pytest.approx(got['0'][0], abs=x_tol)
     assert got['1'][2] == pytest.approx(got['0'][2], abs=e_tol)
     assert np.max(np.abs(got['1'][1] - got['0'][1])) <= v_tol
     if n <= 13:
         ref_v = psi.cpu().numpy().astype(np.complex128)
-        assert got['1'][0] == pytest.approx(O.pauli_sum_expectation(ref_v, terms, n), abs=1e-9)
+        assert got['1'][0] == pytest.approx(O.pauli_sum_expectation(ref_v, terms, n), abs=max(x_tol, 1e-9))
         assert np.max(np.abs(got['1'][1] - O.pauli_sum_matvec(ref_v, terms, n))) <= (1e-12 if dt == torch.complex128
                                                                                       else 1e-5)
