@@ -547,6 +547,8 @@ def pauli_roofline(prog, theta, n, reps=10):
     for name, fn, nbytes in (('expect', lambda: plan.expect(psi), plan.npasses * amp),
                              ('matvec', lambda: plan.matvec(psi, out), plan.npasses * amp + amp +
                               (plan.npasses - 1) * 2 * amp)):
+        # an NVTX range per kind, so that a profiler can pick these launches out
+        torch.cuda.nvtx.range_push(f'pauli_{name}')
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
@@ -556,6 +558,7 @@ def pauli_roofline(prog, theta, n, reps=10):
             fn()
         e1.record()
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         ms = e0.elapsed_time(e1) / reps
         res[name] = {'ms': ms, 'algorithmic_bytes': nbytes, 'gbs': nbytes / ms / 1e6,
                      'frac_of_hbm': nbytes / ms / 1e6 / _peaks()[0]}
@@ -575,10 +578,12 @@ def run_batch(args, layers=6):
     ncirc = args.batch_circuits
     rng = np.random.default_rng(SEED)
     ns = rng.integers(10, 21, ncirc)
+    if args.batch_qubits:
+        ns = np.full(ncirc, args.batch_qubits)      # one width only (profiling a single rows group)
     jz = rng.uniform(0.5, 1.5, ncirc)
     srng = np.random.default_rng(SEED + 7)
     sample = hea_xxz_batch(srng.integers(10, 21, 256), layers, srng.uniform(0.5, 1.5, 256))
-    tune = autotune.tune_batch(sample, use_float32=True)
+    tune = autotune.tune_batch(sample, use_float32=True) if not args.batch_no_tune else {}
     t0 = time.perf_counter()
     b = BatchVQE(hea_xxz_batch(ns, layers, jz), use_float32=True)
     build_s = time.perf_counter() - t0
@@ -635,7 +640,8 @@ def run_batch(args, layers=6):
         rows_tab.append({'qubits': g.plan.n, 'rows': g.B, 'ms': gms, 'algorithmic_bytes': gb,
                          'gbs': gb / (gms / 1e3) / 1e9, 'frac_of_hbm': gb / (gms / 1e3) / 1e9 / _peaks()[0]})
     parts['rows_groups'] = rows_tab
-    return {'workload': f'{ncirc} circuits, qubits uniform in 10..20, HEA {layers} layers (RY,RZ + CX ladder), '
+    widths = f'{args.batch_qubits} qubits each' if args.batch_qubits else 'qubits uniform in 10..20'
+    return {'workload': f'{ncirc} circuits, {widths}, HEA {layers} layers (RY,RZ + CX ladder), '
                         f'XXZ open chain J_xy=1, J_z~U[0.5,1.5]; energy + adjoint gradient per circuit',
             'ms_per_batch': ms, 'circuits_per_s': ncirc / (ms / 1e3), 'grads_per_s': ncirc / (ms / 1e3),
             'e2e_ms_per_batch': e2e_ms, 'plans': len(b.plans) + len(b.groups),
@@ -717,6 +723,10 @@ def main():
     ap.add_argument('--vqe-qubits', type=int, default=VQE_N, help='VQE block width (default 24)')
     ap.add_argument('--vqe-no-shift', action='store_true', help='VQE block without the parameter-shift leg')
     ap.add_argument('--batch-circuits', type=int, default=4096, help='batch block size (default 4096)')
+    ap.add_argument('--batch-no-tune', action='store_true',
+                    help='skip the batch tile-width autotuner (its cached or default width is used)')
+    ap.add_argument('--batch-qubits', type=int, default=0,
+                    help='give every batch circuit this width (default 0: widths uniform in 10..20)')
     ap.add_argument('--qubits', type=int, default=N_QUBITS, help='headline circuit width (default 30)')
     ap.add_argument('--layers', type=int, default=LAYERS, help='headline circuit depth (default 40)')
     args = ap.parse_args()

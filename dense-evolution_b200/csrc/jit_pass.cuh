@@ -106,18 +106,17 @@ __device__ __forceinline__ double jit_grad_lane(const T (&a)[16], const T (&b)[1
 template <int S, int CS, typename T>
 __device__ __forceinline__ double jit_grad_y(const T (&a)[16], const T (&b)[16], decltype(T().x) h) {
     typedef decltype(T().x) R;
-    R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    // (s0, s1) and (s2, s3) as packed pairs: one packed FMA per pair and product
+    T s01 = mk(R(0), R(0)), s23 = mk(R(0), R(0));
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         if ((j >> S) & 1) continue;
         if (CS >= 0 && !((j >> CS) & 1)) continue;
         const int j1 = j | (1 << S);
-        s0 = fma(b[j1].x, a[j].x, s0);
-        s1 = fma(b[j1].y, a[j].y, s1);
-        s2 = fma(b[j].x, a[j1].x, s2);
-        s3 = fma(b[j].y, a[j1].y, s3);
+        s01 = bfma(b[j1], a[j], s01);
+        s23 = bfma(b[j], a[j1], s23);
     }
-    return (double)(((s0 + s1) - (s2 + s3)) * h);
+    return (double)(((s01.x + s01.y) - (s23.x + s23.y)) * h);
 }
 // X type, G = [[0, -i h], [-i h, 0]] with h real (rx): h (Im conj(b0) a1 + Im conj(b1) a0),
 // Im conj(b) a = b.x a.y - b.y a.x.

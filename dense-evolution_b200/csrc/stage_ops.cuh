@@ -67,8 +67,12 @@ __device__ __forceinline__ void m1_reg(T (&a)[16], const M22<T> &m) {
             a[j] = cmul(m.m01, x1);
             a[j1] = cmul(m.m10, x0);
         } else if (VAR == V_REAL) {
-            a[j] = rfma(m.m01.x, x1, rfma(m.m00.x, x0, mk(decltype(x0.x)(0), decltype(x0.x)(0))));
-            a[j1] = rfma(m.m11.x, x1, rfma(m.m10.x, x0, mk(decltype(x0.x)(0), decltype(x0.x)(0))));
+            // (v, v) pairs of the real entries: one packed multiply and one packed
+            // FMA per amplitude (the same roundings as the scalar form)
+            const T p00 = mk(m.m00.x, m.m00.x), p01 = mk(m.m01.x, m.m01.x);
+            const T p10 = mk(m.m10.x, m.m10.x), p11 = mk(m.m11.x, m.m11.x);
+            a[j] = bfma(p01, x1, bmul(p00, x0));
+            a[j1] = bfma(p11, x1, bmul(p10, x0));
         } else if (VAR == V_BREAL) {
             a[j] = bfma(m.m01, x1, bmul(m.m00, x0));
             a[j1] = bfma(m.m11, x1, bmul(m.m10, x0));
