@@ -164,6 +164,50 @@ __device__ __forceinline__ double jit_grad_dim(const T (&a)[16], const T (&b)[16
     return (double)acc;
 }
 
+// Tangent forms of the adjoint passes (the tangent variant of a backward pass).
+// A real rotation [[c, -s], [s, c]] on register slot S becomes
+// x0 -= t x1, x1 += t x0 with t = s / c: one packed FMA per amplitude, and the
+// result is 1/c times the exact one.  A conjugate pair of phases
+// diag(c + i s, c - i s) on index bit b becomes x += i t x (bit 0) or
+// x -= i t x (bit 1): two FMAs per amplitude, again 1/c times the exact one.
+// The host keeps the running product of the 1/c of a pass: every gradient
+// probe is multiplied by the inverse square of it (both arrays carry it) and
+// the pass ends by multiplying both arrays by its inverse.
+template <int S, typename T>
+__device__ __forceinline__ void tan_rot(T (&a)[16], decltype(T().x) t) {
+    const T pt = mk(t, t), nt = mk(-t, -t);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if ((j >> S) & 1) continue;
+        const int j1 = j | (1 << S);
+        const T x0 = a[j], x1 = a[j1];
+        a[j] = bfma(nt, x1, x0);
+        a[j1] = bfma(pt, x0, x1);
+    }
+}
+// SA >= 0: the phase's bit is register slot SA; SA < 0: the thread-fixed bit fbit
+template <int SA, typename T>
+__device__ __forceinline__ void tan_phase(T (&a)[16], decltype(T().x) t, int fbit) {
+    typedef decltype(T().x) R;
+    const R tf = fbit ? -t : t;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const R tt = SA >= 0 ? (((j >> SA) & 1) ? -t : t) : tf;
+        const R re = a[j].x, im = a[j].y;
+        a[j].x = fma(-tt, im, re);
+        a[j].y = fma(tt, re, im);
+    }
+}
+template <typename T>
+__device__ __forceinline__ void scale_both(T (&a)[16], T (&b)[16], decltype(T().x) f) {
+    const T ff = mk(f, f);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        a[j] = bmul(ff, a[j]);
+        b[j] = bmul(ff, b[j]);
+    }
+}
+
 // Controlled X on register slot S (control register slot CS, or none): a
 // swap of register pairs, no arithmetic.
 template <int S, int CS, typename T>

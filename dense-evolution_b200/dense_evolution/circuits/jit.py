@@ -148,7 +148,23 @@ def _op_code(o, words: np.ndarray, wpe: int) -> str:
     return call
 
 
-def _grad_code(o, words: Optional[np.ndarray] = None, wpe: int = 2) -> str:
+def grad_reads_pool(o, words: Optional[np.ndarray] = None, wpe: int = 2) -> bool:
+    """True when the probe's code reads its generator from the pool at run time
+    (False: the generator is compiled in as immediates, _grad_code's y, x and
+    imaginary-diagonal forms)."""
+    g = mat_values(words, int(o['mat']), wpe)
+    if int(o['s1']) == 1:
+        return not (g is not None and all(v.real == 0 for v in g))
+    if int(o['s0']) >= 16:
+        return True
+    if g is not None and g[0] == 0 and g[3] == 0 and g[1].imag == 0 and g[2].imag == 0 and g[1] == -g[2]:
+        return False
+    if g is not None and g[0] == 0 and g[3] == 0 and g[1].real == 0 and g[2].real == 0 and g[1] == g[2]:
+        return False
+    return True
+
+
+def _grad_code(o, words: Optional[np.ndarray] = None, wpe: int = 2, corr: bool = False) -> str:
     """A GRAD probe with its generator's placement compiled in (grad_term's
     forms); generators of the known shapes (ry: real antisymmetric, rx: -i h X,
     rz / p / cp / crz: imaginary diagonal) get probes with their values as
@@ -175,12 +191,15 @@ def _grad_code(o, words: Optional[np.ndarray] = None, wpe: int = 2) -> str:
     else:
         call = f'jit_grad_reg<{int(o["s0"])}, {cs}>(a, b, {mp})'
     pred = f'(tg & {_hex(o["cmask"])}) == {_hex(o["cval"])}'
-    return (f'{{ double v = {call}; v = warp_sum_d({pred} ? v : 0.0); '
+    # tangent passes: an immediate-form probe is scaled by the correction the
+    # host writes into its (otherwise unread) pool slot
+    cv = f' v *= (double)mats[{int(o["mat"])}].x;' if corr and not grad_reads_pool(o, words, wpe) else ''
+    return (f'{{ double v = {call}; v = warp_sum_d({pred} ? v : 0.0);{cv} '
             f'if (lane == 0) acc[warp * nparams + {int(o["param"])}] += v; }}')
 
 
 def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: int, complex64: bool,
-                   words: np.ndarray, wpe: int) -> str:
+                   words: np.ndarray, wpe: int, tangent=None) -> str:
     """CUDA source of one specialised adjoint backward pass over ops[begin:end]
     (absolute indices into the op array the kernel receives): every inverse
     gate is applied to phi (a) and lambda (b); a GRAD op adds its probe
@@ -217,12 +236,26 @@ def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: 
         for q in range(k + 1, k + 1 + cnt):
             o = ops[q]
             if int(o['kind']) == N.OP_GRAD:
-                lines.append('            ' + _grad_code(o, words, wpe))
+                lines.append('            ' + _grad_code(o, words, wpe, corr=tangent is not None))
+                continue
+            if tangent is not None and q in tangent[0]:
+                tv = f'mats[{int(o["mat"])}].x'
+                if tangent[0][q] == 'rot':
+                    S = (int(o['code']) - 1) // 5
+                    lines.append(f'            {{ const auto t = {tv}; tan_rot<{S}>(a, t); tan_rot<{S}>(b, t); }}')
+                else:
+                    x = (int(o['code']) & 0x7FFF) - 83
+                    SA = x // 5 - 1
+                    fb = '0' if SA >= 0 else f'(int)((tg >> {int(o["ga"])}) & 1ull)'
+                    lines.append(f'            {{ const auto t = {tv}; const int fb = {fb}; '
+                                 f'tan_phase<{SA}>(a, t, fb); tan_phase<{SA}>(b, t, fb); }}')
                 continue
             code = _op_code(o, words, wpe)
             if code:
                 lines.append('            ' + code)
                 lines.append('            ' + code.replace('(a, ', '(b, ').replace('(a);', '(b);'))
+        if last and tangent is not None:
+            lines.append(f'            scale_both(a, b, mats[{tangent[1]}].x);')
         if last:
             lines.append('            S::store_global(a, phi, tg, ctab, L);')
             lines.append('            S::store_global(b, lam, tg, ctab, L);')
@@ -669,17 +702,21 @@ def compile_passes(ops: np.ndarray, passes: np.ndarray, mats_host: np.ndarray, c
 
 
 def compile_adjoint(ops: np.ndarray, passes: np.ndarray, mats_host: np.ndarray, complex64: bool, device: int,
-                    workers: int = 0) -> list:
-    """One specialised adjoint backward kernel per pass (None for an empty pass)."""
+                    workers: int = 0, tangents=None) -> list:
+    """One specialised adjoint backward kernel per pass (None for an empty pass).
+    tangents: per pass None (the general form) or (records in tangent form,
+    pool offset of the pass-end factor) for the tangent variant."""
     words = np.ascontiguousarray(mats_host).view(np.uint32)
     wpe = mats_host.dtype.itemsize // 4
     code = N.DESV_C64 if complex64 else N.DESV_C128
     jobs = []
-    for p in passes:
+    for i, p in enumerate(passes):
         K = int(p['tile_bits'])
         nb = adjoint_nbuf_for(K, complex64)
         b, e = int(p['op_begin']), int(p['op_end'])
-        jobs.append((adjoint_source(ops, b, e, K, nb, complex64, words, wpe), K, nb) if 0 < e - b <= MAX_OPS else None)
+        tg = tangents[i] if tangents is not None else None
+        jobs.append((adjoint_source(ops, b, e, K, nb, complex64, words, wpe, tangent=tg), K, nb)
+                    if 0 < e - b <= MAX_OPS else None)
     return _compile(jobs, code, device, KIND_ADJOINT, workers)
 
 

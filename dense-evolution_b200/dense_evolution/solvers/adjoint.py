@@ -103,6 +103,102 @@ def _classify_backward(op: BOp):
     op.nd, op.d = nd, d
 
 
+class TangentPlan:
+    """The tangent variant of a program's backward passes (complex64,
+    specialised kernels).  Uncontrolled ry inverses on register slots become
+    x0 -= t x1, x1 += t x0 and uncontrolled rz inverses x += i t x / x -= i t x
+    (jit_pass.cuh: tan_rot, tan_phase): half the FP32 work of the general
+    forms, each 1/c times the exact gate.  Per call and pass the host forms
+    t = s / c and the running product S of the 1/c; a gradient probe is
+    multiplied by 1/S^2 (both arrays carry S), and the pass ends by scaling
+    both arrays by 1/S.  A pass whose |t| or S leaves [0, TMAX] runs in the
+    general form (its matrices untouched) -- the tangent blows up near
+    theta = pi."""
+
+    TMAX = 2.0 ** 20
+
+    def __init__(self, back: fusion.Packed, pool_len: int, generic_pool: np.ndarray):
+        words = np.ascontiguousarray(generic_pool).view(np.uint32)
+        wpe = generic_pool.dtype.itemsize // 4
+        name_of = {rec: back.fops[fi].src[0].name for rec, fi in back.op_slots}
+        kind_of = {rec: back.fops[fi].kind for rec, fi in back.op_slots}
+        ops = back.ops
+        self.end_base = pool_len
+        self.passes = []      # per pass: (records in tangent form {rec: 'rot' | 'phase'}, events)
+        for ps in back.passes:
+            tan, events = {}, []
+            if int(ps['op_end']) - int(ps['op_begin']) > jit.MAX_OPS:
+                self.passes.append((tan, events))     # no specialised kernel: the interpreter runs it
+                continue
+            for q in range(int(ps['op_begin']), int(ps['op_end'])):
+                o = ops[q]
+                k = int(o['kind'])
+                if k == N.OP_STAGE:
+                    continue
+                off = int(o['mat'])
+                if k == N.OP_GRAD:
+                    events.append(('g', off, jit.grad_reads_pool(o, words, wpe)))
+                    continue
+                code = int(o['code'])
+                if code & 0x8000 or kind_of.get(q) != 'm1':
+                    continue
+                nm = name_of.get(q)
+                if nm == 'ry' and 1 <= code <= 20 and (code - 1) % 5 == 1 and int(o['cslot']) < 0:
+                    tan[q] = 'rot'
+                elif nm == 'rz' and 83 <= code <= 107 and (code - 83) % 5 == 0 and int(o['gb']) == 0xFF:
+                    tan[q] = 'phase'
+                else:
+                    continue
+                events.append(('t', off, tan[q]))
+            self.passes.append((tan, events))
+
+    def sources_info(self) -> list:
+        """Per pass the tangent argument of jit.adjoint_source (None: no record
+        in tangent form, the general kernel serves it)."""
+        return [(tan, self.end_base + i) if tan else None for i, (tan, _) in enumerate(self.passes)]
+
+    def transform(self, mats: np.ndarray):
+        """(pool extended by one pass-end factor per pass, with every pass that
+        can run in tangent form rewritten for it; per-pass flags)."""
+        out = np.concatenate([mats, np.ones(len(self.passes), mats.dtype)])
+        flags = []
+        for i, (tan, events) in enumerate(self.passes):
+            if not tan:
+                flags.append(False)
+                continue
+            S, ok, writes = 1.0, True, []
+            for kind, off, extra in events:
+                if kind == 't':
+                    if extra == 'rot':
+                        c = float(mats[off].real)
+                        t = float(mats[off + 2].real) / c if c != 0.0 else np.inf
+                    else:
+                        c = float(mats[off].real)
+                        t = float(mats[off].imag) / c if c != 0.0 else np.inf
+                    if not abs(t) <= self.TMAX:
+                        ok = False
+                        break
+                    S /= c
+                    if not abs(S) <= self.TMAX:
+                        ok = False
+                        break
+                    writes.append((off, t, None))
+                else:
+                    writes.append((off, 1.0 / (S * S), extra))
+            flags.append(ok)
+            if not ok:
+                continue
+            for off, v, reads_pool in writes:
+                if reads_pool is None:
+                    out[off] = v                       # the tangent t
+                elif reads_pool:
+                    out[off:off + 4] = mats[off:off + 4] * v   # generator read at run time: pre-scaled
+                else:
+                    out[off] = v                       # immediate-form probe: its correction
+            out[self.end_base + i] = 1.0 / S
+        return out, flags
+
+
 def _adjoint_tile_bits(n: int, dtype) -> int:
     return min(11 if dtype == torch.complex64 else 10, n)
 
@@ -131,6 +227,10 @@ class AdjointProgram:
         self._map_dev = None
         self._stage: dict = {}
         self._scratch = None
+        self._tangent = None          # TangentPlan, built with the first specialised gradient
+        import os
+        self._use_tangent = (self.back is not None and dtype == torch.complex64 and jit.enabled(self.n)
+                             and os.environ.get('DESV_ADJ_TANGENT', '1') != '0')
 
     # ------------------------------------------------------------ helpers
     def _device(self):
@@ -254,15 +354,23 @@ class AdjointProgram:
         cdt = np.complex64 if self.dtype == torch.complex64 else np.complex128
         mats = self.back.materialize(theta, cdt)
         ops_t = self._staged('ops', self.back.ops, dev)
-        mats_t = self._staged('mats', mats, dev)
+        flags = None
+        up = mats
+        if self._use_tangent:
+            if self._tangent is None:
+                self._tangent = TangentPlan(self.back, len(mats),
+                                            self.back.materialize(0.37 + 0.0137 * np.arange(max(self.nparams, 1)),
+                                                                  cdt))
+            up, flags = self._tangent.transform(mats)
+        mats_t = self._staged('mats', up, dev)
         if self._map_dev is None or self._map_dev.device != dev:
             self._map_dev = torch.tensor(self.back.param_map or [0], dtype=torch.int32, device=dev)
-        self._back_dev = (key, ops_t, mats_t, self._map_dev, mats)
+        self._back_dev = (key, ops_t, mats_t, self._map_dev, mats, flags)
         return self._back_dev
 
     def _gradient_fused(self, theta, mu, lam, grad):
         dev = mu.device
-        _, ops_t, mats_t, map_t, mats = self._upload_backward(theta, dev)
+        _, ops_t, mats_t, map_t, mats, flags = self._upload_backward(theta, dev)
         need = int(N.lib().desv_adjoint_scratch_bytes(max(self.back.max_params, 1)))
         if self._scratch is None or self._scratch.numel() * 8 < need:
             self._scratch = torch.empty((need + 7) // 8, dtype=torch.float64, device=dev)
@@ -276,11 +384,24 @@ class AdjointProgram:
             # change with the angles: reuse them while those stay the same
             import hashlib
             okey = (hashlib.sha1(self.back.ops.tobytes()).hexdigest(), jit.value_key(self.back.ops, mats), dev.index)
+            dix = dev.index if dev.index is not None else torch.cuda.current_device()
             if getattr(self, '_adj_kernels', None) is None or self._adj_kernels[0] != okey:
-                kernels = jit.compile_adjoint(self.back.ops, p, mats, self.dtype == torch.complex64,
-                                              dev.index if dev.index is not None else torch.cuda.current_device())
-                self._adj_kernels = (okey, kernels)
-            kernels = self._adj_kernels[1]
+                kt = None
+                if flags is not None:
+                    info = self._tangent.sources_info()
+                    kt = jit.compile_adjoint(self.back.ops, p, mats, True, dix, tangents=info)
+                    kt = [k if inf is not None else None for k, inf in zip(kt, info)]
+                # the general kernels of every pass as well: a pass whose angles
+                # leave the tangent range (near theta = pi) runs in the general form,
+                # and which passes do changes with every theta
+                kg = jit.compile_adjoint(self.back.ops, p, mats, self.dtype == torch.complex64, dix)
+                self._adj_kernels = (okey, kg, kt)
+            _, kg, kt = self._adj_kernels
+            kernels = list(kg)
+            if kt is not None:
+                for i, (use, k) in enumerate(zip(flags, kt)):
+                    if use and k is not None:
+                        kernels[i] = k
             jit.run_adjoint(kernels, mu.data_ptr(), lam.data_ptr(), self.n, N.dtype_code(mu), p, ops_t.data_ptr(),
                             mats_t.data_ptr(), map_t.data_ptr(), grad.data_ptr(), self._scratch.data_ptr(),
                             self._scratch.numel() * 8, N.stream_ptr())

@@ -93,3 +93,60 @@ def test_rows_plan_energy_and_gradient(n, dtype_name):
         assert float(np.real(np.vdot(psi, lam))) == pytest.approx(e_ref, abs=1e-12)
         fd = O.fd_gradient(theta, orows, n, terms, h=1e-5, indices=[0, npar // 2, npar - 1])
         assert np.allclose(grad[[0, npar // 2, npar - 1]], fd, atol=1e-7)
+
+
+def test_adjoint_tangent_plan_bookkeeping():
+    """The tangent variant's host bookkeeping (tangents, running 1/c products,
+    probe corrections, pass-end factors) gives the exact gradient when every
+    tangent record is read as (1/c) times its gate -- the kernel's arithmetic in
+    exact form -- every probe is scaled by its correction and every pass ends by
+    scaling both arrays by its end factor."""
+    import os
+    import torch
+    from dense_evolution.solvers.adjoint import AdjointProgram, TangentPlan
+    from dense_evolution.solvers.autodiff import build_template
+    from dense_evolution.workloads import hea_circuit, tfim_terms
+    os.environ['DESV_JIT'] = '1'
+    try:
+        n = 11
+        circ = hea_circuit(n, 3)
+        rows, slots, npar = build_template(circ, n)
+        prog = AdjointProgram(rows, slots, n, torch.complex64)
+    finally:
+        del os.environ['DESV_JIT']
+    theta = np.random.default_rng(5).uniform(-np.pi, np.pi, npar)
+    mats = prog.back.materialize(theta, np.complex128)
+    tp = TangentPlan(prog.back, len(mats), prog.back.materialize(0.37 + 0.0137 * np.arange(npar), np.complex128))
+    out, flags = tp.transform(mats)
+    assert any(flags) and sum(len(t) for t, _ in tp.passes) > npar // 2
+    # exact-arithmetic reading of the tangent pool: a tangent record is (1/c) U
+    emu = out[:len(mats)].copy()
+    for i, (tan, events) in enumerate(tp.passes):
+        if not flags[i]:
+            continue
+        for kind, off, extra in events:
+            if kind == 't':
+                t = out[off].real
+                if extra == 'rot':
+                    emu[off:off + 4] = [1.0, -t, t, 1.0]        # [[1, -t], [t, 1]] = [[c, s], [-s, c]] / c
+                else:
+                    emu[off:off + 4] = [1 + 1j * t, 1 - 1j * t, 1 + 1j * t, 1 - 1j * t]
+            elif not extra:
+                emu[off:off + 4] = mats[off:off + 4] * out[off].real    # immediate probe: its correction
+    terms = tfim_terms(n)
+    orows, _ = O.energy_template([{'name': c[0], 'qubits': [q for q in c[1:] if isinstance(q, int)]}
+                                  for c in circ], n)
+    _, psi = O.energy(theta, orows, n, terms)
+    lam = O.pauli_sum_matvec(psi, terms)
+    mu = psi.copy()
+    grad = np.zeros(npar)
+    for i, ps in enumerate(prog.back.passes):
+        one = prog.back.passes[i:i + 1]
+        mu, lam, grad = run_passes(mu, n, one, prog.back.ops, emu if flags[i] else mats, lam=lam, grad=grad,
+                                   param_map=np.asarray(prog.back.param_map))
+        if flags[i]:
+            f = out[tp.end_base + i].real
+            mu, lam = mu * f, lam * f
+    fd = O.fd_gradient(theta, orows, n, terms, h=1e-5, indices=list(range(0, npar, 7)))
+    assert np.allclose(grad[list(range(0, npar, 7))], fd, atol=1e-7)
+    assert np.max(np.abs(mu - O.zero_state(n))) < 1e-10

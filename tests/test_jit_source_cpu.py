@@ -69,3 +69,43 @@ def test_sources_compile_with_nvrtc():
     if r == N.DESV_EUNSUPPORTED:
         pytest.skip('NVRTC not available: ' + N.last_error())
     assert r == 0, log.value.decode()[-3000:]
+
+
+def test_tangent_variant_sources():
+    """The tangent variant of the backward passes: uncontrolled ry / rz inverses
+    on register slots or thread-fixed bits become tan_rot / tan_phase on both
+    arrays, every immediate-form probe is scaled by its pool slot, the last stage
+    scales both arrays by the pass-end factor, and the sources compile."""
+    import os
+    from dense_evolution.solvers.adjoint import TangentPlan
+    os.environ['DESV_JIT'] = '1'
+    try:
+        prog, mats, theta, _ = _sources()
+    finally:
+        del os.environ['DESV_JIT']
+    tp = TangentPlan(prog.back, len(mats), mats)
+    info = tp.sources_info()
+    words = np.ascontiguousarray(mats).view(np.uint32)
+    srcs = []
+    for p, inf in zip(prog.back.passes, info):
+        b, e = int(p['op_begin']), int(p['op_end'])
+        if inf is None or not 0 < e - b <= jit.MAX_OPS:
+            continue
+        K = int(p['tile_bits'])
+        srcs.append(jit.adjoint_source(prog.back.ops, b, e, K, jit.adjoint_nbuf_for(K, True), True, words, 2,
+                                       tangent=inf))
+    assert srcs
+    text = '\n'.join(srcs)
+    assert 'tan_rot<' in text and 'tan_phase<' in text and 'scale_both(a, b, mats[' in text
+    assert '(a, t); tan_rot' in text or 'tan_rot<' in text
+    assert all(src.count('scale_both(') == 1 for src in srcs)
+    for ln in text.splitlines():
+        if 'tan_rot<' in ln or 'tan_phase<' in ln:
+            assert '(a, t' in ln and '(b, t' in ln
+        if 'jit_grad_y<' in ln or 'jit_grad_dim<' in ln:
+            assert 'v *= (double)mats[' in ln
+    log = ctypes.create_string_buffer(16384)
+    r = N.lib().desv_jit_compile_check(srcs[0].encode(), jit.INCLUDE_PATH.encode(), log, 16384)
+    if r == N.DESV_EUNSUPPORTED:
+        pytest.skip('NVRTC not available: ' + N.last_error())
+    assert r == 0, log.value.decode()[-3000:]
