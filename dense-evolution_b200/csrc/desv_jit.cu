@@ -40,6 +40,7 @@ struct JitApi {
     CUresult_t (*ModuleGetFunction)(CUfunction_t *, CUmodule_t, const char *);
     CUresult_t (*ModuleGetGlobal)(CUdeviceptr_t *, size_t *, CUmodule_t, const char *);
     CUresult_t (*FuncSetAttribute)(CUfunction_t, int, int);
+    CUresult_t (*FuncGetAttribute)(int *, int, CUfunction_t);
     CUresult_t (*OccupancyMaxActiveBlocksPerMultiprocessor)(int *, CUfunction_t, int, size_t);
     CUresult_t (*LaunchKernel)(CUfunction_t, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                                void *, void **, void **);
@@ -83,6 +84,7 @@ static const JitApi &api() {
                sym(drv, "cuModuleGetFunction", g_api.ModuleGetFunction, w) &&
                sym(drv, "cuModuleGetGlobal_v2", g_api.ModuleGetGlobal, w) &&
                sym(drv, "cuFuncSetAttribute", g_api.FuncSetAttribute, w) &&
+               sym(drv, "cuFuncGetAttribute", g_api.FuncGetAttribute, w) &&
                sym(drv, "cuOccupancyMaxActiveBlocksPerMultiprocessor",
                    g_api.OccupancyMaxActiveBlocksPerMultiprocessor, w) &&
                sym(drv, "cuLaunchKernel", g_api.LaunchKernel, w);
@@ -102,7 +104,7 @@ struct JitKernel {
 
 // kind of a rotation-pass kernel (desv_rot_load)
 constexpr int JIT_KIND_ROT = 5;
-constexpr int ROT_REG_BITS = 5;     // register slots per stage (rot_pass.cuh: 32 amplitudes per thread)
+constexpr int ROT_REG_BITS = 5;     // fewest register slots per stage (rot_pass.cuh: 32 amplitudes per thread)
 constexpr int ROT_MAX_PARAM_FLOATS = 7936;  // by-value parameter block <= 31 KiB (limit 32764 bytes)
 
 // padded stage layout of a 2^K tile: one spare amplitude after every 16
@@ -440,7 +442,7 @@ extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile
     k->K = tile_bits;
     k->nbuf = nbuf;
     k->dtype = DESV_C64;
-    k->threads = 1 << (tile_bits - ROT_REG_BITS);
+    k->threads = 0;   // from the kernel's launch bounds once it is loaded (2^(K - register slots))
     k->param_floats = param_floats;
     k->smem = PIPE_HDR_BYTES + (size_t)nbuf * rot_slot_elems(tile_bits) * sizeof(float2);
     size_t ssz = 0;
@@ -459,6 +461,16 @@ extern "C" int desv_rot_load(const char *src, const char *include_dirs, int tile
         delete k;
         return fail(DESV_ECUDA, "rotation pass load: shared-memory attribute refused");
     }
+    // the generated kernel declares its block size (2^(K - register slots per
+    // stage)) in its launch bounds: CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK
+    int maxt = 0;
+    if (a.FuncGetAttribute(&maxt, 0, k->fn) != 0 || maxt < 32 || maxt > (1 << (tile_bits - ROT_REG_BITS)) ||
+        (maxt & (maxt - 1))) {
+        a.ModuleUnload(k->mod);
+        delete k;
+        return fail(DESV_EINVAL, "rotation pass load: the kernel's launch bounds are not a block of 2^(K - slots)");
+    }
+    k->threads = maxt;
     int b = 0;
     a.OccupancyMaxActiveBlocksPerMultiprocessor(&b, k->fn, k->threads, k->smem);
     k->blocks_per_sm = b > 0 ? b : 1;

@@ -13,7 +13,7 @@
 
 namespace desv {
 
-constexpr int ROT_NA = 32;   // amplitudes per thread (5 register slots)
+constexpr int ROT_NA = 32;   // amplitudes per thread with 5 register slots (the default; 6 slots: 64)
 
 // (re, im) * (cr + i ci)
 __device__ __forceinline__ float2 cmulc(float2 a, float cr, float ci) {
@@ -25,12 +25,12 @@ __device__ __forceinline__ float2 cmulc(float2 a, float cr, float ci) {
 // then 1/c too large, which the pass-end factor corrects), form 1 the general
 // form.  The values are kernel parameters (uniform across the grid), so the
 // branch never diverges.
-template <int S>
-__device__ __forceinline__ void rot(float2 (&a)[ROT_NA], float t, float c, float s, float form) {
+template <int S, int NA>
+__device__ __forceinline__ void rot(float2 (&a)[NA], float t, float c, float s, float form) {
     if (form == 0.f) {
         const float2 pt = make_float2(t, t), nt = make_float2(-t, -t);
 #pragma unroll
-        for (int j = 0; j < ROT_NA; ++j) {
+        for (int j = 0; j < NA; ++j) {
             if (j & (1 << S)) continue;
             const float2 x0 = a[j], x1 = a[j | (1 << S)];
             a[j] = __ffma2_rn(nt, x1, x0);
@@ -39,7 +39,7 @@ __device__ __forceinline__ void rot(float2 (&a)[ROT_NA], float t, float c, float
     } else {
         const float2 pc = make_float2(c, c), ps = make_float2(s, s), ns = make_float2(-s, -s);
 #pragma unroll
-        for (int j = 0; j < ROT_NA; ++j) {
+        for (int j = 0; j < NA; ++j) {
             if (j & (1 << S)) continue;
             const float2 x0 = a[j], x1 = a[j | (1 << S)];
             a[j] = __ffma2_rn(ns, x1, __fmul2_rn(pc, x0));
@@ -51,11 +51,11 @@ __device__ __forceinline__ void rot(float2 (&a)[ROT_NA], float t, float c, float
 // The tangent form alone: the pass variant run when every rotation of the
 // call takes the tangent form (the usual case), without the general form's
 // code, which doubles the size of a pass.
-template <int S>
-__device__ __forceinline__ void rot_t(float2 (&a)[ROT_NA], float t) {
+template <int S, int NA>
+__device__ __forceinline__ void rot_t(float2 (&a)[NA], float t) {
     const float2 pt = make_float2(t, t), nt = make_float2(-t, -t);
 #pragma unroll
-    for (int j = 0; j < ROT_NA; ++j) {
+    for (int j = 0; j < NA; ++j) {
         if (j & (1 << S)) continue;
         const float2 x0 = a[j], x1 = a[j | (1 << S)];
         a[j] = __ffma2_rn(nt, x1, x0);
@@ -93,16 +93,16 @@ __device__ __forceinline__ void rot_t(float2 (&a)[ROT_NA], float t) {
 #endif
 
 // every amplitude times the real f
-__device__ __forceinline__ void scale_all(float2 (&a)[ROT_NA], float f) {
+template <int NA> __device__ __forceinline__ void scale_all(float2 (&a)[NA], float f) {
     const float2 ff = make_float2(f, f);
 #pragma unroll
-    for (int j = 0; j < ROT_NA; ++j) a[j] = __fmul2_rn(ff, a[j]);
+    for (int j = 0; j < NA; ++j) a[j] = __fmul2_rn(ff, a[j]);
 }
 
 // every amplitude times the complex (fr + i fi)
-__device__ __forceinline__ void scale_all_c(float2 (&a)[ROT_NA], float fr, float fi) {
+template <int NA> __device__ __forceinline__ void scale_all_c(float2 (&a)[NA], float fr, float fi) {
 #pragma unroll
-    for (int j = 0; j < ROT_NA; ++j) a[j] = cmulc(a[j], fr, fi);
+    for (int j = 0; j < NA; ++j) a[j] = cmulc(a[j], fr, fi);
 }
 
 // negate the amplitude when bit 31 of w is set (sign-bit flips of re and im)
@@ -126,7 +126,7 @@ template <int K, int NBUF, uint32_t SLOT> struct RotRing {
     uint64_t *full;
     float2 *bufs;
     uint32_t tid, nthr, lane, ntile, nchunks, chunk_bytes, warp_bytes, cnt;
-    uint64_t my_off, rmask, tstride, lbase, cbase;
+    uint64_t my_off, my_off2, rmask, tstride, lbase, cbase;
     const float2 *src;
 
     __device__ __forceinline__ void init(const TileGeom &geom, const float2 *sv, unsigned char *smem) {
@@ -147,6 +147,8 @@ template <int K, int NBUF, uint32_t SLOT> struct RotRing {
             fence_mbar_init();
         }
         my_off = tid < nchunks ? chunk_offset(geom, tid) : 0ull;
+        // with 6 register slots a tile has up to twice as many runs as threads
+        my_off2 = tid + nthr < nchunks ? chunk_offset(geom, tid + nthr) : 0ull;
         rmask = 0;
         for (int r = 0; r < geom.nrest; ++r) rmask |= 1ull << geom.rest[r];
         tstride = tile_base(geom, gridDim.x);
@@ -162,10 +164,14 @@ template <int K, int NBUF, uint32_t SLOT> struct RotRing {
         lbase = next(lbase);
         if (lane == 0) mbar_arrive_expect_tx(&full[sl], warp_bytes);
         __syncwarp();
-        // one run per thread: nchunks = 2^(K-L) <= 2^(K-5) = threads (L >= 5)
-        if (tid < nchunks) {
-            float2 *dst = slot(i) + (size_t)tid * (chunk_bytes / sizeof(float2));
-            const float2 *from = src + base + my_off;
+        // runs c = tid and tid + threads: nchunks = 2^(K-L) <= 2^(K-5) and threads =
+        // 2^(K - register slots), so at most two runs per thread for up to 6 slots
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const uint32_t c = tid + (uint32_t)r * nthr;
+            if (c >= nchunks) break;
+            float2 *dst = slot(i) + (size_t)c * (chunk_bytes / sizeof(float2));
+            const float2 *from = src + base + (r ? my_off2 : my_off);
 #ifdef DESV_ROT_CHECK
             if ((reinterpret_cast<uint64_t>(from) & 15u) || (smem_addr(dst) & 15u) || (chunk_bytes & 15u)) {
                 atomicOr(&g_dev_status, DESV_DEV_BADPLAN);  // the tile's bounded wait then gives up

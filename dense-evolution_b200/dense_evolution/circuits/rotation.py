@@ -67,7 +67,11 @@ import numpy as np
 from . import fusion
 from .gates import GATES
 
-RB = 5                 # register bits per stage (32 amplitudes per thread)
+# register bits per stage: 5 (32 amplitudes per thread, 128 threads per 4096-amplitude tile) or 6
+# (64 amplitudes, 64 threads); DESV_ROT_RB overrides the default (tuning)
+RB = int(os.environ.get('DESV_ROT_RB', '5'))
+if RB not in (5, 6):
+    raise ValueError('DESV_ROT_RB must be 5 or 6')
 LOW_FIXED = 5          # index bits 0..LOW_FIXED-1 are in every tile (contiguous bulk-copy runs)
 TMAX = 2.0 ** 20       # tangent form while |tan| <= TMAX (FP32 keeps its relative accuracy; see materialize)
 SCALE_LIMIT = 2.0 ** 60  # pending tangent scale above which rotations switch to the general form
@@ -77,7 +81,9 @@ PAD_SHIFT = 4          # padded stage layout: physical = i + (i >> 4)
 # per SM, 207 ms (the next tile loads while the last stage computes and stores); 2 -> three CTAs,
 # 233 ms; 3 -> two CTAs, 274 ms
 NBUF = 1
-CTAS_PER_SM = {1: 4, 2: 3, 3: 2}   # register bound of the kernel per ring depth (shared memory allows as many)
+# register bound of the kernel per ring depth (shared memory allows as many); with 6 register
+# slots a CTA is half as wide and holds twice the amplitudes per thread
+CTAS_PER_SM = {1: 4, 2: 3, 3: 2} if RB == 5 else {1: 5, 2: 4, 3: 3}
 
 
 def tuning() -> Tuple[int, int]:
