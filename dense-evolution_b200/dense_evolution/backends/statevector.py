@@ -34,6 +34,50 @@ def _freeze(circuit) -> tuple:
     return tuple(out)
 
 
+_SLOT_1Q = frozenset(('rx', 'ry', 'rz', 'p', 'u1', 'phase', 'gphase'))
+_SLOT_2Q = frozenset(('cp', 'cphase', 'crz'))
+
+
+def _structure(circuit):
+    """(structure key, slots, angles) of a transpiled gate list: the angle of
+    every one-angle gate (rx/ry/rz/p/u1/phase/gphase with one qubit, cp/cphase/
+    crz with two) becomes a parameter slot, so circuits that differ only in
+    those angles share a key; every other gate enters the key whole."""
+    key, slots, angles = [], [], []
+    for cmd in circuit:
+        name = cmd[0].lower() if isinstance(cmd[0], str) else str(cmd[0]).lower()
+        if name in _SLOT_1Q and len(cmd) == 3:
+            key.append((name, int(cmd[1])))
+        elif name in _SLOT_2Q and len(cmd) == 4:
+            key.append((name, int(cmd[1]), int(cmd[2])))
+        else:
+            key.append(tuple(float(x) if isinstance(x, np.floating) else
+                             (int(x) if isinstance(x, np.integer) else x) for x in cmd))
+            slots.append(-1)
+            continue
+        slots.append(len(angles))
+        angles.append(float(cmd[-1]))
+    return tuple(key), slots, np.asarray(angles, dtype=np.float64)
+
+
+class BoundCircuit:
+    """A compiled circuit structure together with one call's angles: run(sv)
+    applies it; every other attribute is the CompiledCircuit's."""
+    __slots__ = ('plan', 'theta')
+
+    def __init__(self, plan: CompiledCircuit, theta):
+        self.plan, self.theta = plan, theta
+
+    def run(self, sv, stream=None):
+        return self.plan.run(sv, theta=self.theta, stream=stream)
+
+    def device_arrays(self, device):
+        return self.plan.device_arrays(device, self.theta)
+
+    def __getattr__(self, name):
+        return getattr(self.plan, name)
+
+
 def _unknown_jit(name):
     return ValueError(
         f"unknown gate '{name}' -- not in GATE_IDS. A typo in a gate name used to be silently dropped "
@@ -224,18 +268,23 @@ class DenseSVSimulator:
         return np.array([total - 2.0 * marg[self._bit(q)] for q in range(self.n)])
 
     # ------------------------------------------------------------------ circuits
-    def compile(self, circuit, transpile: bool = True) -> CompiledCircuit:
+    def compile(self, circuit, transpile: bool = True) -> BoundCircuit:
+        """The circuit's compiled structure with its angles.  Plans are cached by
+        structure (gate names, qubits and the fixed parameters), so a circuit
+        run again with new angles -- a variational loop -- reuses its lowering,
+        fusion plan and kernels and only recomputes the per-call values."""
         target = QuantumTranspiler.transpile(circuit) if transpile else list(circuit)
-        key = (_freeze(target), self.n, self.use_float32)
+        skey, slots, angles = _structure(target)
+        key = (skey, self.n, self.use_float32)
         plan = self._plans.get(key)
         if plan is None:
-            plan = CompiledCircuit(target, self.n, self.tdtype)
+            plan = CompiledCircuit(target, self.n, self.tdtype, slots=slots if len(angles) else None)
             self._plans[key] = plan
             if len(self._plans) > self._PLAN_CACHE_SIZE:
                 self._plans.popitem(last=False)
         else:
             self._plans.move_to_end(key)
-        return plan
+        return BoundCircuit(plan, angles if len(angles) else None)
 
     def run_circuit(self, circuit: List[Tuple], transpile: bool = True):
         """Transpile, fuse and run `circuit` in place (statevector.py:362-410).

@@ -196,3 +196,21 @@ def test_fidelity_and_counts(de):
     assert set(c) <= {'00', '11'} and sum(c.values()) == 1000
     with pytest.raises(ValueError):
         de.statevector_fidelity(sv, np.ones(8))
+
+
+@pytest.mark.parametrize('n,f32', [(10, False), (20, True)])
+def test_run_circuit_reuses_the_structure_with_new_angles(de, n, f32):
+    """Circuits that differ only in their angles share one compiled plan (the
+    angles become parameter slots); each call's state still matches the oracle
+    (general fused passes at 10 qubits complex128, rotation passes at 20
+    qubits complex64)."""
+    from dense_evolution.workloads import brick_u3_circuit
+    sim = de.DenseSVSimulator(n, use_float32=f32)
+    for seed in (1, 2, 3):
+        circ = brick_u3_circuit(n, 3, seed=seed)
+        sim.set_initial_state(None)
+        sim.run_circuit(circ)
+        ref = O.run_circuit(O.zero_state(n), n, circ)
+        err = float(np.max(np.abs(sim.get_statevector().astype(np.complex128) - ref)))
+        assert err < (1e-5 if f32 else 1e-12), err
+    assert len(sim._plans) == 1
