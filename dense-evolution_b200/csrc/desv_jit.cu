@@ -162,6 +162,29 @@ int jit_pauli_launch(void *handle, const void *psi, void *out, int dtype, int mo
     return DESV_OK;
 }
 
+// The same for a rows launch (a kernel compiled with per-row coefficient
+// symbols): one grid row per state, CTAs per row by the rows grid rule (at
+// most 64), the row's coefficients at csym + row * nsym.
+int jit_pauli_rows_launch(void *handle, const void *psi, void *out, int dtype, int mode, const TileGeom &g,
+                          int want_e, double *part, int *grid_out, int rows, const RowStrides &rs,
+                          const double *csym, int nsym, cudaStream_t st) {
+    auto *k = static_cast<JitKernel *>(handle);
+    if (k->kind != 2 + mode) return fail(DESV_EINVAL, "jit rows Pauli pass: the kernel was compiled for another mode");
+    if (dtype != k->dtype || g.K != k->K || g.K - g.L > 8)
+        return fail(DESV_EINVAL, "jit rows Pauli pass: dtype or tile geometry differs from the compiled kernel");
+    const uint64_t ntiles = 1ull << (g.n - k->K);
+    const uint64_t cap = (uint64_t)sm_count() * k->blocks_per_sm;
+    int gx = rows_grid_x(ntiles, cap, rows);
+    if (gx > 64) gx = 64;
+    *grid_out = gx;
+    TileGeom gg = g;
+    RowStrides r2 = rs;
+    void *args[] = {const_cast<void **>(&psi), &out, &gg, &want_e, &part, const_cast<double **>(&csym), &nsym, &r2};
+    if (api().LaunchKernel(k->fn, (unsigned)gx, (unsigned)rows, 1, 256, 1, 1, (unsigned)k->smem, st, args, nullptr) !=
+        0)
+        return fail(DESV_ECUDA, "jit rows Pauli pass: launch failed");
+    return DESV_OK;
+}
 
 // Compile CUDA source for sm_100a with NVRTC; the log (if any) goes to log.
 static int nvrtc_compile(const char *src, const char *include_dir, std::vector<char> &cubin, char *log,

@@ -26,6 +26,8 @@ int rows_prepare(int, const desv_batch_recipe *, int, const double *, int64_t, c
                  int, int, cudaStream_t);
 int rows_norm(const void *, int, int, int, double *, double *, cudaStream_t);
 int rows_sum(const double *, int64_t, int, int, double *, int, cudaStream_t);
+int jit_pauli_rows_launch(void *, const void *, void *, int, int, const TileGeom &, int, double *, int *, int,
+                          const RowStrides &, const double *, int, cudaStream_t);
 
 // partial-sum slots per state and pass (the rows grid bound of every kernel)
 constexpr int ROWS_SLOTS = 64;
@@ -92,9 +94,11 @@ int desv_apply_passes_rows(void *states, int n, int dtype, int rows, const desv_
     return DESV_OK;
 }
 
-int desv_pauli_matvec_rows(const void *psi, void *out, int n, int dtype, int rows, const desv_pauli_pass *passes,
-                           int npasses, const desv_pauli_term *terms, int64_t term_stride, double *expect,
-                           double *norm, void *scratch, size_t sb, void *stream) {
+// handles: NULL, or per pass a specialised rows kernel (or NULL: the
+// interpreter runs that pass) reading csym (rows x nsym coefficients)
+static int matvec_rows(void *const *handles, const double *csym, int nsym, const void *psi, void *out, int n,
+                       int dtype, int rows, const desv_pauli_pass *passes, int npasses, const desv_pauli_term *terms,
+                       int64_t term_stride, double *expect, double *norm, void *scratch, size_t sb, void *stream) {
     int r = check_rows(psi, n, dtype, rows);
     if (r) return r;
     if ((r = check_rows(out, n, dtype, rows))) return r;
@@ -123,8 +127,12 @@ int desv_pauli_matvec_rows(const void *psi, void *out, int n, int dtype, int row
             TileGeom g;
             if (ps.tile_bits > n || ps.low_bits < (n < 5 ? n : 5) || !make_geom(g, n, ps.tile_bits, ps.low_bits, ps.high))
                 return fail(DESV_EINVAL, "rows Pauli pass " + std::to_string(p) + ": invalid tile geometry");
-            r = pauli_pass_rows(psi, out, dtype, mode, g, terms + ps.term_begin, nt, expect ? 1 : 0, pp, &grid, rows, rs,
-                                S(stream));
+            if (handles && handles[p])
+                r = jit_pauli_rows_launch(handles[p], psi, out, dtype, mode, g, expect ? 1 : 0, pp, &grid, rows, rs,
+                                          csym, nsym, S(stream));
+            else
+                r = pauli_pass_rows(psi, out, dtype, mode, g, terms + ps.term_begin, nt, expect ? 1 : 0, pp, &grid,
+                                    rows, rs, S(stream));
         }
         if (r) return r;
         if (grid > ROWS_SLOTS) return fail(DESV_EINVAL, "rows matvec: grid above the partial-sum slots");
@@ -149,6 +157,23 @@ int desv_pauli_matvec_rows(const void *psi, void *out, int n, int dtype, int row
         if ((r = rows_norm(psi, n, dtype, rows, np, norm, S(stream)))) return r;
     }
     return DESV_OK;
+}
+
+int desv_pauli_matvec_rows(const void *psi, void *out, int n, int dtype, int rows, const desv_pauli_pass *passes,
+                           int npasses, const desv_pauli_term *terms, int64_t term_stride, double *expect,
+                           double *norm, void *scratch, size_t sb, void *stream) {
+    return matvec_rows(nullptr, nullptr, 0, psi, out, n, dtype, rows, passes, npasses, terms, term_stride, expect, norm,
+                       scratch, sb, stream);
+}
+
+int desv_jit_pauli_matvec_rows(void *const *handles, const double *csym, int nsym, const void *psi, void *out, int n,
+                               int dtype, int rows, const desv_pauli_pass *passes, int npasses,
+                               const desv_pauli_term *terms, int64_t term_stride, double *expect, double *norm,
+                               void *scratch, size_t sb, void *stream) {
+    if (!handles) return fail(DESV_EINVAL, "jit rows matvec: null handle array");
+    if (nsym < 0 || (nsym > 0 && !csym)) return fail(DESV_EINVAL, "jit rows matvec: null coefficient table");
+    return matvec_rows(handles, csym, nsym, psi, out, n, dtype, rows, passes, npasses, terms, term_stride, expect, norm,
+                       scratch, sb, stream);
 }
 
 int desv_adjoint_passes_rows(void *phi, void *lam, int n, int dtype, int rows, const desv_adj_pass *passes,

@@ -302,6 +302,31 @@ class _RowsGroup:
         self.term_stride = tr.shape[1]
         self.d_terms = up(tr.reshape(-1))
         self.ppasses = np.ascontiguousarray(plan.pauli.passes)
+        # specialised H psi kernels: a coefficient column equal in every row is
+        # compiled in, the others become per-row symbols (equal columns share one)
+        self.pk = None
+        if plan.use_jit and len(plan.pauli.terms):
+            from .circuits import jit
+            co = np.asarray(coefs, dtype=np.float64)[:, plan.pauli.order]          # (rows, terms)
+            terms = plan.pauli.terms.copy()
+            syms, cols = [], {}
+            for k in range(co.shape[1]):
+                col = co[:, k]
+                if np.all(col == col[0]):
+                    terms['cre'][k] *= col[0]
+                    terms['cim'][k] *= col[0]
+                    syms.append(None)
+                else:
+                    syms.append(cols.setdefault(col.tobytes(), len(cols)))
+            csym = np.zeros((B, max(len(cols), 1)))
+            for key, i in cols.items():
+                csym[:, i] = np.frombuffer(key, dtype=np.float64)
+            ks = jit.compile_pauli_rows(terms, self.ppasses, syms, plan.dtype == torch.complex64,
+                                        dev.index if dev.index is not None else torch.cuda.current_device())
+            if any(k is not None for k in ks):
+                self.pk = (ks, (ctypes.c_void_p * len(ks))(*[k.handle.value if k is not None else None for k in ks]))
+                self.d_csym = torch.from_numpy(csym.reshape(-1)).to(dev)
+                self.nsym = csym.shape[1]
         self.expect = torch.zeros((B, 2), dtype=torch.float64, device=dev)
         self.norm = torch.ones(B, dtype=torch.float64, device=dev)
         sb = int(N.lib().desv_rows_scratch_bytes(B, max(plan.bwd.max_params, 1), max(len(self.ppasses), 1)))
@@ -319,13 +344,15 @@ class _RowsGroup:
         rows_forward(self.kf, self.psi, n, self.code, B, self.fwd_passes, self.d_fwd_ops, self.pools, p.pool_stride,
                      st)
         want_norm = p.dtype == torch.complex64
-        N.check(N.lib().desv_pauli_matvec_rows(vp(self.psi.data_ptr()), vp(self.lam.data_ptr()), n, self.code, B,
-                                               vp(self.ppasses.ctypes.data), len(self.ppasses),
-                                               vp(self.d_terms.data_ptr()), self.term_stride,
-                                               vp(self.expect.data_ptr()),
-                                               vp(self.norm.data_ptr()) if want_norm else None,
-                                               vp(self.scratch.data_ptr()), self.scratch.numel() * 8, st),
-                'rows H psi')
+        args = (vp(self.psi.data_ptr()), vp(self.lam.data_ptr()), n, self.code, B, vp(self.ppasses.ctypes.data),
+                len(self.ppasses), vp(self.d_terms.data_ptr()), self.term_stride, vp(self.expect.data_ptr()),
+                vp(self.norm.data_ptr()) if want_norm else None, vp(self.scratch.data_ptr()),
+                self.scratch.numel() * 8, st)
+        if self.pk is not None:
+            N.check(N.lib().desv_jit_pauli_matvec_rows(self.pk[1], vp(self.d_csym.data_ptr()), self.nsym, *args),
+                    'rows H psi (jit)')
+        else:
+            N.check(N.lib().desv_pauli_matvec_rows(*args), 'rows H psi')
         with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
             grad.zero_()
         lib, sc, nsc = N.lib(), vp(self.scratch.data_ptr()), self.scratch.numel() * 8

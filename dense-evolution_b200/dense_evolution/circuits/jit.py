@@ -20,7 +20,7 @@ import hashlib
 import os
 import threading
 from concurrent.futures import ThreadPoolExecutor
-from typing import List, Optional
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -461,13 +461,20 @@ def _expect_source(terms: np.ndarray, K: int, L: int, high, complex64: bool) -> 
     return '\n'.join(lines)
 
 
-def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: int, complex64: bool) -> str:
+def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: int, complex64: bool,
+                 syms: Optional[Sequence[Optional[int]]] = None) -> str:
     """CUDA source of one specialised Pauli pass (the interpreter k_pauli with
     the pass's terms compiled in): mode 0 <H> only, 1 write H psi, 2 add into
     H psi.  Terms with one flip mask share the partner amplitude; real
     coefficients take the two-FMA form.  (P psi)[i] = psi[i ^ x] c
     (-1)^popcount((i ^ x) & z); the z bits outside the tile give a per-tile
-    parity."""
+    parity.
+
+    syms (H psi modes, rows launches): per term None (its coefficient is
+    compiled in) or the index of a per-row coefficient that multiplies it:
+    the kernel then runs one grid row per state and reads its row's values
+    from csym[blockIdx.y * nsym + ...] (terms with equal per-row values share
+    an index and still fold into one class)."""
     if mode == 0:
         return _expect_source(terms, tile_bits, low_bits, high, complex64)
     T = 'float2' if complex64 else 'double2'
@@ -475,11 +482,34 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
     K, L = tile_bits, low_bits
     high = [int(h) for h in high[:K - L]]
     tile_mask = ((1 << L) - 1) | sum(1 << h for h in high)
-    lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
-             'extern "C" __global__ void __launch_bounds__(256)',
-             f'desv_jit_kernel(const {T} *psi, {T} *out, TileGeom g, int want_e, double *part) {{',
-             '    extern __shared__ __align__(128) unsigned char smem[];',
-             f'    auto body = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L, double &ere, double &eim) {{']
+    rows = syms is not None
+    if not rows:
+        syms = [None] * len(terms)
+    nsym = 1 + max([x for x in syms if x is not None], default=-1)
+
+    def cx(v: float, sym) -> str:
+        """the coefficient v (times the row's value of symbol sym) as an expression"""
+        return repr(v) if sym is None else f'({v!r} * C{sym})'
+
+    if rows:
+        lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
+                 'extern "C" __global__ void __launch_bounds__(256)',
+                 f'desv_jit_kernel(const {T} *psi, {T} *out, TileGeom g, int want_e, double *part, '
+                 'const double *__restrict__ csym, int nsym, RowStrides rs) {',
+                 '    extern __shared__ __align__(128) unsigned char smem[];',
+                 '    // rows: this grid row\'s state, output, partial sums and coefficients',
+                 '    psi += blockIdx.y * rs.amps;',
+                 '    out += blockIdx.y * rs.amps;',
+                 '    part += blockIdx.y * rs.part;',
+                 '    csym += (size_t)blockIdx.y * nsym;']
+        lines += [f'    const double C{k} = csym[{k}];' for k in range(nsym)]
+        lines.append(f'    auto body = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L, double &ere, double &eim) {{')
+    else:
+        lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
+                 'extern "C" __global__ void __launch_bounds__(256)',
+                 f'desv_jit_kernel(const {T} *psi, {T} *out, TileGeom g, int want_e, double *part) {{',
+                 '    extern __shared__ __align__(128) unsigned char smem[];',
+                 f'    auto body = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L, double &ere, double &eim) {{']
     groups = {}
     for k, t in enumerate(terms):
         groups.setdefault(int(t['xmask']), []).append(k)
@@ -502,27 +532,28 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
             zl = _tile_local(int(t['zmask']) & tile_mask, L, high)
             zo = int(t['zmask']) & ~tile_mask
             cre, cim = float(t['cre']), float(t['cim'])
+            sy = syms[k]
             if cim != 0.0:
-                cplx.append((k, zl, zo, cre, cim))
+                cplx.append((k, zl, zo, cre, cim, sy))
             elif zl == 0:
-                outside.append((k, zo, cre))
+                outside.append((k, zo, cre, sy))
             elif zo == 0 and bin(zl).count('1') <= 2:
                 lo = (zl & -zl).bit_length() - 1
                 d = zl.bit_length() - 1 - lo
                 for cl in classes:
-                    if cl[0] == cre and cl[1] == d and not (cl[2] >> lo) & 1:
+                    if cl[0] == (cre, sy) and cl[1] == d and not (cl[2] >> lo) & 1:
                         cl[2] |= 1 << lo
                         cl[3] += 1
                         break
                 else:
-                    classes.append([cre, d, 1 << lo, 1])
+                    classes.append([(cre, sy), d, 1 << lo, 1])
             else:
-                single.append((k, zl, zo, cre))
+                single.append((k, zl, zo, cre, sy))
         plan.append((xl, classes, outside, single, cplx))
-        const = sum(c for (_, zo, c) in outside if not zo)
-        ts = [f'(pb{k} ? {-c!r} : {c!r})' for (k, zo, c) in outside if zo]
+        const = [cx(c, sy) for (_, zo, c, sy) in outside if not zo]
+        ts = [f'(pb{k} ? {cx(-c, sy)} : {cx(c, sy)})' for (k, zo, c, sy) in outside if zo]
         if const or ts:
-            lines.append(f'        const double dg{gi} = {" + ".join(([repr(const)] if const else []) + ts)};')
+            lines.append(f'        const double dg{gi} = {" + ".join(const + ts)};')
     lines += ['#pragma unroll 1',
               f'        for (uint32_t j0 = threadIdx.x; j0 < {1 << K}u; j0 += 1024u) {{',
               '            double2 v[4];',
@@ -540,36 +571,33 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
         real = bool(classes or outside or single)
         if real:
             lines.append(f'                    double cr = {"dg%d" % gi if outside else "0.0"};')
-            for c, d, m, cnt in classes:
+            for (c, sy), d, m, cnt in classes:
                 pc = f'__popc(jx & {m}u)' if d == 0 else f'__popc((jx ^ (jx >> {d})) & {m}u)'
-                lines.append(f'                    cr = fma({c!r}, (double)({cnt} - 2 * (int){pc}), cr);')
-            for k, zl, zo, c in single:
+                lines.append(f'                    cr = fma({cx(c, sy)}, (double)({cnt} - 2 * (int){pc}), cr);')
+            for k, zl, zo, c, sy in single:
                 parts = [f'__popc(jx & {zl}u)'] + ([f'pb{k}'] if zo else [])
-                lines.append(f'                    cr += (({" ^ ".join(parts)}) & 1u) ? {-c!r} : {c!r};')
+                lines.append(f'                    cr += (({" ^ ".join(parts)}) & 1u) ? {cx(-c, sy)} : {cx(c, sy)};')
             lines.append('                    v[r].x = fma(cr, p[r].x, v[r].x); v[r].y = fma(cr, p[r].y, v[r].y);')
-        for k, zl, zo, cre, cim in cplx:
+        for k, zl, zo, cre, cim, sy in cplx:
             parts = ([f'__popc(jx & {zl}u)'] if zl else []) + ([f'pb{k}'] if zo else [])
             sg = f'(({" ^ ".join(parts)}) & 1u)' if parts else None
-            c = (f'make_double2({cre!r}, {cim!r})' if sg is None else
-                 f'({sg} ? make_double2({-cre!r}, {-cim!r}) : make_double2({cre!r}, {cim!r}))')
+            pos = f'make_double2({cx(cre, sy)}, {cx(cim, sy)})'
+            ng = f'make_double2({cx(-cre, sy)}, {cx(-cim, sy)})'
+            c = pos if sg is None else f'({sg} ? {ng} : {pos})'
             lines.append(f'                    v[r] = cfma({c}, p[r], v[r]);')
         lines.append('                }')
         lines.append('            }')
     lines += ['#pragma unroll',
               '            for (int r = 0; r < 4; ++r) {',
-              '                const uint32_t j = j0 + r * 256u;']
-    if mode != 0:
-        lines.append('                { const ' + T + ' a = s[j]; ere += (double)a.x * v[r].x + (double)a.y * v[r].y; '
-                     'eim += (double)a.x * v[r].y - (double)a.y * v[r].x; }')
-        lines.append('                const uint64_t gi = base + tl2g(ctab, L, j);')
-        if mode == 1:
-            lines.append(f'                out[gi] = mk(({R})v[r].x, ({R})v[r].y);')
-        else:
-            lines.append(f'                {{ {T} o = out[gi]; o.x = ({R})((double)o.x + v[r].x); '
-                         f'o.y = ({R})((double)o.y + v[r].y); out[gi] = o; }}')
+              '                const uint32_t j = j0 + r * 256u;',
+              '                { const ' + T + ' a = s[j]; ere += (double)a.x * v[r].x + (double)a.y * v[r].y; '
+              'eim += (double)a.x * v[r].y - (double)a.y * v[r].x; }',
+              '                const uint64_t gi = base + tl2g(ctab, L, j);']
+    if mode == 1:
+        lines.append(f'                out[gi] = mk(({R})v[r].x, ({R})v[r].y);')
     else:
-        lines.append('                if (want_e) { const ' + T + ' a = s[j]; ere += (double)a.x * v[r].x + '
-                     '(double)a.y * v[r].y; eim += (double)a.x * v[r].y - (double)a.y * v[r].x; }')
+        lines.append(f'                {{ {T} o = out[gi]; o.x = ({R})((double)o.x + v[r].x); '
+                     f'o.y = ({R})((double)o.y + v[r].y); out[gi] = o; }}')
     lines += ['            }', '        }', '    };',
               f'    jit_pauli_kernel<{T}, {K}, 4>(psi, g, want_e, part, smem, body);', '}', '']
     return '\n'.join(lines)
@@ -603,6 +631,28 @@ def compile_pauli(terms: np.ndarray, passes: np.ndarray, matvec: bool, complex64
             kinds.append(None)
             continue
         jobs.append((pauli_source(terms[b:e], K, L, p['high'], mode, complex64), K, 4))
+        kinds.append(KIND_PAULI + mode)
+    workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(lambda a: None if a[0] is None else _load(a[0][0], a[0][1], a[0][2], code, device, a[1]),
+                           zip(jobs, kinds)))
+
+
+def compile_pauli_rows(terms: np.ndarray, passes: np.ndarray, syms: Sequence[Optional[int]], complex64: bool,
+                       device: int, workers: int = 0) -> list:
+    """H psi kernels for rows launches (desv_jit_pauli_matvec_rows): one per
+    tiled pass in the mode the rows driver runs it, with the terms' per-row
+    coefficient symbols (None: the term's coefficient is compiled in)."""
+    code = N.DESV_C64 if complex64 else N.DESV_C128
+    jobs, kinds = [], []
+    for p, mode in zip(passes, pauli_modes(passes, True)):
+        K, L = int(p['tile_bits']), int(p['low_bits'])
+        b, e = int(p['term_begin']), int(p['term_end'])
+        if mode is None or K < 10 or K - L > 8 or not 0 < e - b <= MAX_PAULI_TERMS:
+            jobs.append(None)
+            kinds.append(None)
+            continue
+        jobs.append((pauli_source(terms[b:e], K, L, p['high'], mode, complex64, syms=list(syms[b:e])), K, 4))
         kinds.append(KIND_PAULI + mode)
     workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
     with ThreadPoolExecutor(max_workers=workers) as ex:

@@ -276,6 +276,15 @@ int desv_apply_passes_rows(void *states, int n, int dtype, int rows, const desv_
 int desv_pauli_matvec_rows(const void *psi, void *out, int n, int dtype, int rows, const desv_pauli_pass *passes,
                            int npasses, const desv_pauli_term *terms_dev, int64_t term_stride, double *expect_dev,
                            double *norm_dev, void *scratch, size_t scratch_bytes, void *stream);
+/* desv_pauli_matvec_rows with the tiled passes that have a specialised rows
+ * kernel (handles[p] != NULL, desv_jit_load kind 3 / 4 for the first / later
+ * passes, compiled with per-row coefficient symbols): such a kernel reads row
+ * r's coefficients from csym_dev + r * nsym; the other passes run on the
+ * interpreter from the term tables. */
+int desv_jit_pauli_matvec_rows(void *const *handles, const double *csym_dev, int nsym, const void *psi, void *out,
+                               int n, int dtype, int rows, const desv_pauli_pass *passes, int npasses,
+                               const desv_pauli_term *terms_dev, int64_t term_stride, double *expect_dev,
+                               double *norm_dev, void *scratch, size_t scratch_bytes, void *stream);
 /* desv_adjoint_passes on every row: grad_dev[r * grad_stride + map[...]] +=
  * 2 Re<lambda_r|G|phi_r> (not zeroed here). */
 int desv_adjoint_passes_rows(void *phi, void *lam, int n, int dtype, int rows, const desv_adj_pass *passes,

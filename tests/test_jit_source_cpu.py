@@ -109,3 +109,63 @@ def test_tangent_variant_sources():
     if r == N.DESV_EUNSUPPORTED:
         pytest.skip('NVRTC not available: ' + N.last_error())
     assert r == 0, log.value.decode()[-3000:]
+
+
+def test_rows_pauli_sources_read_per_row_coefficients():
+    """H psi kernels of a rows group: coefficients equal in every row (the XX and
+    YY terms of the XXZ chains) are compiled in, the others (each row's J_z)
+    are read per row from the symbol table, terms sharing a column fold into one
+    class, and the sources compile with NVRTC."""
+    from dense_evolution.physics.observables import plan_for
+    from dense_evolution.workloads import xxz_terms
+    n = 14
+    plan = plan_for([(1.0, p) for _, p in xxz_terms(n, 1.0)], n, None, torch.complex64)
+    jz = np.array([0.7, 1.3, 0.9])
+    co = np.array([[float(c) for c, _ in xxz_terms(n, z)] for z in jz])[:, plan.order]
+    syms = [None if np.all(co[:, k] == co[0, k]) else 0 for k in range(co.shape[1])]
+    assert syms.count(0) == n - 1
+    srcs = []
+    for p, mode in zip(plan.passes, jit.pauli_modes(plan.passes, True)):
+        b, e = int(p['term_begin']), int(p['term_end'])
+        if mode is None or int(p['tile_bits']) < 10:
+            continue
+        srcs.append(jit.pauli_source(plan.terms[b:e], int(p['tile_bits']), int(p['low_bits']), p['high'], mode, True,
+                                     syms=syms[b:e]))
+    assert srcs
+    text = '\n'.join(srcs)
+    assert 'const double C0 = csym[0];' in text and 'RowStrides rs' in text and '* C0)' in text
+    log = ctypes.create_string_buffer(16384)
+    for src in srcs:
+        r = N.lib().desv_jit_compile_check(src.encode(), jit.INCLUDE_PATH.encode(), log, 16384)
+        if r == N.DESV_EUNSUPPORTED:
+            pytest.skip('NVRTC not available: ' + N.last_error())
+        assert r == 0, log.value.decode()[-3000:]
+
+
+@pytest.mark.parametrize('dtname', ['complex64', 'complex128'])
+def test_pauli_sources_of_mixed_terms_compile(dtname):
+    """Every specialised Pauli pass (both <H> and H psi modes) of a term set
+    mixing flip masks, Y phases, negative and complex coefficients, sign masks
+    reaching outside the tile and a wide mask compiles with NVRTC."""
+    from dense_evolution.physics.observables import plan_for
+    from dense_evolution.workloads import tfim_terms, xxz_terms
+    n = 13
+    terms = (tfim_terms(n) + xxz_terms(n, 0.7) + [(0.3, {0: 'Y', n - 1: 'Y'}), (0.2, {1: 'X', 2: 'Y', 7: 'Z'}),
+             (-0.4, 'Z' * n), (0.15j, {q: 'X' for q in range(0, n, 2)}), (-0.25, {3: 'Y'})])
+    dt = getattr(torch, dtname)
+    plan = plan_for(terms, n, dtype=dt)
+    log = ctypes.create_string_buffer(16384)
+    count = 0
+    for p, mode in zip(plan.passes, jit.pauli_modes(plan.passes, True)):
+        K, L = int(p['tile_bits']), int(p['low_bits'])
+        b, e = int(p['term_begin']), int(p['term_end'])
+        if mode is None or K < 10 or K - L > 8 or not 0 < e - b <= jit.MAX_PAULI_TERMS:
+            continue
+        for m in (mode, 0):
+            src = jit.pauli_source(plan.terms[b:e], K, L, p['high'], m, dt == torch.complex64)
+            r = N.lib().desv_jit_compile_check(src.encode(), jit.INCLUDE_PATH.encode(), log, 16384)
+            if r == N.DESV_EUNSUPPORTED:
+                pytest.skip('NVRTC not available: ' + N.last_error())
+            assert r == 0, log.value.decode()[-3000:]
+            count += 1
+    assert count >= 2
