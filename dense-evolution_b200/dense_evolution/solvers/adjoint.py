@@ -462,6 +462,10 @@ class AdjointProgram:
             e = _EnergyFunction.apply(theta, self, h, stato_zero, box, noise)
             return e, box['sv']
         th = _as_theta(theta)
+        if noise is not None and self._fused_noise_applies(noise):
+            psi = self._noisy_state(th, stato_zero, noise)
+            _, e = self.apply_h(h, psi, need_lambda=False)
+            return torch.tensor(e, dtype=torch.float64), psi
         psi = self.forward_state(th, stato_zero)
         if noise is not None:
             psi, _ = self.apply_noise(psi, noise)
@@ -470,6 +474,61 @@ class AdjointProgram:
             ratio = self.norm_ratio(psi, stato_zero)
         _, e = self.apply_h(h, psi, need_lambda=False)
         return torch.tensor(e * ratio, dtype=torch.float64), psi
+
+    # ------------------------------------------------------------ noise in the circuit's passes
+    @staticmethod
+    def _fused_noise_applies(noise) -> bool:
+        from ..noise import kraus_channels as K
+        return noise.model in K.PAULI_MODELS and float(noise.p) > 0.0
+
+    def _noise_template(self, model: str, bits):
+        """(CompiledCircuit, slot of every (bit, letter), gphase slot): the
+        circuit followed by a parametric Pauli template on the noise qubits --
+        per noise qubit rx / ry / rz (depolarizing), rx (bitflip) or rz
+        (phaseflip), then one gphase -- compiled once per (model, qubits), so
+        the template's gates ride in the circuit's own passes.  A fired error w
+        on bit q sets its gate's angle to pi (X = i Rx(pi), Y = i Ry(pi),
+        Z = i Rz(pi)) and adds pi/2 to the gphase angle; every other angle is 0."""
+        key = (model, tuple(bits))
+        cache = self.__dict__.setdefault('_noise_tpl', {})
+        got = cache.get(key)
+        if got is not None:
+            return got
+        letters = 'xyz' if model == 'depolarizing' else ('x' if model == 'bitflip' else 'z')
+        rows, slots = list(self.rows), list(self.slots)
+        k = max(self.nparams, 1 + max(slots, default=-1))
+        where = {}
+        for q in bits:
+            for w in letters:
+                rows.append((f'r{w}', self.n - 1 - int(q), 0.0))
+                slots.append(k)
+                where[(int(q), w)] = k
+                k += 1
+        rows.append(('gphase', 0, 0.0))
+        slots.append(k)
+        got = (CompiledCircuit(rows, self.n, self.dtype, slots=slots), where, k)
+        cache[key] = got
+        return got
+
+    def _noisy_state(self, th: np.ndarray, stato_zero, noise) -> torch.Tensor:
+        """The circuit's output under one Pauli-channel shot, normalised as the
+        reference does (division by norm + 1e-15): the drawn errors are the
+        angles of the noise template, so they are applied inside the circuit's
+        passes instead of as passes of their own over a copy."""
+        from ..noise import kraus_channels as K
+        rng = K.resolve_rng(getattr(noise, 'rng', None), getattr(noise, 'jax_key', None))
+        qubits = list(noise.qubits) if getattr(noise, 'qubits', None) is not None else list(range(self.n))
+        errs = K.draw_pauli_errors(noise.model, float(noise.p), self.n, rng, qubits)
+        cc, where, gslot = self._noise_template(noise.model, qubits)
+        full = np.zeros(gslot + 1)
+        full[:min(th.size, gslot + 1)] = th[:gslot + 1]
+        for q, w in errs:
+            full[where[(int(q), w)]] = np.pi
+        full[gslot] = 0.5 * np.pi * len(errs)
+        psi = self.initial_state(stato_zero)
+        cc.run(psi, theta=full)
+        K.normalize_plus_eps(psi)
+        return psi
 
     def apply_noise(self, psi: torch.Tensor, noise):
         """(noisy normalised copy of psi, Pauli errors or None for damping channels)."""

@@ -109,3 +109,24 @@ def test_energy_fn_damping_gradient_refused():
     e, _ = fn(th, terms, noise=de.NoiseSpec('amplitude_damping', 0.3, 1))
     with pytest.raises(NotImplementedError):
         e.backward()
+
+
+@pytest.mark.parametrize('model', ['depolarizing', 'bitflip', 'phaseflip'])
+def test_noise_rides_in_the_circuit_passes(model):
+    """energy_fn(noise=...) without a gradient applies the Pauli shot inside the
+    circuit's own passes (the noise template's angles); at 20 qubits complex64
+    (rotation passes) it matches the shot applied as passes of their own over a
+    copy of the state: |dE| <= 1e-6, amplitudes to 1e-5."""
+    import dense_evolution as de
+    n = 20
+    circ, rows, npar, theta, terms = _problem(n)
+    fn, _ = de.circuit_to_energy_fn(circ, n, use_float32=True)
+    prog = fn.program
+    spec = de.NoiseSpec(model, 0.3, 7, qubits=[0, 5, 13, 19])
+    e1, sv1 = fn(theta, terms, noise=spec)
+    psi = prog.forward_state(np.asarray(theta))
+    noisy, errs = prog.apply_noise(psi, spec)
+    _, e2 = prog.apply_h(terms, noisy, need_lambda=False)
+    assert errs                      # the seed fires at least one error
+    assert float(e1) == pytest.approx(e2, abs=1e-6)
+    assert float(np.max(np.abs(sv1.cpu().numpy() - noisy.cpu().numpy()))) < 1e-5
