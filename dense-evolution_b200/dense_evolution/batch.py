@@ -194,7 +194,7 @@ class _RowsPlan:
             specs = adjoint._split_params(fusion.schedule(bops, n, kb), bops, 1024) if bops else []
             if self.use_jit and dtype == torch.complex64:
                 # every backward pass short enough for a specialised kernel
-                specs = adjoint._split_ops(specs, adjoint.SPECIALISED_OPS_PER_PASS)
+                specs = adjoint._split_ops(specs, adjoint.ops_per_pass())
             self.bwd = fusion.Packed(n, bops, specs, adjoint=True)
         cdt = np.complex64 if dtype == torch.complex64 else np.complex128
         th0 = 0.37 + 0.0137 * np.arange(max(self.nparams, 1))   # generic angles: flags valid for every theta

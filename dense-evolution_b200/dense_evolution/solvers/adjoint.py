@@ -219,7 +219,7 @@ class AdjointProgram:
             specs = fusion.schedule(self.bops, self.n, kb)
             specs = _split_params(specs, self.bops, 1024)
             if dtype == torch.complex64 and jit.enabled(self.n):
-                specs = _split_ops(specs, SPECIALISED_OPS_PER_PASS)
+                specs = _split_ops(specs, ops_per_pass())
             self.back = fusion.Packed(self.n, self.bops, specs, adjoint=True)
         else:
             self.back = None
@@ -639,6 +639,15 @@ def _split_params(specs, ops, cap):
 # layers of the circuit) took 15.8 ms interpreted, and the gradient went from
 # 30.0 ms to 19.4 ms (cap 60) and 17.5 ms (cap 40).
 SPECIALISED_OPS_PER_PASS = 40
+
+
+def ops_per_pass() -> int:
+    """SPECIALISED_OPS_PER_PASS, or DESV_ADJ_OPS_PER_PASS (tuning sweeps)."""
+    import os
+    v = int(os.environ.get('DESV_ADJ_OPS_PER_PASS', SPECIALISED_OPS_PER_PASS))
+    if not 8 <= v <= 90:
+        raise ValueError('DESV_ADJ_OPS_PER_PASS must be in [8, 90]')
+    return v
 
 
 def _split_ops(specs, cap):
