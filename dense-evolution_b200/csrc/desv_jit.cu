@@ -389,7 +389,10 @@ extern "C" int desv_jit_adjoint(void *handle, void *phi, void *lam, int n, int d
     int np = ps->nparams;
     double *part = static_cast<double *>(scratch);
     RowStrides rs{0, 0, 0, 0};
-    void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&mats_dev), &np, &part, &rs};
+    const unsigned char *rflag = nullptr;
+    int want = 0;
+    void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&mats_dev), &np, &part, &rs,
+                    &rflag, &want};
     if (api().LaunchKernel(k->fn, grid, 1, 1, 1u << (k->K - 4), 1, 1, (unsigned)smem, stream, args, nullptr) != 0)
         return fail(DESV_ECUDA, "jit adjoint: launch failed");
     if (np > 0) return grad_reduce(part, (int)grid, np, map_dev + ps->map_begin, grad_dev, static_cast<cudaStream_t>(stream));
@@ -435,11 +438,72 @@ extern "C" int desv_jit_adjoint_rows(void *handle, void *phi, void *lam, int n, 
     int np = ps->nparams;
     double *part = static_cast<double *>(scratch);
     RowStrides rs{(int64_t)1 << n, pool_stride, 0, (int64_t)gx * np};
+    const unsigned char *rflag = nullptr;
+    int want = 0;
     void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&pools_dev), &np, &part,
-                    &rs};
+                    &rs, &rflag, &want};
     if (api().LaunchKernel(k->fn, (unsigned)gx, (unsigned)rows, 1, 1u << (k->K - 4), 1, 1, (unsigned)smem, stream,
                            args, nullptr) != 0)
         return fail(DESV_ECUDA, "jit rows adjoint: launch failed");
+    if (np > 0)
+        return grad_reduce_rows(part, gx, np, map_dev + ps->map_begin, grad_dev, rows, grad_stride,
+                                static_cast<cudaStream_t>(stream));
+    return DESV_OK;
+}
+
+extern "C" int desv_jit_adjoint_rows_split(void *handle_tangent, void *handle_general, const unsigned char *rflag_dev,
+                                           void *phi, void *lam, int n, int dtype, int rows, const desv_adj_pass *ps,
+                                           const desv_op *ops_dev, const void *pools_dev, int64_t pool_stride,
+                                           const int32_t *map_dev, double *grad_dev, int64_t grad_stride,
+                                           void *scratch, size_t scratch_bytes, void *stream) {
+    if (!handle_tangent || !handle_general || !rflag_dev || !phi || !lam || !ps || !ops_dev || !pools_dev ||
+        !map_dev || !grad_dev || !scratch)
+        return fail(DESV_EINVAL, "jit rows adjoint (split): null argument");
+    if (phi == lam) return fail(DESV_EINVAL, "jit rows adjoint (split): phi and lambda must be distinct buffers");
+    auto *kt = static_cast<JitKernel *>(handle_tangent);
+    auto *kg = static_cast<JitKernel *>(handle_general);
+    if (kt->kind != 1 || kg->kind != 1) return fail(DESV_EINVAL, "jit rows adjoint (split): not adjoint kernels");
+    if (dtype != kt->dtype || dtype != kg->dtype || kt->K != kg->K)
+        return fail(DESV_EINVAL, "jit rows adjoint (split): the two kernels differ in dtype or tile width");
+    if (n < 1 || n > 34) return fail(DESV_EINVAL, "jit rows adjoint (split): n out of range");
+    if (rows < 1 || rows > 65535) return fail(DESV_EINVAL, "jit rows adjoint (split): row count must be in [1, 65535]");
+    if (pool_stride < 0 || grad_stride < 0) return fail(DESV_EINVAL, "jit rows adjoint (split): negative stride");
+    if (reinterpret_cast<uintptr_t>(phi) % 16 || reinterpret_cast<uintptr_t>(lam) % 16)
+        return fail(DESV_EINVAL, "jit rows adjoint (split): states not 16-byte aligned");
+    if (ps->nparams < 0 || ps->nparams > JIT_ADJ_MAX_PARAMS || ps->map_begin < 0)
+        return fail(DESV_EINVAL, "jit rows adjoint (split): parameter range invalid");
+    if (scratch_bytes < (size_t)rows * JIT_ADJ_ROWS_X * (size_t)(ps->nparams > 0 ? ps->nparams : 1) * sizeof(double))
+        return fail(DESV_EINVAL, "jit rows adjoint (split): scratch smaller than desv_rows_scratch_bytes");
+    TileGeom g;
+    if (ps->tile_bits != kt->K || ps->tile_bits > n || ps->low_bits < 5 || ps->tile_bits - ps->low_bits > 8 ||
+        !make_geom(g, n, ps->tile_bits, ps->low_bits, ps->high))
+        return fail(DESV_EINVAL, "jit rows adjoint (split): tile geometry does not match the compiled kernels");
+    if (ps->op_end == ps->op_begin) return DESV_OK;
+    const int nw = (1 << (kt->K - 4)) / 32 > 0 ? (1 << (kt->K - 4)) / 32 : 1;
+    const size_t smt = kt->smem + (size_t)nw * ps->nparams * sizeof(double);
+    const size_t smg = kg->smem + (size_t)nw * ps->nparams * sizeof(double);
+    // one grid for both launches (the partial-sum layout the reduction reads):
+    // the fewer resident CTAs of the two kernels
+    int bt = 0, bg = 0;
+    api().OccupancyMaxActiveBlocksPerMultiprocessor(&bt, kt->fn, 1 << (kt->K - 4), smt);
+    api().OccupancyMaxActiveBlocksPerMultiprocessor(&bg, kg->fn, 1 << (kg->K - 4), smg);
+    int bps = bt < bg ? bt : bg;
+    if (bps < 1) bps = 1;
+    const uint64_t ntiles = 1ull << (n - kt->K);
+    int gx = rows_grid_x(ntiles, (uint64_t)sm_count() * bps, rows);
+    if (gx > JIT_ADJ_ROWS_X) gx = JIT_ADJ_ROWS_X;
+    int np = ps->nparams;
+    double *part = static_cast<double *>(scratch);
+    RowStrides rs{(int64_t)1 << n, pool_stride, 0, (int64_t)gx * np};
+    for (int want = 1; want >= 0; --want) {
+        JitKernel *k = want ? kt : kg;
+        int w = want;
+        void *args[] = {&phi, &lam, &g, const_cast<desv_op **>(&ops_dev), const_cast<void **>(&pools_dev), &np, &part,
+                        &rs, const_cast<unsigned char **>(&rflag_dev), &w};
+        if (api().LaunchKernel(k->fn, (unsigned)gx, (unsigned)rows, 1, 1u << (k->K - 4), 1, 1,
+                               (unsigned)(want ? smt : smg), stream, args, nullptr) != 0)
+            return fail(DESV_ECUDA, "jit rows adjoint (split): launch failed");
+    }
     if (np > 0)
         return grad_reduce_rows(part, gx, np, map_dev + ps->map_begin, grad_dev, rows, grad_stride,
                                 static_cast<cudaStream_t>(stream));

@@ -419,6 +419,72 @@ __global__ void k_rows_sum(const double *part, int64_t stride, int count, int wi
     }
 }
 
+// Tangent form of the rows' backward passes (the device side of the host's
+// TangentPlan.transform, one thread per pass and row): event kinds 0 / 1 are
+// the tangent ry / rz records (t from the record's matrix, the running product
+// S of the 1/c), 2 / 3 the gradient probes with the generator compiled in /
+// read from the pool (their 1/S^2 correction written into the slot / scaled
+// into the generator), and the pass-end factor 1/S goes to end_base + pass.
+// flags[pass * rows + row] says whether that row runs the pass in tangent form;
+// a row whose |t| leaves [0, tmax] or whose S leaves [0, tmax^2] keeps its
+// matrices and runs the general kernel.
+__global__ void k_rows_tangent(float2 *pools, int64_t pool_stride, int rows, int npass, const int32_t *ev_begin,
+                               const uint8_t *ev_kind, const uint32_t *ev_off, int64_t end_base, double tmax,
+                               uint8_t *flags) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)rows * npass) return;
+    const int p = (int)(i / rows), r = (int)(i % rows);
+    float2 *pool = pools + (size_t)r * pool_stride;
+    const int b = ev_begin[p], e = ev_begin[p + 1];
+    bool any = false, ok = true;
+    double S = 1.0;
+    for (int k = b; k < e && ok; ++k) {
+        const int kind = ev_kind[k];
+        if (kind > 1) continue;
+        const uint32_t off = ev_off[k];
+        const double c = pool[off].x;
+        const double t = (kind == 0 ? (double)pool[off + 2].x : (double)pool[off].y) / c;
+        any = true;
+        S /= c;
+        if (!(fabs(t) <= tmax) || !(fabs(S) <= tmax * tmax)) ok = false;
+    }
+    ok = ok && any;
+    flags[(size_t)p * rows + r] = ok ? 1 : 0;
+    if (!ok) return;
+    S = 1.0;
+    for (int k = b; k < e; ++k) {
+        const int kind = ev_kind[k];
+        const uint32_t off = ev_off[k];
+        if (kind <= 1) {
+            const double c = pool[off].x;
+            const double t = (kind == 0 ? (double)pool[off + 2].x : (double)pool[off].y) / c;
+            pool[off] = make_float2((float)t, 0.f);
+            S /= c;
+        } else {
+            const double corr = 1.0 / (S * S);
+            if (kind == 2) {
+                pool[off] = make_float2((float)corr, 0.f);
+            } else {
+                for (int q = 0; q < 4; ++q) {
+                    pool[off + q].x = (float)((double)pool[off + q].x * corr);
+                    pool[off + q].y = (float)((double)pool[off + q].y * corr);
+                }
+            }
+        }
+    }
+    pool[end_base + p] = make_float2((float)(1.0 / S), 0.f);
+}
+
+int rows_tangent(void *pools, int64_t pool_stride, int rows, int npass, const int32_t *ev_begin, const uint8_t *ev_kind,
+                 const uint32_t *ev_off, int64_t end_base, double tmax, uint8_t *flags, cudaStream_t st) {
+    const int64_t total = (int64_t)rows * npass;
+    if (total == 0) return DESV_OK;
+    k_rows_tangent<<<(unsigned)((total + 127) / 128), 128, 0, st>>>(static_cast<float2 *>(pools), pool_stride, rows,
+                                                                     npass, ev_begin, ev_kind, ev_off, end_base, tmax,
+                                                                     flags);
+    return check_launch("rows: tangent form");
+}
+
 int rows_prepare(int dtype, const desv_batch_recipe *rec, int nrec, const double *theta, int64_t theta_stride,
                  const void *cpool, void *pools, int64_t pool_stride, void *states, int n, int rows, cudaStream_t st) {
     const size_t es = dtype == DESV_C64 ? 8 : 16;

@@ -28,6 +28,7 @@ in gate order (``solvers/autodiff.py:21,150-157``).
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Dict, List, Sequence, Tuple
 
 import numpy as np
@@ -211,9 +212,30 @@ class _RowsPlan:
             pools.append(bpool)
         self.cpool = np.concatenate(pools)
         self.recipes = np.concatenate(recs)
+        # tangent form of the backward passes (complex64, specialised kernels):
+        # the events the device walks per pass and row, and one pass-end factor
+        # per backward pass after the pool
+        self.tangent = None
+        extra = 0
+        if self.use_jit and dtype == torch.complex64 and self.bwd is not None and len(self.bwd.passes) and \
+                os.environ.get('DESV_ADJ_TANGENT', '1') != '0':
+            tp = adjoint.TangentPlan(self.bwd, len(self.cpool), self.cpool.astype(np.complex64))
+            if any(t for t, _ in tp.passes):
+                self.tangent = tp
+                extra = len(self.bwd.passes)
+                begin, kinds, offs = [0], [], []
+                for tan, events in tp.passes:
+                    if tan:
+                        for kind, off, x in events:
+                            kinds.append((0 if x == 'rot' else 1) if kind == 't' else (3 if x else 2))
+                            offs.append(off)
+                    begin.append(len(kinds))
+                self.ev_begin = np.array(begin, np.int32)
+                self.ev_kind = np.array(kinds or [0], np.uint8)
+                self.ev_off = np.array(offs or [0], np.uint32)
         # every row's pool starts on a 256-byte boundary
         per = 256 // (8 if dtype == torch.complex64 else 16)
-        self.pool_stride = max(per, (len(self.cpool) + per - 1) // per * per)
+        self.pool_stride = max(per, (len(self.cpool) + extra + per - 1) // per * per)
         self.pauli = None
         if terms is not None and not forward_only:
             from .physics.observables import plan_for
@@ -226,7 +248,7 @@ class _RowsPlan:
         records), so one set serves every row.  complex128 backward passes stay
         on the interpreter (two double2 register tiles exceed the register file)."""
         if not self.use_jit:
-            return None, None
+            return None, None, None
         got = self._kernels.get(device)
         if got is None:
             from .circuits import jit
@@ -234,7 +256,12 @@ class _RowsPlan:
             kf = jit.compile_passes(self.fwd.ops, self.fwd.passes, self.cpool, c64, device)
             kb = jit.compile_adjoint(self.bwd.ops, self.bwd.passes, self.cpool, c64, device) \
                 if (self.bwd is not None and c64) else None
-            got = (kf, kb)
+            kt = None
+            if self.tangent is not None:
+                info = self.tangent.sources_info()
+                kt = jit.compile_adjoint(self.bwd.ops, self.bwd.passes, self.cpool, True, device, tangents=info)
+                kt = [k if inf is not None else None for k, inf in zip(kt, info)]
+            got = (kf, kb, kt)
             self._kernels[device] = got
         return got
 
@@ -331,7 +358,14 @@ class _RowsGroup:
         self.norm = torch.ones(B, dtype=torch.float64, device=dev)
         sb = int(N.lib().desv_rows_scratch_bytes(B, max(plan.bwd.max_params, 1), max(len(self.ppasses), 1)))
         self.scratch = torch.empty((sb + 7) // 8, dtype=torch.float64, device=dev)
-        self.kf, self.kb = plan.kernels(dev.index if dev.index is not None else torch.cuda.current_device())
+        self.kf, self.kb, self.kt = plan.kernels(dev.index if dev.index is not None else torch.cuda.current_device())
+        if plan.tangent is not None and self.kt is not None:
+            self.d_ev_begin = torch.from_numpy(plan.ev_begin).to(dev)
+            self.d_ev_kind = torch.from_numpy(plan.ev_kind).to(dev)
+            self.d_ev_off = torch.from_numpy(plan.ev_off.view(np.int32)).to(dev)
+            self.d_flags = torch.zeros(len(self.bwd_passes) * B, dtype=torch.uint8, device=dev)
+        else:
+            self.kt = None
 
     def launch(self, d_theta: torch.Tensor, d_grad: torch.Tensor, stream):
         p, n, B, st = self.plan, self.plan.n, self.B, ctypes.c_void_p(N.stream_ptr(stream))
@@ -341,6 +375,12 @@ class _RowsGroup:
         N.check(N.lib().desv_rows_prepare(vp(self.psi.data_ptr()), n, self.code, B, vp(self.d_recipes.data_ptr()),
                                           len(p.recipes), theta, self.P, vp(self.d_cpool.data_ptr()),
                                           vp(self.pools.data_ptr()), p.pool_stride, st), 'rows prepare')
+        if self.kt is not None:
+            N.check(N.lib().desv_rows_tangent_prepare(vp(self.pools.data_ptr()), self.code, B, p.pool_stride,
+                                                      len(self.bwd_passes), vp(self.d_ev_begin.data_ptr()),
+                                                      vp(self.d_ev_kind.data_ptr()), vp(self.d_ev_off.data_ptr()),
+                                                      p.tangent.end_base, adjoint.TangentPlan.TMAX,
+                                                      vp(self.d_flags.data_ptr()), st), 'rows tangent form')
         rows_forward(self.kf, self.psi, n, self.code, B, self.fwd_passes, self.d_fwd_ops, self.pools, p.pool_stride,
                      st)
         want_norm = p.dtype == torch.complex64
@@ -359,6 +399,15 @@ class _RowsGroup:
         for i in range(len(self.bwd_passes)):
             pp = vp(self.bwd_passes.ctypes.data + i * self.bwd_passes.itemsize)
             k = self.kb[i] if self.kb is not None else None
+            kt = self.kt[i] if self.kt is not None else None
+            if kt is not None and k is not None:
+                N.check(lib.desv_jit_adjoint_rows_split(kt.handle, k.handle, vp(self.d_flags.data_ptr() + i * B),
+                                                        vp(self.psi.data_ptr()), vp(self.lam.data_ptr()), n, self.code,
+                                                        B, pp, vp(self.d_bwd_ops.data_ptr()),
+                                                        vp(self.pools.data_ptr()), p.pool_stride,
+                                                        vp(self.d_map.data_ptr()), vp(grad.data_ptr()), self.P, sc, nsc,
+                                                        st), 'rows adjoint pass (jit, per-row form)')
+                continue
             if k is None:
                 N.check(lib.desv_adjoint_passes_rows(vp(self.psi.data_ptr()), vp(self.lam.data_ptr()), n, self.code,
                                                      B, pp, 1, vp(self.d_bwd_ops.data_ptr()),
@@ -768,7 +817,7 @@ class BatchForward:
                                           len(p.recipes), vp(bufs['theta'].data_ptr()), npar,
                                           vp(bufs['cpool'].data_ptr()), vp(pools.data_ptr()), p.pool_stride, st),
                 'rows prepare')
-        kf, _ = p.kernels(dev.index if dev.index is not None else torch.cuda.current_device())
+        kf, _, _ = p.kernels(dev.index if dev.index is not None else torch.cuda.current_device())
         rows_forward(kf, out, p.n, code, B, passes, bufs['ops'], pools, p.pool_stride, st)
         self._keep = (bufs, pools)     # alive until the stream has run the launches
         return out

@@ -209,8 +209,12 @@ def adjoint_source(ops: np.ndarray, begin: int, end: int, tile_bits: int, nbuf: 
     lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
              f'extern "C" __global__ void __launch_bounds__({1 << (tile_bits - 4)}, {minb})',
              f'desv_jit_kernel({T} *phi, {T} *lam, TileGeom g, const desv_op *__restrict__ ops, '
-             f'const {T} *__restrict__ mats, int nparams, double *part, RowStrides rs) {{',
+             f'const {T} *__restrict__ mats, int nparams, double *part, RowStrides rs, '
+             'const unsigned char *__restrict__ rflag, int want) {',
              '    extern __shared__ __align__(128) unsigned char smem[];',
+             '    // rows launched twice per pass (tangent and general form): a row runs in the',
+             '    // launch its flag selects, the other launch\'s CTAs of that row return at once',
+             '    if (rflag != nullptr && (int)rflag[blockIdx.y] != want) return;',
              '    // rows: this grid row\'s (phi, lambda), pool and partial sums (zero strides: one state)',
              '    phi += blockIdx.y * rs.amps;',
              '    lam += blockIdx.y * rs.amps;',

@@ -111,9 +111,11 @@ class TangentPlan:
     forms, each 1/c times the exact gate.  Per call and pass the host forms
     t = s / c and the running product S of the 1/c; a gradient probe is
     multiplied by 1/S^2 (both arrays carry S), and the pass ends by scaling
-    both arrays by 1/S.  A pass whose |t| or S leaves [0, TMAX] runs in the
-    general form (its matrices untouched) -- the tangent blows up near
-    theta = pi."""
+    both arrays by 1/S.  A pass whose |t| leaves [0, TMAX] or whose S leaves
+    [0, TMAX^2] runs in the general form (its matrices untouched) -- the tangent
+    blows up near theta = pi.  S scales every amplitude alike, so FP32 keeps its
+    relative accuracy; S^2 <= 2^80 keeps the probes' products far inside the
+    FP32 range."""
 
     TMAX = 2.0 ** 20
 
@@ -179,7 +181,7 @@ class TangentPlan:
                         ok = False
                         break
                     S /= c
-                    if not abs(S) <= self.TMAX:
+                    if not abs(S) <= self.TMAX * self.TMAX:
                         ok = False
                         break
                     writes.append((off, t, None))

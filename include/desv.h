@@ -285,6 +285,26 @@ int desv_jit_pauli_matvec_rows(void *const *handles, const double *csym_dev, int
                                int n, int dtype, int rows, const desv_pauli_pass *passes, int npasses,
                                const desv_pauli_term *terms_dev, int64_t term_stride, double *expect_dev,
                                double *norm_dev, void *scratch, size_t scratch_bytes, void *stream);
+/* Tangent form of the rows' backward passes (complex64): per pass p and row r,
+ * walks events [ev_begin[p], ev_begin[p+1]) -- kind 0 / 1: a tangent ry / rz
+ * record at pool offset ev_off (its matrix replaced by t = s / c), kind 2 / 3:
+ * a gradient probe whose generator is compiled in / read from the pool (the
+ * probe's 1/S^2 correction written into its slot / scaled into its generator)
+ * -- and writes the pass-end factor 1/S to end_base + p.  flags_dev[p * rows +
+ * r] = 1 where row r runs pass p in tangent form; a row whose |t| leaves
+ * [0, tmax] or whose S leaves [0, tmax^2] is left untouched (flag 0) and runs
+ * the general kernel. */
+int desv_rows_tangent_prepare(void *pools_dev, int dtype, int rows, int64_t pool_stride, int npasses,
+                              const int32_t *ev_begin_dev, const uint8_t *ev_kind_dev, const uint32_t *ev_off_dev,
+                              int64_t end_base, double tmax, uint8_t *flags_dev, void *stream);
+/* One rows backward pass with the row's form chosen per row: the tangent kernel
+ * runs the rows whose rflag_dev entry is 1, the general kernel the others (both
+ * launched, on one grid), then the per-row gradient reduction. */
+int desv_jit_adjoint_rows_split(void *handle_tangent, void *handle_general, const unsigned char *rflag_dev,
+                                void *phi, void *lam, int n, int dtype, int rows, const desv_adj_pass *pass,
+                                const desv_op *ops_dev, const void *pools_dev, int64_t pool_stride,
+                                const int32_t *map_dev, double *grad_dev, int64_t grad_stride, void *scratch,
+                                size_t scratch_bytes, void *stream);
 /* desv_adjoint_passes on every row: grad_dev[r * grad_stride + map[...]] +=
  * 2 Re<lambda_r|G|phi_r> (not zeroed here). */
 int desv_adjoint_passes_rows(void *phi, void *lam, int n, int dtype, int rows, const desv_adj_pass *passes,

@@ -150,3 +150,50 @@ def test_adjoint_tangent_plan_bookkeeping():
     fd = O.fd_gradient(theta, orows, n, terms, h=1e-5, indices=list(range(0, npar, 7)))
     assert np.allclose(grad[list(range(0, npar, 7))], fd, atol=1e-7)
     assert np.max(np.abs(mu - O.zero_state(n))) < 1e-10
+
+
+def test_rows_tangent_events_reproduce_the_host_transform():
+    """The event arrays a rows plan hands the device (kinds 0/1 tangent ry/rz
+    records, 2/3 probes with compiled-in / pool-read generators, per pass),
+    walked as the device kernel walks them, rewrite a row's pool exactly as the
+    host TangentPlan.transform does, pass-end factors included."""
+    import torch
+    from dense_evolution.batch import _RowsPlan, hea_xxz_batch
+    from dense_evolution.solvers.autodiff import build_template
+    n = 13
+    circ, _, terms = hea_xxz_batch([n], 3, [0.8])[0]
+    rows, slots, npar = build_template(circ, n)
+    p = _RowsPlan(rows, slots, n, torch.complex64, 12, terms=terms, use_jit=True)
+    assert p.tangent is not None
+    theta = np.random.default_rng(2).uniform(-np.pi, np.pi, npar)
+    pool = _recipe_pool(p, theta, p.cpool.astype(np.complex128)).astype(np.complex64)
+    want, flags = p.tangent.transform(pool)
+    dev = np.concatenate([pool, np.ones(p.pool_stride - len(pool), np.complex64)])
+    for q in range(len(p.bwd.passes)):
+        b, e = int(p.ev_begin[q]), int(p.ev_begin[q + 1])
+        S, ok, anyt = 1.0, True, False
+        for k in range(b, e):
+            kind, off = int(p.ev_kind[k]), int(p.ev_off[k])
+            if kind <= 1:
+                c = float(dev[off].real)
+                t = (float(dev[off + 2].real) if kind == 0 else float(dev[off].imag)) / c
+                anyt, S = True, S / c
+                ok = ok and abs(t) <= p.tangent.TMAX and abs(S) <= p.tangent.TMAX ** 2
+        assert (ok and anyt) == flags[q]
+        if not (ok and anyt):
+            continue
+        S = 1.0
+        for k in range(b, e):
+            kind, off = int(p.ev_kind[k]), int(p.ev_off[k])
+            if kind <= 1:
+                c = float(dev[off].real)
+                t = (float(dev[off + 2].real) if kind == 0 else float(dev[off].imag)) / c
+                dev[off] = t
+                S /= c
+            elif kind == 2:
+                dev[off] = 1.0 / (S * S)
+            else:
+                dev[off:off + 4] = dev[off:off + 4] * (1.0 / (S * S))
+        dev[p.tangent.end_base + q] = 1.0 / S
+    m = len(want)
+    assert np.allclose(dev[:m], want, rtol=1e-6, atol=1e-7)
