@@ -677,6 +677,8 @@ class BatchVQE:
             nb = int(np.sum(g.bwd_passes['op_end'] > g.bwd_passes['op_begin']))
             nbr = int(np.sum((g.bwd_passes['op_end'] > g.bwd_passes['op_begin']) & (g.bwd_passes['nparams'] > 0)))
             k += 1 + nf + npl + 1 + (2 if g.plan.dtype == torch.complex64 else 0) + 1 + nb + nbr
+            if g.kt is not None:     # the tangent prepare, and a second launch per tangent pass
+                k += 1 + sum(1 for kt in g.kt if kt is not None)
         return k
 
     def capture(self):
