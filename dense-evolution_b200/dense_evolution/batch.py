@@ -239,7 +239,7 @@ class _RowsPlan:
         self.pauli = None
         if terms is not None and not forward_only:
             from .physics.observables import plan_for
-            self.pauli = plan_for([(1.0, p) for _, p in terms], n, None, dtype)
+            self.pauli = plan_for([(1.0, p) for _, p in terms], n, None, dtype, wide_tiles=self.use_jit)
 
     def kernels(self, device: int):
         """(forward, backward) lists of specialised kernels per pass (None: that

@@ -461,7 +461,7 @@ def _expect_source(terms: np.ndarray, K: int, L: int, high, complex64: bool) -> 
         lines.append('        ere += ' + ' + '.join(er) + ';')
     if ei:
         lines.append('        eim += ' + ' + '.join(ei) + ';')
-    lines += ['    };', f'    jit_pauli_kernel<{T}, {K}, 4>(psi, g, want_e, part, smem, body);', '}', '']
+    lines += ['    };', f'    jit_pauli_kernel<{T}, {K}, {pauli_nbuf(K)}>(psi, g, want_e, part, smem, body);', '}', '']
     return '\n'.join(lines)
 
 
@@ -603,8 +603,14 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
         lines.append(f'                {{ {T} o = out[gi]; o.x = ({R})((double)o.x + v[r].x); '
                      f'o.y = ({R})((double)o.y + v[r].y); out[gi] = o; }}')
     lines += ['            }', '        }', '    };',
-              f'    jit_pauli_kernel<{T}, {K}, 4>(psi, g, want_e, part, smem, body);', '}', '']
+              f'    jit_pauli_kernel<{T}, {K}, {pauli_nbuf(K)}>(psi, g, want_e, part, smem, body);', '}', '']
     return '\n'.join(lines)
+
+
+def pauli_nbuf(tile_bits: int) -> int:
+    """Ring slots of a specialised Pauli pass: four for tiles of up to 11 bits,
+    two for 12-bit tiles (three CTAs of 64 KB per SM)."""
+    return 2 if tile_bits >= 12 else 4
 
 
 def pauli_modes(passes: np.ndarray, matvec: bool) -> list:
@@ -634,7 +640,7 @@ def compile_pauli(terms: np.ndarray, passes: np.ndarray, matvec: bool, complex64
             jobs.append(None)
             kinds.append(None)
             continue
-        jobs.append((pauli_source(terms[b:e], K, L, p['high'], mode, complex64), K, 4))
+        jobs.append((pauli_source(terms[b:e], K, L, p['high'], mode, complex64), K, pauli_nbuf(K)))
         kinds.append(KIND_PAULI + mode)
     workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
     with ThreadPoolExecutor(max_workers=workers) as ex:
@@ -656,7 +662,8 @@ def compile_pauli_rows(terms: np.ndarray, passes: np.ndarray, syms: Sequence[Opt
             jobs.append(None)
             kinds.append(None)
             continue
-        jobs.append((pauli_source(terms[b:e], K, L, p['high'], mode, complex64, syms=list(syms[b:e])), K, 4))
+        jobs.append((pauli_source(terms[b:e], K, L, p['high'], mode, complex64, syms=list(syms[b:e])), K,
+                     pauli_nbuf(K)))
         kinds.append(KIND_PAULI + mode)
     workers = workers or min(32, os.cpu_count() or 1, max(1, len(jobs)))
     with ThreadPoolExecutor(max_workers=workers) as ex:

@@ -242,20 +242,39 @@ def _terms_key(terms, n, nq):
         return None
 
 
-def plan_for(terms, n: int, n_qubits=None, dtype=torch.complex128) -> PauliPlan:
-    tb = 11 if dtype == torch.complex64 else 10
+def _plan(terms, n, n_qubits, dtype, wide_tiles) -> PauliPlan:
+    """The Pauli plan of a term list: 11-bit tiles for complex64 (10 for
+    complex128, the interpreter's bound), or 12-bit ones when every tiled pass
+    of that plan gets a specialised kernel (fewer passes, and twice the work per
+    tile against each tile's barriers)."""
+    if dtype == torch.complex64 and wide_tiles and n >= 12:
+        from ..circuits import jit
+        wide = PauliPlan(terms, n, n_qubits, tile_bits=12)
+        if all(int(p['tile_bits']) == 0 or (int(p['term_end']) - int(p['term_begin']) <= jit.MAX_PAULI_TERMS and
+                                            int(p['tile_bits']) - int(p['low_bits']) <= 8) for p in wide.passes):
+            return wide
+    return PauliPlan(terms, n, n_qubits, tile_bits=11 if dtype == torch.complex64 else 10)
+
+
+def plan_for(terms, n: int, n_qubits=None, dtype=torch.complex128, wide_tiles=None) -> PauliPlan:
+    """Cached Pauli plan; wide_tiles (default: the specialised kernels are in
+    use at this size) allows 12-bit tiles for complex64."""
+    if wide_tiles is None:
+        from ..circuits import jit
+        wide_tiles = jit.enabled(n)
+    wide_tiles = bool(wide_tiles)
     terms = list(terms)
     key = _terms_key(terms, n, n_qubits)
     if key is not None:
-        key = key + (tb,)
+        key = key + (dtype == torch.complex64, wide_tiles)
         p = _plan_cache.get(key)
         if p is None:
-            p = PauliPlan(terms, n, n_qubits, tile_bits=tb)
+            p = _plan(terms, n, n_qubits, dtype, wide_tiles)
             if len(_plan_cache) > 64:
                 _plan_cache.clear()
             _plan_cache[key] = p
         return p
-    return PauliPlan(terms, n, n_qubits, tile_bits=tb)
+    return _plan(terms, n, n_qubits, dtype, wide_tiles)
 
 
 def _to_device_state(statevector) -> Tuple[torch.Tensor, bool]:
