@@ -159,46 +159,68 @@ class TangentPlan:
         in tangent form, the general kernel serves it)."""
         return [(tan, self.end_base + i) if tan else None for i, (tan, _) in enumerate(self.passes)]
 
+    def _flat(self):
+        """Flat event arrays (pass, kind 0 rot / 1 phase / 2 probe with compiled-in
+        generator / 3 probe reading its generator, pool offset), built once."""
+        if getattr(self, '_flat_ev', None) is None:
+            ps, kind, off = [], [], []
+            for i, (tan, events) in enumerate(self.passes):
+                if not tan:
+                    continue
+                for k, o, x in events:
+                    ps.append(i)
+                    kind.append((0 if x == 'rot' else 1) if k == 't' else (3 if x else 2))
+                    off.append(o)
+            self._flat_ev = (np.array(ps, np.int64), np.array(kind, np.int8), np.array(off, np.int64))
+        return self._flat_ev
+
     def transform(self, mats: np.ndarray):
         """(pool extended by one pass-end factor per pass, with every pass that
-        can run in tangent form rewritten for it; per-pass flags)."""
-        out = np.concatenate([mats, np.ones(len(self.passes), mats.dtype)])
-        flags = []
-        for i, (tan, events) in enumerate(self.passes):
-            if not tan:
-                flags.append(False)
-                continue
-            S, ok, writes = 1.0, True, []
-            for kind, off, extra in events:
-                if kind == 't':
-                    if extra == 'rot':
-                        c = float(mats[off].real)
-                        t = float(mats[off + 2].real) / c if c != 0.0 else np.inf
-                    else:
-                        c = float(mats[off].real)
-                        t = float(mats[off].imag) / c if c != 0.0 else np.inf
-                    if not abs(t) <= self.TMAX:
-                        ok = False
-                        break
-                    S /= c
-                    if not abs(S) <= self.TMAX * self.TMAX:
-                        ok = False
-                        break
-                    writes.append((off, t, None))
-                else:
-                    writes.append((off, 1.0 / (S * S), extra))
-            flags.append(ok)
-            if not ok:
-                continue
-            for off, v, reads_pool in writes:
-                if reads_pool is None:
-                    out[off] = v                       # the tangent t
-                elif reads_pool:
-                    out[off:off + 4] = mats[off:off + 4] * v   # generator read at run time: pre-scaled
-                else:
-                    out[off] = v                       # immediate-form probe: its correction
-            out[self.end_base + i] = 1.0 / S
-        return out, flags
+        can run in tangent form rewritten for it; per-pass flags).  Vectorised
+        over the events: the running product S of a pass is a cumulative
+        product of its tangent records' 1/c."""
+        npass = len(self.passes)
+        out = np.concatenate([mats, np.ones(npass, mats.dtype)])
+        ps, kind, off = self._flat()
+        flags = np.zeros(npass, bool)
+        if ps.size == 0:
+            return out, list(flags)
+        tanm = kind <= 1
+        c = np.ones(ps.size)
+        t = np.zeros(ps.size)
+        with np.errstate(divide='ignore', invalid='ignore'):
+            c[tanm] = mats[off[tanm]].real
+            num = np.where(kind == 0, mats[np.minimum(off + 2, len(mats) - 1)].real, mats[off].imag)
+            t[tanm] = (num / c)[tanm]
+            f = 1.0 / c                                   # 1 at probes
+        # S after every event, per pass (cumulative product restarted at each pass)
+        S = np.empty(ps.size)
+        starts = np.flatnonzero(np.r_[True, ps[1:] != ps[:-1]])
+        ends = np.r_[starts[1:], ps.size]
+        ok_pass = np.zeros(npass, bool)
+        for a, b in zip(starts, ends):
+            S[a:b] = np.cumprod(f[a:b])
+            seg_ok = (np.all(np.abs(t[a:b][tanm[a:b]]) <= self.TMAX) and
+                      np.all(np.abs(S[a:b]) <= self.TMAX * self.TMAX) and np.any(tanm[a:b]))
+            ok_pass[ps[a]] = bool(seg_ok)
+        flags = ok_pass
+        use = flags[ps]
+        # tangent records: t; immediate probes: 1/S^2; probes reading their
+        # generator: the generator times 1/S^2 (S at a probe: its factor is 1)
+        sel = use & tanm
+        out[off[sel]] = t[sel]
+        corr = 1.0 / (S * S)
+        sel = use & (kind == 2)
+        out[off[sel]] = corr[sel]
+        sel = np.flatnonzero(use & (kind == 3))
+        for q in range(4):
+            out[off[sel] + q] = mats[off[sel] + q] * corr[sel]
+        # pass-end factors 1/S of the last event of every pass in tangent form
+        last = ends - 1
+        for a, l in zip(starts, last):
+            if flags[ps[a]]:
+                out[self.end_base + ps[a]] = 1.0 / S[l]
+        return out, list(flags)
 
 
 def _adjoint_tile_bits(n: int, dtype) -> int:
