@@ -27,7 +27,7 @@ int rows_prepare(int, const desv_batch_recipe *, int, const double *, int64_t, c
 int rows_norm(const void *, int, int, int, double *, double *, cudaStream_t);
 int rows_sum(const double *, int64_t, int, int, double *, int, cudaStream_t);
 int rows_tangent(void *, int64_t, int, int, const int32_t *, const uint8_t *, const uint32_t *, int64_t, double,
-                 uint8_t *, cudaStream_t);
+                 const uint8_t *, uint8_t *, cudaStream_t);
 int jit_pauli_rows_launch(void *, const void *, void *, int, int, const TileGeom &, int, double *, int *, int,
                           const RowStrides &, const double *, int, cudaStream_t);
 
@@ -76,13 +76,14 @@ int desv_rows_prepare(void *states, int n, int dtype, int rows, const desv_batch
 
 int desv_rows_tangent_prepare(void *pools, int dtype, int rows, int64_t pool_stride, int npasses,
                               const int32_t *ev_begin_dev, const uint8_t *ev_kind_dev, const uint32_t *ev_off_dev,
-                              int64_t end_base, double tmax, uint8_t *flags_dev, void *stream) {
+                              int64_t end_base, double tmax, const uint8_t *allowed_dev, uint8_t *flags_dev,
+                              void *stream) {
     if (dtype != DESV_C64) return fail(DESV_EINVAL, "rows tangent: complex64 pools only");
     if (!pools || !ev_begin_dev || !flags_dev || npasses < 0 || rows < 1 || rows > 65535 || pool_stride < 0 ||
         end_base < 0 || end_base + npasses > pool_stride || !(tmax > 0))
         return fail(DESV_EINVAL, "rows tangent: invalid arguments");
     return rows_tangent(pools, pool_stride, rows, npasses, ev_begin_dev, ev_kind_dev, ev_off_dev, end_base, tmax,
-                        flags_dev, S(stream));
+                        allowed_dev, flags_dev, S(stream));
 }
 
 int desv_apply_passes_rows(void *states, int n, int dtype, int rows, const desv_pass *passes, int npasses,

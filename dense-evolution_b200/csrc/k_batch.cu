@@ -430,7 +430,7 @@ __global__ void k_rows_sum(const double *part, int64_t stride, int count, int wi
 // matrices and runs the general kernel.
 __global__ void k_rows_tangent(float2 *pools, int64_t pool_stride, int rows, int npass, const int32_t *ev_begin,
                                const uint8_t *ev_kind, const uint32_t *ev_off, int64_t end_base, double tmax,
-                               uint8_t *flags) {
+                               const uint8_t *allowed, uint8_t *flags) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)rows * npass) return;
     const int p = (int)(i / rows), r = (int)(i % rows);
@@ -449,6 +449,9 @@ __global__ void k_rows_tangent(float2 *pools, int64_t pool_stride, int rows, int
         if (!(fabs(t) <= tmax) || !(fabs(S) <= tmax * tmax)) ok = false;
     }
     ok = ok && any;
+    // allowed (one entry per pass, decided by the caller from the angles with a
+    // margin): the caller's choice replaces the check
+    if (allowed) ok = allowed[p] != 0 && any;
     flags[(size_t)p * rows + r] = ok ? 1 : 0;
     if (!ok) return;
     S = 1.0;
@@ -476,12 +479,13 @@ __global__ void k_rows_tangent(float2 *pools, int64_t pool_stride, int rows, int
 }
 
 int rows_tangent(void *pools, int64_t pool_stride, int rows, int npass, const int32_t *ev_begin, const uint8_t *ev_kind,
-                 const uint32_t *ev_off, int64_t end_base, double tmax, uint8_t *flags, cudaStream_t st) {
+                 const uint32_t *ev_off, int64_t end_base, double tmax, const uint8_t *allowed, uint8_t *flags,
+                 cudaStream_t st) {
     const int64_t total = (int64_t)rows * npass;
     if (total == 0) return DESV_OK;
     k_rows_tangent<<<(unsigned)((total + 127) / 128), 128, 0, st>>>(static_cast<float2 *>(pools), pool_stride, rows,
                                                                      npass, ev_begin, ev_kind, ev_off, end_base, tmax,
-                                                                     flags);
+                                                                     allowed, flags);
     return check_launch("rows: tangent form");
 }
 

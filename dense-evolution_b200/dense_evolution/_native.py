@@ -86,8 +86,8 @@ _SIGS = {
     'desv_adjoint_passes_rows': ([_vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp, ctypes.c_int64, _vp, _vp,
                                   ctypes.c_int64, _vp, _sz, _vp], _i),
     'desv_jit_pass_rows': ([_vp, _vp, _i, _i, _i, _vp, _vp, ctypes.c_int64, _vp], _i),
-    'desv_rows_tangent_prepare': ([_vp, _i, _i, ctypes.c_int64, _i, _vp, _vp, _vp, ctypes.c_int64, _d, _vp, _vp],
-                                  _i),
+    'desv_rows_tangent_prepare': ([_vp, _i, _i, ctypes.c_int64, _i, _vp, _vp, _vp, ctypes.c_int64, _d, _vp, _vp,
+                                   _vp], _i),
     'desv_jit_adjoint_rows_split': ([_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp,
                                      ctypes.c_int64, _vp, _sz, _vp], _i),
     'desv_jit_pauli_matvec_rows': ([_vp, _vp, _i, _vp, _vp, _i, _i, _i, _vp, _i, _vp, ctypes.c_int64, _vp, _vp, _vp,

@@ -379,7 +379,7 @@ class _RowsGroup:
             N.check(N.lib().desv_rows_tangent_prepare(vp(self.pools.data_ptr()), self.code, B, p.pool_stride,
                                                       len(self.bwd_passes), vp(self.d_ev_begin.data_ptr()),
                                                       vp(self.d_ev_kind.data_ptr()), vp(self.d_ev_off.data_ptr()),
-                                                      p.tangent.end_base, adjoint.TangentPlan.TMAX,
+                                                      p.tangent.end_base, adjoint.TangentPlan.TMAX, None,
                                                       vp(self.d_flags.data_ptr()), st), 'rows tangent form')
         rows_forward(self.kf, self.psi, n, self.code, B, self.fwd_passes, self.d_fwd_ops, self.pools, p.pool_stride,
                      st)

@@ -74,7 +74,12 @@ if RB not in (5, 6):
     raise ValueError('DESV_ROT_RB must be 5 or 6')
 LOW_FIXED = 5          # index bits 0..LOW_FIXED-1 are in every tile (contiguous bulk-copy runs)
 TMAX = 2.0 ** 20       # tangent form while |tan| <= TMAX (FP32 keeps its relative accuracy; see materialize)
-SCALE_LIMIT = 2.0 ** 60  # pending tangent scale above which rotations switch to the general form
+# pending tangent scale above which rotations switch to the general form.  Every tangent rotation
+# scales ALL amplitudes by the same 1/c, and a pass starts from |amp| <= 1, so inside a pass
+# |amp| <= SCALE_LIMIT and each fma result is at most TMAX * SCALE_LIMIT = 2^120 < FP32's 2^128.
+# The product of up to MAX_ROTS_PER_PASS random 1/|cos| is heavy-tailed: at 2^60 about one pass in
+# a few dozen of a random-angle circuit needed the general kernel; at 2^100 that is rare.
+SCALE_LIMIT = 2.0 ** 100
 MAX_ROTS_PER_PASS = 32  # measured on the 30-qubit, 40-layer brick circuit: 24 -> 246 ms, 32 -> 233, 48 -> 236
 PAD_SHIFT = 4          # padded stage layout: physical = i + (i >> 4)
 # ring slots per CTA, measured on the 30-qubit, 40-layer brick circuit: 1 -> four CTAs (16 warps)

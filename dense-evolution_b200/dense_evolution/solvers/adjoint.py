@@ -124,6 +124,8 @@ class TangentPlan:
         wpe = generic_pool.dtype.itemsize // 4
         name_of = {rec: back.fops[fi].src[0].name for rec, fi in back.op_slots}
         kind_of = {rec: back.fops[fi].kind for rec, fi in back.op_slots}
+        slot_of = {rec: back.fops[fi].src[0].slot for rec, fi in back.op_slots}
+        self.off_slot = {}    # pool offset of a tangent record -> its theta slot
         ops = back.ops
         self.end_base = pool_len
         self.passes = []      # per pass: (records in tangent form {rec: 'rot' | 'phase'}, events)
@@ -152,12 +154,44 @@ class TangentPlan:
                 else:
                     continue
                 events.append(('t', off, tan[q]))
+                self.off_slot[off] = int(slot_of.get(q, -1))
             self.passes.append((tan, events))
 
     def sources_info(self) -> list:
         """Per pass the tangent argument of jit.adjoint_source (None: no record
         in tangent form, the general kernel serves it)."""
         return [(tan, self.end_base + i) if tan else None for i, (tan, _) in enumerate(self.passes)]
+
+    def allowed(self, theta: np.ndarray) -> np.ndarray:
+        """Per pass whether it runs in tangent form, from the angles alone and
+        with a margin of 2 on both bounds (|t| <= TMAX / 2, S <= TMAX^2 / 4):
+        the tangent of a ry / rz inverse is +-tan(theta / 2) and every 1/c is
+        1 / cos(theta / 2), so the check needs no matrices (the device then
+        rewrites the allowed passes without checking again)."""
+        ps, kind, off = self._flat()
+        npass = len(self.passes)
+        out = np.zeros(npass, bool)
+        if ps.size == 0:
+            return out
+        tanm = kind <= 1
+        slots = np.array([self.off_slot.get(int(o), -1) for o in off[tanm]], np.int64) \
+            if not hasattr(self, '_tan_slots') else self._tan_slots
+        self._tan_slots = slots
+        if np.any(slots < 0):
+            return out
+        half = 0.5 * np.asarray(theta, dtype=np.float64)[slots]
+        c = np.abs(np.cos(half))
+        with np.errstate(divide='ignore'):
+            t = np.abs(np.sin(half)) / c
+            lg = -np.log(c)
+        tp = ps[tanm]
+        ok_t = np.ones(npass, bool)
+        np.logical_and.at(ok_t, tp, t <= 0.5 * self.TMAX)
+        logs = np.zeros(npass)
+        np.add.at(logs, tp, lg)
+        has = np.zeros(npass, bool)
+        has[tp] = True
+        return has & ok_t & (logs <= np.log(0.25 * self.TMAX * self.TMAX))
 
     def _flat(self):
         """Flat event arrays (pass, kind 0 rot / 1 phase / 2 probe with compiled-in
@@ -252,6 +286,7 @@ class AdjointProgram:
         self._stage: dict = {}
         self._scratch = None
         self._tangent = None          # TangentPlan, built with the first specialised gradient
+        self._dv = None               # device-built backward values (recipes + tangent form), or False
         import os
         self._use_tangent = (self.back is not None and dtype == torch.complex64 and jit.enabled(self.n)
                              and os.environ.get('DESV_ADJ_TANGENT', '1') != '0')
@@ -368,7 +403,80 @@ class AdjointProgram:
         ev.record()
         return devbuf
 
+    def _device_values(self, dev):
+        """Recipes, constants and event tables that build the backward passes'
+        values on the device from theta (complex64 tangent-form programs):
+        the host then uploads only theta and one byte per pass.  False when a
+        record has no recipe (a controlled parametric diagonal, a dense 4x4)."""
+        if self._dv is not None:
+            return self._dv
+        self._dv = False
+        if not self._use_tangent:
+            return False
+        from ..batch import _Plan
+        cdt = np.complex64
+        generic = self.back.materialize(0.37 + 0.0137 * np.arange(max(self.nparams, 1)), cdt)
+        try:
+            recipes = _Plan._recipes(self.back, 0)
+        except (RuntimeError, KeyError):
+            return False
+        if self._tangent is None:
+            self._tangent = TangentPlan(self.back, len(generic), generic)
+        tp = self._tangent
+        begin, kinds, offs = [0], [], []
+        for tan, events in tp.passes:
+            if tan:
+                for kind, off, x in events:
+                    kinds.append((0 if x == 'rot' else 1) if kind == 't' else (3 if x else 2))
+                    offs.append(off)
+            begin.append(len(kinds))
+
+        def up(a):
+            return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+
+        npass = len(self.back.passes)
+        self._dv = dict(
+            generic=generic, recipes=up(recipes), nrec=len(recipes),
+            cpool=torch.from_numpy(generic.view(np.float32).copy()).to(dev),
+            pool=torch.empty(len(generic) + npass, dtype=torch.complex64, device=dev),
+            ev_begin=up(np.array(begin, np.int32)), ev_kind=up(np.array(kinds or [0], np.uint8)),
+            ev_off=up(np.array(offs or [0], np.uint32)), flags=torch.empty(npass, dtype=torch.uint8, device=dev))
+        return self._dv
+
+    def _upload_backward_device(self, theta, dev, dv):
+        key = np.asarray(theta, dtype=np.float64).tobytes()
+        if self._back_dev is not None and self._back_dev[0] == key:
+            return self._back_dev
+        th = np.zeros(max(self.nparams, 1))
+        t = np.asarray(theta, dtype=np.float64).reshape(-1)[:th.size]
+        th[:t.size] = t
+        allowed = self._tangent.allowed(th)
+        ops_t = self._staged('ops', self.back.ops, dev)
+        th_t = self._staged('theta', th, dev)
+        al_t = self._staged('allowed', allowed.astype(np.uint8), dev)
+        vp = ctypes.c_void_p
+        st = vp(N.stream_ptr())
+        pool = dv['pool']
+        N.check(N.lib().desv_rows_prepare(None, self.n, N.DESV_C64, 1, vp(dv['recipes'].data_ptr()), dv['nrec'],
+                                          vp(th_t.data_ptr()), th.size, vp(dv['cpool'].data_ptr()),
+                                          vp(pool.data_ptr()), pool.numel(), st), 'backward values')
+        N.check(N.lib().desv_rows_tangent_prepare(vp(pool.data_ptr()), N.DESV_C64, 1, pool.numel(),
+                                                  len(self.back.passes), vp(dv['ev_begin'].data_ptr()),
+                                                  vp(dv['ev_kind'].data_ptr()), vp(dv['ev_off'].data_ptr()),
+                                                  self._tangent.end_base, TangentPlan.TMAX, vp(al_t.data_ptr()),
+                                                  vp(dv['flags'].data_ptr()), st), 'backward tangent form')
+        if self._map_dev is None or self._map_dev.device != dev:
+            self._map_dev = torch.tensor(self.back.param_map or [0], dtype=torch.int32, device=dev)
+        self._back_dev = (key, ops_t, pool, self._map_dev, dv['generic'], [bool(x) for x in allowed])
+        return self._back_dev
+
     def _upload_backward(self, theta, dev):
+        dv = self._device_values(dev) if self._use_tangent else False
+        if dv:
+            return self._upload_backward_device(theta, dev, dv)
+        return self._upload_backward_host(theta, dev)
+
+    def _upload_backward_host(self, theta, dev):
         """(key, ops, mats, map, host mats) of the backward passes for theta;
         the host work and the uploads do not wait for the device, so they
         overlap forward passes already queued."""

@@ -293,10 +293,12 @@ int desv_jit_pauli_matvec_rows(void *const *handles, const double *csym_dev, int
  * -- and writes the pass-end factor 1/S to end_base + p.  flags_dev[p * rows +
  * r] = 1 where row r runs pass p in tangent form; a row whose |t| leaves
  * [0, tmax] or whose S leaves [0, tmax^2] is left untouched (flag 0) and runs
- * the general kernel. */
+ * the general kernel.  allowed_dev (NULL, or one byte per pass, the caller's
+ * choice from the angles) replaces that check. */
 int desv_rows_tangent_prepare(void *pools_dev, int dtype, int rows, int64_t pool_stride, int npasses,
                               const int32_t *ev_begin_dev, const uint8_t *ev_kind_dev, const uint32_t *ev_off_dev,
-                              int64_t end_base, double tmax, uint8_t *flags_dev, void *stream);
+                              int64_t end_base, double tmax, const uint8_t *allowed_dev, uint8_t *flags_dev,
+                              void *stream);
 /* One rows backward pass with the row's form chosen per row: the tangent kernel
  * runs the rows whose rflag_dev entry is 1, the general kernel the others (both
  * launched, on one grid), then the per-row gradient reduction. */

@@ -197,3 +197,47 @@ def test_rows_tangent_events_reproduce_the_host_transform():
         dev[p.tangent.end_base + q] = 1.0 / S
     m = len(want)
     assert np.allclose(dev[:m], want, rtol=1e-6, atol=1e-7)
+
+
+def test_single_circuit_backward_values_from_recipes():
+    """The single-circuit gradient builds its backward passes' values on the
+    device: the batched VQE's recipes applied to theta reproduce the host
+    materialisation of the backward pool, and the angle-only tangent choice
+    (TangentPlan.allowed, with its margin) never admits a pass the full check
+    on the matrices would refuse."""
+    import os
+    import torch
+    from dense_evolution.batch import _Plan
+    from dense_evolution.solvers.adjoint import AdjointProgram, TangentPlan
+    from dense_evolution.solvers.autodiff import build_template
+    from dense_evolution.workloads import hea_circuit
+    os.environ['DESV_JIT'] = '1'
+    try:
+        n = 12
+        rows, slots, npar = build_template(hea_circuit(n, 3), n)
+        prog = AdjointProgram(rows, slots, n, torch.complex64)
+    finally:
+        del os.environ['DESV_JIT']
+    generic = prog.back.materialize(0.37 + 0.0137 * np.arange(npar), np.complex128)
+    recipes = _Plan._recipes(prog.back, 0)
+
+    class _P:
+        pass
+    holder = _P()
+    holder.recipes = recipes
+    tp = TangentPlan(prog.back, len(generic), generic.astype(np.complex64))
+    rng = np.random.default_rng(4)
+    for k in range(5):
+        theta = rng.uniform(-np.pi, np.pi, npar)
+        if k == 4:
+            theta[::3] = np.pi - 1e-9          # near pi: tangents out of range
+        dev = _recipe_pool(holder, theta, generic)
+        host = prog.back.materialize(theta, np.complex128)
+        assert np.allclose(dev, host, atol=1e-12)
+        _, ok = tp.transform(host.astype(np.complex64))
+        al = tp.allowed(theta)
+        assert all((not a) or o for a, o in zip(al, ok))
+        if k < 4:
+            assert all(al)
+        else:
+            assert not all(al)
