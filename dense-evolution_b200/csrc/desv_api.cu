@@ -235,6 +235,60 @@ int desv_collapse(void *sv, int n, int dtype, int bit, int outcome, double s, vo
     return collapse(sv, n, dtype, bit, outcome, s, S(stream));
 }
 
+// Side streams of the current device for the <H> passes: they only read psi and
+// each writes its own partial rows, so pass p > 0 runs on side stream (p - 1) %
+// PAULI_SIDE, forked from and joined back into the caller's stream by events.
+// One pass's tail then overlaps the next pass's start.  The mutex is held from the
+// fork to the join, so two host threads never interleave their event records.
+constexpr int PAULI_SIDE = 3;
+struct PauliSide {
+    cudaStream_t s[PAULI_SIDE];
+    cudaEvent_t fork, join[PAULI_SIDE];
+    bool ok;
+};
+static std::mutex g_side_mu;
+
+static PauliSide *pauli_side() {  // called with g_side_mu held
+    static PauliSide side[64];
+    static bool made[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    PauliSide &ps = side[dev];
+    if (!made[dev]) {
+        made[dev] = true;
+        ps.ok = cudaEventCreateWithFlags(&ps.fork, cudaEventDisableTiming) == cudaSuccess;
+        for (int k = 0; k < PAULI_SIDE && ps.ok; ++k)
+            ps.ok = cudaStreamCreateWithFlags(&ps.s[k], cudaStreamNonBlocking) == cudaSuccess &&
+                    cudaEventCreateWithFlags(&ps.join[k], cudaEventDisableTiming) == cudaSuccess;
+        if (!ps.ok) cudaGetLastError();
+    }
+    return ps.ok ? &ps : nullptr;
+}
+
+// Whether the <H> passes may fork: not while the caller's stream is being captured
+// into a graph (the capture would pull the side streams in), and only with a
+// working set of side streams.
+static PauliSide *pauli_fork(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (cs != cudaStreamCaptureStatusNone) return nullptr;
+    PauliSide *ps = pauli_side();
+    if (!ps) return nullptr;
+    if (cudaEventRecord(ps->fork, st) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    for (int k = 0; k < PAULI_SIDE; ++k)
+        if (cudaStreamWaitEvent(ps->s[k], ps->fork, 0) != cudaSuccess) return nullptr;
+    return ps;
+}
+
 // handles: NULL, or one specialised kernel (or NULL) per pass (desv_jit_pauli)
 static int pauli_common(const void *psi, void *out, int n, int dtype, const desv_pauli_pass *passes, int npasses,
                         const desv_pauli_term *terms, double *expect, void *scratch, size_t sb, bool matvec,
@@ -252,30 +306,60 @@ static int pauli_common(const void *psi, void *out, int n, int dtype, const desv
     for (int p = 0; p < npasses; ++p) {
         const desv_pauli_pass &ps = passes[p];
         if (ps.term_begin < 0 || ps.term_end < ps.term_begin) return fail(DESV_EINVAL, "Pauli term range invalid");
-        const int nt = ps.term_end - ps.term_begin;
-        if (nt == 0 && (!matvec || wrote)) continue;
-        if (want_e && rows + 4096 > cap_rows) return fail(DESV_EINVAL, "scratch too small for this many Pauli passes");
-        const int mode = matvec ? (wrote ? 2 : 1) : 0;
-        int grid = 0;
-        if (ps.tile_bits == 0) {  // flip masks wider than a tile: global-memory partner reads
-            r = pauli_direct(psi, out, dtype, mode, n, terms + ps.term_begin, nt, want_e ? 1 : 0, part + 2 * rows,
-                             &grid, S(stream));
-        } else {
+        if (ps.tile_bits != 0) {
             TileGeom g;
             if (ps.tile_bits > n || ps.low_bits < (n < 5 ? n : 5) ||
                 !make_geom(g, n, ps.tile_bits, ps.low_bits, ps.high))
                 return fail(DESV_EINVAL, "Pauli pass " + std::to_string(p) + ": invalid tile geometry");
+        }
+    }
+    int launching = 0;
+    for (int p = 0; p < npasses; ++p) launching += passes[p].term_end > passes[p].term_begin;
+    // <H> alone: the passes are independent reads of psi, run concurrently
+    std::unique_lock<std::mutex> side_lock(g_side_mu, std::defer_lock);
+    PauliSide *side = nullptr;
+    if (!matvec && launching > 1) {
+        side_lock.lock();
+        side = pauli_fork(S(stream));
+        if (!side) side_lock.unlock();
+    }
+    int launched = 0;
+    for (int p = 0; p < npasses && !r; ++p) {
+        const desv_pauli_pass &ps = passes[p];
+        const int nt = ps.term_end - ps.term_begin;
+        if (nt == 0 && (!matvec || wrote)) continue;
+        if (want_e && rows + 4096 > cap_rows) {
+            r = fail(DESV_EINVAL, "scratch too small for this many Pauli passes");
+            break;
+        }
+        const int mode = matvec ? (wrote ? 2 : 1) : 0;
+        const cudaStream_t ls = side && launched > 0 ? side->s[(launched - 1) % PAULI_SIDE] : S(stream);
+        int grid = 0;
+        if (ps.tile_bits == 0) {  // flip masks wider than a tile: global-memory partner reads
+            r = pauli_direct(psi, out, dtype, mode, n, terms + ps.term_begin, nt, want_e ? 1 : 0, part + 2 * rows,
+                             &grid, ls);
+        } else {
+            TileGeom g;
+            make_geom(g, n, ps.tile_bits, ps.low_bits, ps.high);
             if (handles && handles[p])
-                r = jit_pauli_launch(handles[p], psi, out, dtype, mode, g, want_e ? 1 : 0, part + 2 * rows, &grid,
-                                     S(stream));
+                r = jit_pauli_launch(handles[p], psi, out, dtype, mode, g, want_e ? 1 : 0, part + 2 * rows, &grid, ls);
             else
                 r = pauli_pass(psi, out, dtype, mode, g, terms + ps.term_begin, nt, want_e ? 1 : 0,
-                               part + 2 * rows, &grid, S(stream));
+                               part + 2 * rows, &grid, ls);
         }
-        if (r) return r;
+        if (r) break;
         if (want_e) rows += grid;
         wrote = true;
+        ++launched;
     }
+    if (side) {  // join every side stream back into the caller's stream, also on an error
+        for (int k = 0; k < PAULI_SIDE; ++k) {
+            cudaEventRecord(side->join[k], side->s[k]);
+            cudaStreamWaitEvent(S(stream), side->join[k], 0);
+        }
+        side_lock.unlock();
+    }
+    if (r) return r;
     if (matvec && !wrote) {
         const size_t es = dtype == DESV_C64 ? 8 : 16;
         if (cudaMemsetAsync(out, 0, (1ull << n) * es, S(stream)) != cudaSuccess) return check_launch("matvec zero");

@@ -161,10 +161,11 @@ def dtype_code(t: torch.Tensor) -> int:
 _scratch = {}
 
 
-def scratch(n: int, device: torch.device) -> torch.Tensor:
-    """Per-device reduction scratch, grown on demand and reused by every call."""
+def scratch(n: int, device: torch.device, stream=None) -> torch.Tensor:
+    """Reduction scratch per device and stream, grown on demand and reused by every
+    call on that stream (calls on one stream are ordered; two streams never share)."""
     need = int(lib().desv_scratch_bytes(n, 0))
-    key = device.index if device.index is not None else torch.cuda.current_device()
+    key = (device.index if device.index is not None else torch.cuda.current_device(), stream_ptr(stream))
     buf = _scratch.get(key)
     if buf is None or buf.numel() * 8 < need:
         buf = torch.empty((need + 7) // 8, dtype=torch.float64, device=device)

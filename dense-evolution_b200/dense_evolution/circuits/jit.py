@@ -363,8 +363,11 @@ def _expect_source(terms: np.ndarray, K: int, L: int, high, complex64: bool) -> 
     R = 'float' if complex64 else 'double'
     high = [int(h) for h in high[:K - L]]
     tile_mask = ((1 << L) - 1) | sum(1 << h for h in high)
+    # as many CTAs per SM as the ring allows (three for 64 KB): without the
+    # bound the compiler took 128 registers for 8-mask passes of 12-bit tiles,
+    # which left two CTAs (16 warps) per SM; with it they take 80, no spills
     lines = ['#include "jit_pass.cuh"', 'using namespace desv;',
-             'extern "C" __global__ void __launch_bounds__(256)',
+             f'extern "C" __global__ void __launch_bounds__(256, {_pauli_min_blocks(K, complex64)})',
              f'desv_jit_kernel(const {T} *psi, {T} *out, TileGeom g, int want_e, double *part) {{',
              '    extern __shared__ __align__(128) unsigned char smem[];',
              f'    auto body = [=]({T} *s, uint64_t base, const uint64_t *ctab, int L, double &ere, double &eim) {{']
@@ -413,16 +416,26 @@ def _expect_source(terms: np.ndarray, K: int, L: int, high, complex64: bool) -> 
         for k, *_ in cplx:
             decl += [f'sr{k}', f'si{k}']
     lines += [f'        {R} {", ".join(n + " = 0" for n in decl)};'] if decl else []
+    # Amplitude j = t | (k << 8) of the tile (t the thread, k the unrolled row):
+    # its partner j ^ x is (t ^ x_lo) ^ ((k ^ x_hi) << 8), a per-thread part
+    # formed once per flip mask and a compile-time offset, so no index
+    # arithmetic is left per amplitude (the form j0 + r * 256 hid that from the
+    # compiler, which cannot know threadIdx.x < 256 from it)
+    if K < 8:
+        raise ValueError('specialised <H> passes need tiles of at least 8 bits')
+    lines.append('        const uint32_t t = threadIdx.x & 255u;')
+    for gi, (xl, *_rest) in enumerate(plan):
+        lines.append(f'        const uint32_t tx{gi} = t ^ {xl & 255}u;')
+        lines.append(f'        const {T} *q{gi} = s + tx{gi};')
     lines += ['#pragma unroll',
-              f'        for (uint32_t j0 = threadIdx.x; j0 < {1 << K}u; j0 += 1024u) {{',
-              '#pragma unroll',
-              '            for (int r = 0; r < 4; ++r) {',
-              '                const uint32_t j = j0 + r * 256u;',
-              f'                const {T} a = s[j];']
+              f'        for (uint32_t k = 0; k < {1 << (K - 8)}u; ++k) {{',
+              '            {',
+              f'                const {T} a = s[t + (k << 8)];']
     for gi, (xl, classes, outside, single, cplx) in enumerate(plan):
         lines.append('                {')
-        lines.append(f'                    const uint32_t jx = j ^ {xl}u;')
-        lines.append(f'                    const {T} q = s[jx];')
+        lines.append(f'                    const uint32_t kx = (k ^ {xl >> 8}u) << 8;')
+        lines.append(f'                    const uint32_t jx = tx{gi} ^ kx;')
+        lines.append(f'                    const {T} q = q{gi}[kx];')
         lines.append(f'                    const {R} w = a.x * q.x + a.y * q.y;')
         if cplx:
             lines.append(f'                    const {R} wi = a.x * q.y - a.y * q.x;')
@@ -609,8 +622,17 @@ def pauli_source(terms: np.ndarray, tile_bits: int, low_bits: int, high, mode: i
 
 def pauli_nbuf(tile_bits: int) -> int:
     """Ring slots of a specialised Pauli pass: four for tiles of up to 11 bits,
-    two for 12-bit tiles (three CTAs of 64 KB per SM)."""
-    return 2 if tile_bits >= 12 else 4
+    two for 12-bit tiles (three CTAs of 64 KB per SM; DESV_PAULI_NBUF12
+    overrides the latter, for tuning)."""
+    if tile_bits >= 12:
+        return int(os.environ.get('DESV_PAULI_NBUF12', '2'))
+    return 4
+
+
+def _pauli_min_blocks(tile_bits: int, complex64: bool) -> int:
+    """CTAs per SM the ring of a Pauli pass leaves room for (at most three)."""
+    ring = pauli_nbuf(tile_bits) * ((8 if complex64 else 16) << tile_bits) + 4096
+    return max(1, min(3, (220 << 10) // ring))
 
 
 def pauli_modes(passes: np.ndarray, matvec: bool) -> list:

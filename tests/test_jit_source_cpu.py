@@ -169,3 +169,44 @@ def test_pauli_sources_of_mixed_terms_compile(dtname):
             assert r == 0, log.value.decode()[-3000:]
             count += 1
     assert count >= 2
+
+
+@pytest.mark.parametrize('K', [11, 12])
+@pytest.mark.parametrize('which', ['tfim', 'xxz', 'random'])
+def test_pauli_plan_balance_keeps_every_term_in_a_covering_tile(K, which):
+    """The planner spreads flip masks that several tiles cover over the passes:
+    every term still sits in exactly one pass whose tile holds all its flip bits,
+    the packed terms are the caller's (a permutation), and for the TFIM chain no
+    pass carries more than one flip mask above an even share."""
+    import torch
+    from dense_evolution.physics.observables import PauliPlan
+    from dense_evolution.workloads import tfim_terms, xxz_terms
+    n = 24
+    if which == 'tfim':
+        terms = tfim_terms(n)
+    elif which == 'xxz':
+        terms = xxz_terms(n, 1.0)
+    else:
+        rng = np.random.default_rng(3)
+        terms = []
+        for _ in range(90):
+            w = int(rng.integers(1, 4))
+            qs = rng.choice(n, w, replace=False)
+            terms.append((float(rng.normal()), {int(q): str(rng.choice(list('XYZ'))) for q in qs}))
+    plan = PauliPlan(terms, n, tile_bits=K)
+    assert sorted(plan.order.tolist()) == list(range(len(terms)))
+    masks_per_pass = []
+    for r in plan.passes:
+        b, e = int(r['term_begin']), int(r['term_end'])
+        assert e - b <= PauliPlan.MAX_TERMS_PER_PASS
+        if int(r['tile_bits']) == 0:
+            continue
+        L = int(r['low_bits'])
+        high = [int(h) for h in r['high'][:int(r['tile_bits']) - L]]
+        cover = ((1 << L) - 1) | sum(1 << h for h in high)
+        xs = plan.terms['xmask'][b:e].astype(np.uint64)
+        assert all(int(x) & ~cover == 0 for x in xs)
+        masks_per_pass.append(len({int(x) for x in xs if int(x)}))
+    if which == 'tfim':
+        share = -(-n // len(masks_per_pass))
+        assert max(masks_per_pass) <= share + 1, masks_per_pass
