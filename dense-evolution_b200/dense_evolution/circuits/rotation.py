@@ -675,40 +675,68 @@ class RotationPlan:
 
     _KIND = {'rx': 1, 'ry': 2, 'rz': 3, 'p': 4, 'u1': 4, 'phase': 4}
 
-    def uop_matrices(self, theta=None, runs_=None) -> np.ndarray:
-        """FP64 2x2 matrix of every fused run for these parameters (vectorised:
-        every gate's matrix at once by kind, then the products along the runs
-        position by position)."""
+    def gate_table(self, runs_=None) -> dict:
+        """Per-gate arrays of the fused runs (kind, theta slot, fixed value,
+        constant matrices), built once per bound circuit so that a call only
+        gathers theta."""
         runs_ = [u.gates for u in self.uops] if runs_ is None else runs_
-        R_ = len(runs_)
-        M = np.tile(np.eye(2, dtype=np.complex128), (R_, 1, 1))
-        if R_ == 0:
-            return M
-        lens = np.array([len(r) for r in runs_])
+        lens = np.array([len(r) for r in runs_], np.int64)
         flat = [g for r in runs_ for g in r]
         G = len(flat)
         kind = np.zeros(G, np.int8)
-        val = np.zeros(G)
-        mats = np.tile(np.eye(2, dtype=np.complex128), (G, 1, 1))
-        th = None if theta is None else np.asarray(theta, dtype=np.float64)
+        slot = np.full(G, -1, np.int64)
+        sval = np.zeros(G)
+        cidx, cmats = [], []
         for i, g in enumerate(flat):
             if g.const is not None:
-                mats[i] = g.const
+                cidx.append(i)
+                cmats.append(np.asarray(g.const, dtype=np.complex128))
             else:
                 kind[i] = self._KIND[g.name]
-                val[i] = g.value if g.slot < 0 or th is None else th[g.slot]
+                slot[i] = g.slot
+                sval[i] = g.value if g.value is not None else 0.0
+        return dict(R=len(runs_), lens=lens, kind=kind, slot=slot, sval=sval, cidx=np.array(cidx, np.int64),
+                    cmats=np.array(cmats).reshape(-1, 2, 2), start=np.concatenate([[0], np.cumsum(lens)[:-1]]))
+
+    def uop_matrices(self, theta=None, runs_=None, gtab=None) -> np.ndarray:
+        """FP64 2x2 matrix of every fused run for these parameters (vectorised:
+        every gate's matrix at once by kind, then the products along the runs
+        position by position)."""
+        if gtab is None:
+            if runs_ is None:
+                if getattr(self, '_gtab', None) is None:
+                    self._gtab = self.gate_table()
+                gtab = self._gtab
+            else:
+                gtab = self.gate_table(runs_)
+        R_ = gtab['R']
+        M = np.tile(np.eye(2, dtype=np.complex128), (R_, 1, 1))
+        if R_ == 0:
+            return M
+        lens, kind = gtab['lens'], gtab['kind']
+        G = len(kind)
+        mats = np.tile(np.eye(2, dtype=np.complex128), (G, 1, 1))
+        if len(gtab['cidx']):
+            mats[gtab['cidx']] = gtab['cmats']
+        val = gtab['sval'].copy()
+        if theta is not None:
+            th = np.asarray(theta, dtype=np.float64)
+            m = gtab['slot'] >= 0
+            val[m] = th[gtab['slot'][m]]
         c, s_ = np.cos(val / 2), np.sin(val / 2)
-        k = kind == 1
-        mats[k] = np.stack([np.stack([c[k], -1j * s_[k]], -1), np.stack([-1j * s_[k], c[k]], -1)], -2)
-        k = kind == 2
-        mats[k] = np.stack([np.stack([c[k], -s_[k]], -1), np.stack([s_[k], c[k]], -1)], -2)
-        k = kind == 3
-        mats[k] = 0
+        if 'by_kind' not in gtab:
+            gtab['by_kind'] = [np.nonzero(kind == q)[0] for q in range(5)]
+        k = gtab['by_kind'][1]          # rx
+        mats[k, 0, 0] = mats[k, 1, 1] = c[k]
+        mats[k, 0, 1] = mats[k, 1, 0] = -1j * s_[k]
+        k = gtab['by_kind'][2]          # ry
+        mats[k, 0, 0] = mats[k, 1, 1] = c[k]
+        mats[k, 0, 1], mats[k, 1, 0] = -s_[k], s_[k]
+        k = gtab['by_kind'][3]          # rz
         mats[k, 0, 0], mats[k, 1, 1] = np.exp(-0.5j * val[k]), np.exp(0.5j * val[k])
-        k = kind == 4
-        mats[k] = 0
-        mats[k, 0, 0], mats[k, 1, 1] = 1.0, np.exp(1j * val[k])
-        start = np.concatenate([[0], np.cumsum(lens)[:-1]])
+        k = gtab['by_kind'][4]          # phase
+        mats[k, 1, 1] = np.exp(1j * val[k])
+        start = gtab['start']
         for pos in range(int(lens.max())):
             sel = np.nonzero(lens > pos)[0]
             M[sel] = mats[start[sel] + pos] @ M[sel]
@@ -792,17 +820,26 @@ class RotationPlan:
                         diag_u=np.array([i for i, u in enumerate(self.uops) if u.diag], np.int64))
         return self._vp
 
-    def materialize(self, theta=None, dtype=np.float32, ir=None) -> Tuple[List[np.ndarray], complex]:
+    def bound(self, ir: Sequence[fusion.IRGate]):
+        """bind(ir) and the gate table of its runs: what materialize needs of a
+        circuit of this structure, computed once per circuit."""
+        runs_, d2g, scalars = self.bind(ir)
+        return runs_, d2g, scalars, self.gate_table(runs_)
+
+    def materialize(self, theta=None, dtype=np.float32, ir=None, bound=None) -> Tuple[List[np.ndarray], complex]:
         """Per-pass parameter blocks (float32 for the kernels; float64 for exact
         emulation in tests) for these parameters, and the circuit's global
-        factor (applied by the last pass's end factor)."""
+        factor (applied by the last pass's end factor).  bound: the result of
+        bound(ir), when the caller keeps it across calls."""
         vp = self._prepare_values()
-        if ir is not None:
-            runs_, d2g, scalars = self.bind(ir)
+        if ir is not None and bound is None:
+            bound = self.bound(ir)
+        if bound is not None:
+            runs_, d2g, scalars, gtab = bound
         else:
-            runs_, d2g, scalars = None, {pi: pr.gate for pi, pr in enumerate(self.prims) if pr.kind == 'd2'}, \
-                self.scalars
-        M = self.uop_matrices(theta, runs_)
+            runs_, d2g, scalars, gtab = None, {pi: pr.gate for pi, pr in enumerate(self.prims) if pr.kind == 'd2'}, \
+                self.scalars, None
+        M = self.uop_matrices(theta, runs_, gtab)
         det = M[:, 0, 0] * M[:, 1, 1] - M[:, 0, 1] * M[:, 1, 0]
         g = np.sqrt(det)
         V = M / np.where(g == 0, 1, g)[:, None, None]
@@ -850,33 +887,48 @@ class RotationPlan:
             cv = np.exp(1j * src[vp['cval_src']])
             flat[vp['cval_pos']] = cv.real
             flat[vp['cval_pos'] + 1] = cv.imag
-        for pidx, ps in enumerate(self.passes):
-            us, pos = vp['rots'][pidx]
-            scale = 1.0
-            if len(us):
-                ci, si = c[us], s[us]
-                with np.errstate(divide='ignore'):
-                    t = np.where(ci > 0, si / np.where(ci > 0, ci, 1.0), np.inf)
-                tan = np.abs(t) <= TMAX
-                grow = np.cumprod(np.where(tan, 1.0 / np.where(tan, ci, 1.0), 1.0))
-                if grow[-1] > SCALE_LIMIT or np.any(grow > SCALE_LIMIT):
-                    # rare: keep the pending scale bounded rotation by rotation
-                    tan = tan.copy()
+        # every pass's rotations at once: tangents, forms and the pending scale
+        ra = vp.get('rot_all')
+        if ra is None:
+            lens = np.array([len(us) for us, _ in vp['rots']], np.int64)
+            live = np.nonzero(lens)[0]
+            ra = dict(us=np.concatenate([us for us, _ in vp['rots']] + [np.zeros(0, np.int64)]),
+                      pos=np.concatenate([pos for _, pos in vp['rots']] + [np.zeros(0, np.int64)]),
+                      lens=lens, live=live, starts=np.concatenate([[0], np.cumsum(lens)[:-1]])[live],
+                      pid=np.repeat(np.arange(len(lens)), lens))
+            vp['rot_all'] = ra
+        scales = np.ones(len(self.passes))
+        if len(ra['us']):
+            ci, si = c[ra['us']], s[ra['us']]
+            with np.errstate(divide='ignore'):
+                t = np.where(ci > 0, si / np.where(ci > 0, ci, 1.0), np.inf)
+            tan = np.abs(t) <= TMAX
+            inv = np.where(tan, 1.0 / np.where(tan, ci, 1.0), 1.0)
+            scales[ra['live']] = np.multiply.reduceat(inv, ra['starts'])
+            # the pending scale inside each pass, from logs; a pass that may pass
+            # SCALE_LIMIT (rare) is redone exactly, rotation by rotation
+            lg = np.log(inv)
+            cs = np.cumsum(lg)
+            within = cs - np.repeat((cs - lg)[ra['starts']], ra['lens'][ra['live']])
+            over = within > np.log(SCALE_LIMIT) - 1e-6
+            if over.any():
+                for pidx in np.unique(ra['pid'][over]):
+                    a = int(np.searchsorted(ra['pid'], pidx))
                     sc = 1.0
-                    for k in range(len(us)):
+                    for k in range(a, a + int(ra['lens'][pidx])):
                         if tan[k] and sc / ci[k] <= SCALE_LIMIT:
                             sc /= ci[k]
                         else:
                             tan[k] = False
-                    scale = sc
-                else:
-                    scale = float(grow[-1])
-                flat[pos] = np.where(tan, t, 0.0)
-                flat[pos + 1] = ci
-                flat[pos + 2] = si
-                flat[pos + 3] = np.where(tan, 0.0, 1.0)
+                    scales[pidx] = sc
+            pos = ra['pos']
+            flat[pos] = np.where(tan, t, 0.0)
+            flat[pos + 1] = ci
+            flat[pos + 2] = si
+            flat[pos + 3] = np.where(tan, 0.0, 1.0)
+        for pidx, ps in enumerate(self.passes):
             if ps.end_scale_off >= 0:
-                f = complex(1.0 / scale) * (glob if ps.end_complex else 1.0)
+                f = complex(1.0 / scales[pidx]) * (glob if ps.end_complex else 1.0)
                 o = int(vp['offs'][pidx]) + ps.end_scale_off
                 flat[o], flat[o + 1] = f.real, f.imag
         blocks = [flat[vp['offs'][i]:vp['offs'][i + 1]].astype(dtype) for i in range(len(self.passes))]
@@ -1260,6 +1312,7 @@ class BoundProgram:
         self.ir = ir
         self._key = None
         self._blocks = None
+        self._bound = None
 
     @property
     def plan(self) -> RotationPlan:
@@ -1268,8 +1321,10 @@ class BoundProgram:
     def blocks(self, theta=None) -> list:
         key = None if theta is None else np.asarray(theta, dtype=np.float64).tobytes()
         if self._blocks is None or key != self._key:
+            if self._bound is None:
+                self._bound = self.prog.plan.bound(self.ir)
             self._blocks = [np.ascontiguousarray(b, dtype=np.float32)
-                            for b in self.prog.plan.materialize(theta, np.float32, self.ir)[0]]
+                            for b in self.prog.plan.materialize(theta, np.float32, bound=self._bound)[0]]
             self._key = key
         return self._blocks
 

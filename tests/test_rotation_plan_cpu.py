@@ -195,3 +195,41 @@ def test_generated_sources_compile_with_nvrtc():
                 assert r == 0, log.value.decode()[-3000:]
         finally:
             os.environ.pop('DESV_ROT_CHECK', None)
+
+
+def test_pending_scale_limit_splits_the_tangent_form():
+    """Rotations near pi have cos(theta / 2) near 0, so their tangent scales
+    1 / cos multiply past SCALE_LIMIT inside one pass: the value program then
+    takes the general form for the rotations past the limit, keeps every
+    pass's tangent scale at or under it, and the state still matches the oracle."""
+    n = 12
+    rng = np.random.default_rng(8)
+    circ = []
+    for _ in range(6):
+        for q in range(n):
+            circ.append(('ry', q, float(np.pi - rng.uniform(1e-4, 1e-3))))
+        for q in range(0, n - 1, 2):
+            circ.append(('cz', q, q + 1))
+    plan = R.RotationPlan(QuantumTranspiler.transpile(circ), n, 12)
+    blocks, _ = plan.materialize(None, np.float64)
+    vp = plan._prepare_values()
+    split = 0
+    for pidx, ps in enumerate(plan.passes):
+        us, pos = vp['rots'][pidx]
+        if not len(us):
+            continue
+        off = pos - int(vp['offs'][pidx])
+        b = blocks[pidx]
+        tan = b[off + 3] == 0
+        split += int(np.sum(~tan))
+        scale = np.prod(1.0 / b[off + 1][tan])
+        assert scale <= R.SCALE_LIMIT
+        if ps.end_scale_off >= 0:
+            o = ps.end_scale_off
+            assert abs(complex(b[o], b[o + 1]) * scale) == pytest.approx(1.0, rel=1e-9)
+    assert split > 0
+    sv = np.zeros(1 << n, dtype=np.complex128)
+    sv[0] = 1
+    E.run(plan, sv, blocks)
+    ref = O.run_circuit(O.zero_state(n), n, circ)
+    assert np.max(np.abs(sv - ref)) <= 1e-9
