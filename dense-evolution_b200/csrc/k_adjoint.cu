@@ -110,27 +110,40 @@ __global__ void __launch_bounds__(1 << (K - 4), 1) k_adjoint_pass(T *phi, T *lam
 }
 
 // grad[map[p]] += 2 * sum_r part[r * np + p]   (fixed summation order); one
-// block per state of a rows launch (part and grad offset by the row strides)
-__global__ void k_grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad,
-                              int64_t part_stride, int64_t grad_stride) {
-    __shared__ double sh[32];
+// block per state of a rows launch (part and grad offset by the row strides).
+// One warp per parameter sums its column (lane-strided, then the warp tree);
+// then the first record of each distinct map target adds, in record order, the
+// sums of every record with that target, so a parameter that several records
+// of the pass probe is updated by one thread, exactly as the records come.
+constexpr int GRAD_REDUCE_THREADS = 512;
+__global__ void __launch_bounds__(GRAD_REDUCE_THREADS)
+k_grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad, int64_t part_stride,
+              int64_t grad_stride) {
+    extern __shared__ double sh[];  // np sums, then np map entries
+    int32_t *mp = reinterpret_cast<int32_t *>(sh + np);
     part += blockIdx.x * part_stride;
     grad += blockIdx.x * grad_stride;
-    for (int p = 0; p < np; ++p) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) mp[p] = map[p];
+    for (int p = w; p < np; p += nw) {
         double v = 0;
-        for (int r = threadIdx.x; r < rows; r += blockDim.x) v += part[(size_t)r * np + p];
+        for (int r = l; r < rows; r += 32) v += part[(size_t)r * np + p];
         v = warp_sum_d(v);
-        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        __syncthreads();
-        if (l == 0) sh[w] = v;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0;
-            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
-            grad[map[p]] += 2.0 * t;
-        }
+        if (l == 0) sh[p] = v;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const int32_t m = mp[p];
+        bool first = true;
+        for (int q = 0; q < p && first; ++q) first = mp[q] != m;
+        if (!first) continue;
+        double g = grad[m];
+        for (int q = p; q < np; ++q)
+            if (mp[q] == m) g += 2.0 * sh[q];
+        grad[m] = g;
     }
 }
+static size_t grad_reduce_smem(int np) { return (size_t)(np > 0 ? np : 1) * (sizeof(double) + sizeof(int32_t)); }
 
 constexpr int ADJ_MAX_PARAMS = 1024;
 constexpr int ADJ_MAX_ROWS = 1184;  // partial-sum rows per pass (= grid bound)
@@ -210,14 +223,15 @@ int adjoint_pass_rows(void *phi, void *lam, int dtype, const TileGeom &g, const 
 }
 
 int grad_reduce(const double *part, int rows, int np, const int32_t *map, double *grad, cudaStream_t st) {
-    k_grad_reduce<<<1, 256, 0, st>>>(part, rows, np, map, grad, 0, 0);
+    k_grad_reduce<<<1, GRAD_REDUCE_THREADS, grad_reduce_smem(np), st>>>(part, rows, np, map, grad, 0, 0);
     return check_launch("gradient reduce");
 }
 
 // the reduction of a rows adjoint pass: one block per state
 int grad_reduce_rows(const double *part, int rows_x, int np, const int32_t *map, double *grad, int nrows,
                      int64_t grad_stride, cudaStream_t st) {
-    k_grad_reduce<<<nrows, 256, 0, st>>>(part, rows_x, np, map, grad, (int64_t)rows_x * np, grad_stride);
+    k_grad_reduce<<<nrows, GRAD_REDUCE_THREADS, grad_reduce_smem(np), st>>>(part, rows_x, np, map, grad,
+                                                                       (int64_t)rows_x * np, grad_stride);
     return check_launch("gradient reduce (rows)");
 }
 
