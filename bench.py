@@ -210,16 +210,21 @@ def config1_cpu(layers=20, n=20):
             'z0': z[0]}
 
 
-def config1_gpu(layers=20, n=20, reps=3):
+def config1_gpu(layers=20, n=20, reps=20, warm=5):
     """Config 1 whole on the GPU through the public API (DenseSVSimulator,
-    complex128): seconds per circuit, state resident, <Z_i> read back."""
+    complex128): seconds per circuit, state resident, <Z_i> read back.  This
+    leg runs after the CPU baseline has left the GPU idle for half a minute, so
+    warm-up circuits come first and the mean is over 20 circuits (one full run
+    with one warm-up and three timed circuits read 17 ms; alone, 1.5 ms)."""
     import torch
     import dense_evolution as de
     from dense_evolution.workloads import brick_u3_circuit
     circ = brick_u3_circuit(n, layers, SEED)
     sim = de.DenseSVSimulator(n)
-    sim.run_circuit(circ)
-    z = sim.expectation_z()
+    for _ in range(warm):
+        sim.set_initial_state(None)
+        sim.run_circuit(circ)
+        z = sim.expectation_z()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(reps):

@@ -423,7 +423,13 @@ int desv_jit_adjoint_rows(void *handle, void *phi, void *lam, int n, int dtype, 
 
 /* ---- Pauli sums (replaces pauli_sum_expectation / pauli_sum_matvec,
  *      physics/observables.py:63-186,250-308) ------------------------------- */
-/* out_dev[0..1] = sum_k <psi|c_k P_k|psi> (re, im), FP64 accumulation. */
+/* out_dev[0..1] = sum_k <psi|c_k P_k|psi> (re, im), FP64 accumulation.  The
+ * passes only read psi and write disjoint partial rows, so pass p > 0 runs on
+ * one of three library-owned side streams of the current device, forked from
+ * `stream` and joined back into it by events before the final reduction: work
+ * queued on `stream` afterwards sees the result as usual.  While `stream` is
+ * being captured into a CUDA graph the passes run on `stream` in order.  The
+ * same holds for desv_jit_pauli with matvec = 0. */
 int desv_pauli_expect(const void *psi, int n, int dtype, const desv_pauli_pass *passes, int npasses,
                       const desv_pauli_term *terms_dev, double *out_dev, void *scratch,
                       size_t scratch_bytes, void *stream);
